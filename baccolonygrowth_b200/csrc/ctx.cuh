@@ -1,0 +1,93 @@
+/*
+ * ctx.cuh -- the bcg_ctx structure shared by the translation units.
+ */
+#pragma once
+#include "common.cuh"
+
+#define BCG_MAX_MG_LEVELS 16
+#define BCG_MAX_AGAR_LEVELS 8
+
+/* one multigrid level: three species, Sol/Res/Err, (nx+1) x (nz+1) points
+ * stored k-major (row k holds i = 0..nx contiguously, row pitch `pitch`) */
+struct MgLevel {
+    int nx, nz, pitch;
+    double* sol[3];   /* species 0 = carbon, 1 = oxygen, 2 = acetate */
+    double* res[3];
+    double* err[3];
+    float* errf[3];   /* FP32 shadows used by the mixed-precision solve */
+    float* resf[3];
+};
+
+/* one buffer of the colony environment (LocalEnv fields kept on device) */
+struct EnvBuf {
+    double *C, *W, *A, *O;     /* Carbon, Waste, Acetate, Oxygen */
+    double *gr1, *gr2;         /* GrowthRate1/2 */
+    double *ph, *hydrox, *acetic, *buffer;
+};
+
+/* one buffer of the wall rows, per composite level, 4 species */
+struct WallBuf {
+    double *C[BCG_MAX_AGAR_LEVELS], *W[BCG_MAX_AGAR_LEVELS], *O[BCG_MAX_AGAR_LEVELS], *A[BCG_MAX_AGAR_LEVELS];
+};
+
+struct bcg_ctx {
+    bcg_params P;
+    int device;
+    cudaStream_t stream;
+    int n;                 /* cells */
+    int cap;               /* max_cells */
+    int cur;               /* index of the "old" record buffer */
+    CellRec* rec[2];
+    CellSoA soa;
+    /* neighbours */
+    int kmax;
+    int* nbr;
+    int* ncount;
+    /* bins */
+    int nbox;
+    int* box_cnt;
+    int* box_start;        /* nbox + 1 */
+    int* box_ids;          /* cap */
+    int* cell_box;         /* cap */
+    int n_binned;          /* cells covered by the last binning */
+    int* scan_tmp;         /* block sums */
+    /* divisions */
+    int* div_list;         /* cap */
+    int* div_count;        /* device counter */
+    unsigned long long* fcw_count;
+    int* moved;            /* cap, per-step division bookkeeping */
+    int* delta_ids;        /* 2*cap */
+    int* delta_box;
+    int* lineage;          /* 2*cap */
+    int* n_done_dev;
+    float* draws_dev;      /* 9*cap */
+    int last_ndiv;
+    /* status */
+    DevStatus* status;     /* device */
+    /* pinned host staging */
+    void* pinned;
+    size_t pinned_bytes;
+    /* fields */
+    double *height, *rough_height, *nrm_x, *nrm_y, *nrm_z, *wall;
+    EnvBuf env[2];         /* [0] = Environment, [1] = oldEnvironment */
+    WallBuf wal[2];        /* [0] = FieldWall, [1] = oldFieldWall */
+    double *rd, *inside, *rds, *ds, *dens, *rws, *wds, *rw, *wd;
+    int* bbox;             /* device: minx, maxx, maxz (after +-5) */
+    int host_bbox[3];
+    MgLevel mg[BCG_MAX_MG_LEVELS];
+    int mg_levels;
+    double* mg_scratch;    /* reductions */
+    /* timers */
+    int timers_on;
+    cudaEvent_t ev[BCG_T_COUNT][2];
+    double timer_ms[BCG_T_COUNT];
+    long long timer_launches[BCG_T_COUNT];
+    long long launches;    /* kernels queued by this context (all kinds) */
+};
+
+MechParams mech_params(const bcg_ctx* c);
+FieldPtrs field_ptrs(const bcg_ctx* c);
+int ctx_check_status(bcg_ctx* c);   /* syncs, reads the device status word */
+void timer_begin(bcg_ctx* c, int t);
+void timer_end(bcg_ctx* c, int t, int launches);
+int ensure_pinned(bcg_ctx* c, size_t bytes);

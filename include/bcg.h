@@ -1,0 +1,349 @@
+/*
+ * bcg.h -- C ABI of the B200 (sm_100a) hot path of the BacColonyGrowth
+ * agent-based colony simulator.
+ *
+ * The library replaces the calls that the reference time loop
+ * (AgentBasedModel-BacColonyGrowth/Simulation.cpp:42-434, SimSingleThread)
+ * makes into Neighbours / Forces / Integrate / grow / Cells / Compute /
+ * Nutrients / Multigrid.  All colony and field state lives on one GPU in
+ * structure-of-arrays form inside a bcg_ctx; the host keeps the glibc rand()
+ * stream, the output/restart files and the loop flags, exactly as the
+ * reference does.  Every entry point returns a bcg_status (0 = OK); no entry
+ * point aborts the process, and no kernel traps.
+ *
+ * Citations are "file:line" inside AgentBasedModel-BacColonyGrowth/.
+ */
+#ifndef BCG_H_
+#define BCG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes (replace MyAssert, tools.h:13-27, and the silent break   */
+/* on maxCells, Simulation.cpp:382-386)                                  */
+/* ------------------------------------------------------------------ */
+typedef enum bcg_status {
+    BCG_OK = 0,
+    BCG_E_ARG = 1,              /* bad argument, size or null pointer            */
+    BCG_E_CUDA = 2,             /* CUDA runtime / launch error                   */
+    BCG_E_BOX_OVERFLOW = 3,     /* "Tried to add too many cells", UniformGrid.h:35 */
+    BCG_E_NEIGH_OVERFLOW = 4,   /* neighbour list over capacity, UniformGrid.h:162 */
+    BCG_E_OUT_OF_GRID = 5,      /* "Cells have expanded farther than boxes allows", UniformGrid.h:96 */
+    BCG_E_NAN = 6,              /* non-finite position / velocity detected        */
+    BCG_E_MAXCELLS = 7,         /* division stopped at MaxCells, Simulation.cpp:382 */
+    BCG_E_TIMEOUT = 8,          /* a bounded device wait gave up                  */
+    BCG_E_UNSUPPORTED = 9,      /* parameter combination the reference leaves undefined */
+    BCG_E_NEED_MORE_BOXES = 10, /* colony too close to the grid edge, Nutrients.cpp:360 */
+    BCG_E_NO_DEVICE = 11        /* no CUDA device / kernels not loadable          */
+} bcg_status;
+
+/* ------------------------------------------------------------------ */
+/* cell record: byte-identical to `struct Cell` (Cell.h:15-28, with      */
+/* Segment from tools.h:71-87), 208 bytes, so the reference's cell arrays */
+/* and its binary restart files (InputOutput.cpp:394-448) are passed       */
+/* through unchanged.                                                      */
+/* ------------------------------------------------------------------ */
+typedef struct bcg_vec3 { double x, y, z; } bcg_vec3;
+
+typedef struct bcg_cell {
+    bcg_vec3 p;             /* Segment.p */
+    bcg_vec3 q;             /* Segment.q */
+    double   time_p;        /* Segment.time_p */
+    double   time_q;        /* Segment.time_q */
+    int32_t  age_p;         /* Segment.age_p */
+    int32_t  age_q;         /* Segment.age_q */
+    double   length;        /* Cell.Length */
+    double   ldiv;          /* Cell.Ldiv */
+    double   radius;        /* Cell.Radius */
+    double   growth_rate;   /* Cell.GrowthRate */
+    bcg_vec3 velocity;      /* Cell.Velocity */
+    bcg_vec3 angular_velocity; /* Cell.AngularVelocity */
+    bcg_vec3 dyn_fric;      /* Cell.DynFric */
+    bcg_vec3 sta_fric;      /* Cell.StaFric */
+    int32_t  type;          /* Cell.Type */
+    int32_t  ancestor;      /* Cell.Ancestor */
+} bcg_cell;
+
+/* ------------------------------------------------------------------ */
+/* parameters: one POD mirror of the reference's mutable globals        */
+/* (Constants.h, defaults Constants.cpp:1-112, input keys                */
+/* InputOutput.cpp:450-677) plus the schedule constants the reference     */
+/* hard-codes (Multigrid.cpp:995-1017).                                   */
+/* ------------------------------------------------------------------ */
+typedef struct bcg_params {
+    /* grid (input keys Box_x, Box_y, Box_z, Box_z_agar, maxLevelsMG,
+     * FilterLen, refinementGridHeight, MaxCells) */
+    int32_t box_x, box_y, box_z, box_z_agar;
+    int32_t max_levels_mg;          /* composite agar levels (agarLevels) */
+    int32_t filter_len;
+    int32_t refinement_grid_height;
+    int32_t max_cells;
+    /* derived by bcg_params_finalize (CellMD3D.cpp:52-54, 141) */
+    int32_t max_cells_per_box;
+    int32_t max_neighbours;         /* capacity of one reduced neighbour list (device) */
+    double  box_length;
+
+    /* cell mechanics */
+    double cell_radius, l_divide, k_cc, k_wc, var_l, var_angle, var_pos;
+    double viscosity, wall_rough, gamma_t, cell_mu, wall_mu;
+    double density_threshold, tension, delta_h, rc;
+
+    /* time */
+    double dt, t0, t_max, output_time, update_time;
+
+    /* nutrients (Nutrients.cpp, Multigrid.cpp) */
+    double kc_aer, kc_ana, kw, ko, ka, ki;
+    double carbon_to_waste, c_rate, w_rate, maintenance_rate;
+    double q_car_aer, q_car_ana, q_ace_aer, q_o2_car, q_o2_ace, p_ace_aer, p_ace_ana;
+    double diff_colony, diff_agar;
+    double diff_colony_carbon, diff_agar_carbon;
+    double diff_colony_o2, diff_agar_o2;
+    double diff_colony_ace, diff_agar_ace;
+    double max_carbon, max_o2, max_o2_agar;
+    double max_growth_rate1, max_growth_rate2;
+    double max_gr_car_aer, max_gr_car_ana, max_gr_ace_aer;
+    double cdt;
+    double q_car_aer_nt, q_car_ana_nt, q_ace_aer_nt, q_o2_car_nt, q_o2_ace_nt, p_ace_ana_nt;
+    double kw_ph, ka_ph, kb_ph, cb_ph, c1_ph;     /* Kw, Ka, Kb, Cb, c1 */
+    int32_t cross_feeding;          /* only 0 is defined for the oxygen/acetate model */
+    int32_t interface_condition;    /* only 1 is implemented by the reference */
+    int32_t nutrient_gsi;           /* 0 = Jacobi with buffer swap */
+
+    /* schedule (reference constants as defaults) */
+    int32_t mg_levels;              /* 8, Simulation.cpp:157 */
+    int32_t mg_vcycles;             /* 3, Multigrid.cpp:869 */
+    int32_t mg_mu1;                 /* 3, Multigrid.cpp:1002 */
+    int32_t mg_mu2;                 /* 100, Multigrid.cpp:1002 */
+    int32_t sweeps_per_solve;       /* 200, Multigrid.cpp:1017 */
+    int32_t solves_per_update;      /* <=0: int(3600*UpdateTime*740/mg_dt), Multigrid.cpp:996 */
+    double  mg_dt;                  /* 100, Multigrid.cpp:995 */
+} bcg_params;
+
+/* Fill *p with the reference defaults (Constants.cpp:1-112). */
+int bcg_params_default(bcg_params* p);
+/* Derive box_length, max_cells_per_box (CellMD3D.cpp:52-54) and the device
+ * neighbour capacity; validate the combination.  Must be called after any
+ * change and before bcg_create. */
+int bcg_params_finalize(bcg_params* p);
+
+/* ------------------------------------------------------------------ */
+/* context                                                              */
+/* ------------------------------------------------------------------ */
+typedef struct bcg_ctx bcg_ctx;
+
+/* Allocate all device state for p on the current CUDA device.  Replaces
+ * the allocations of CellMD3D.cpp:46-142 and the Multigrid constructor
+ * (Multigrid.cpp:5-33); fields start at the LocalEnv/LocalAga defaults
+ * (Nutrients.h:13-38, 68-74). */
+int bcg_create(const bcg_params* p, bcg_ctx** out);
+int bcg_destroy(bcg_ctx* ctx);
+/* Last device error word (0 if none) and a static message for a status. */
+const char* bcg_status_string(int status);
+/* The CUDA stream all work of this context is queued on (cudaStream_t). */
+void* bcg_stream(bcg_ctx* ctx);
+/* Block until all queued work of ctx is done; returns the first pending error. */
+int bcg_synchronize(bcg_ctx* ctx);
+
+/* ------------------------------------------------------------------ */
+/* cells                                                                */
+/* ------------------------------------------------------------------ */
+/* Replace the colony with n cells (AoS records, host memory); replaces
+ * LoadCells' copy + Grid.Add (InputOutput.cpp:394-431). */
+int bcg_upload_cells(bcg_ctx* ctx, const bcg_cell* cells, int n);
+/* Copy the colony back as AoS records; *n receives the cell count. */
+int bcg_download_cells(bcg_ctx* ctx, bcg_cell* cells, int capacity, int* n);
+int bcg_num_cells(bcg_ctx* ctx, int* n);
+
+/* ------------------------------------------------------------------ */
+/* neighbours (Neighbours.cpp:24-93, UniformGrid.h:87-170)              */
+/* ------------------------------------------------------------------ */
+/* Full rebuild: bin every cell by UniformGrid::GetAddress (counting sort),
+ * gather the 3x3x3 box stencil and apply reduceNeighbours.  Replaces
+ * getNeighbours(cells, N, Grid, NeighbourList, maxNeighbours),
+ * Neighbours.cpp:24-37, as called at Simulation.cpp:292. */
+int bcg_rebuild_neighbours(bcg_ctx* ctx);
+/* Copy the reduced neighbour lists to the host: counts[N] and
+ * lists[N*stride] (row i holds counts[i] ids, in device order). */
+int bcg_get_neighbours(bcg_ctx* ctx, int* counts, int* lists, int stride);
+/* Set the lists from the host (same layout); used to restore a state. */
+int bcg_set_neighbours(bcg_ctx* ctx, const int* counts, const int* lists, int stride);
+
+/* ------------------------------------------------------------------ */
+/* mechanics step                                                       */
+/* ------------------------------------------------------------------ */
+/* One pass of MoveCell + GrowCell over every cell (Simulation.cpp:330-336,
+ * Cells.cpp:14-57, Integrate.cpp:11-127, Forces.cpp:13-381, grow.cpp:17-102):
+ * two-stage inertial integration with forces from the current (stale)
+ * neighbour lists, then growth from Environment.GrowthRate1.
+ * Outputs: *n_div = cells with Length >= Ldiv (their ids are kept on the
+ * device in ascending order, the 1-thread reference order), *fcw_calls =
+ * number of F_cw evaluations, i.e. the rand() calls Forces.cpp:102 made. */
+int bcg_move_grow(bcg_ctx* ctx, double dt, int* n_div, int64_t* fcw_calls);
+/* Ids of the cells flagged by the last bcg_move_grow, ascending. */
+int bcg_get_dividing(bcg_ctx* ctx, int* ids, int capacity);
+/* The division loop (Simulation.cpp:380-404) followed by the buffer swap
+ * (:408-413).  draws holds 9 floats per division, in call order, each equal
+ * to (float)rand()/RAND_MAX as drawn by divide() (grow.cpp:109-152).
+ * n_draw_sets must equal the n_div of the preceding bcg_move_grow.  Each
+ * division applies divide() and the partial neighbour rebuild for
+ * {mother, mother's neighbours, daughter} in ascending parent order.
+ * lineage (optional, 2 ints per division) receives "parent daughter" pairs
+ * as written at Simulation.cpp:392; *n_done receives the divisions done
+ * (fewer than requested when MaxCells is reached). */
+int bcg_divide(bcg_ctx* ctx, const float* draws, int n_draw_sets, double t,
+               int* n_done, int* lineage);
+
+/* ------------------------------------------------------------------ */
+/* fields                                                               */
+/* ------------------------------------------------------------------ */
+typedef enum bcg_field_id {
+    BCG_F_HEIGHT = 0,        /* Height (box_x*rGH)                         */
+    BCG_F_NORMAL_X = 1,      /* Normal.x (box_x*rGH)                       */
+    BCG_F_NORMAL_Z = 2,      /* Normal.z (box_x*rGH)                       */
+    BCG_F_WALL = 3,          /* rough wall height (box_x), Simulation.cpp:161-168 */
+    BCG_F_DENSITY_SHIFT = 4, /* DensityShiftP (box_x*box_z)                */
+    BCG_F_WALL_DENSITY_SHIFT = 5, /* WallDensityShiftP (box_x)             */
+    BCG_F_INSIDE = 6,        /* insideColonyDen (box_x*box_z)              */
+    BCG_F_ENV_CARBON = 7,    /* Environment (current buffer), box_x*box_z  */
+    BCG_F_ENV_WASTE = 8,
+    BCG_F_ENV_OXYGEN = 9,
+    BCG_F_ENV_ACETATE = 10,
+    BCG_F_ENV_GROWTH1 = 11,
+    BCG_F_ENV_GROWTH2 = 12,
+    BCG_F_ENV_PH = 13,
+    BCG_F_OLDENV_CARBON = 14, /* oldEnvironment buffer                     */
+    BCG_F_OLDENV_WASTE = 15,
+    BCG_F_OLDENV_OXYGEN = 16,
+    BCG_F_OLDENV_ACETATE = 17,
+    BCG_F_WALLF_CARBON = 18, /* FieldWall[level] (box_x), level in `level` */
+    BCG_F_WALLF_WASTE = 19,
+    BCG_F_WALLF_OXYGEN = 20,
+    BCG_F_WALLF_ACETATE = 21,
+    BCG_F_OLDWALLF_CARBON = 22, /* oldFieldWall[level]                     */
+    BCG_F_OLDWALLF_WASTE = 23,
+    BCG_F_OLDWALLF_OXYGEN = 24,
+    BCG_F_OLDWALLF_ACETATE = 25,
+    BCG_F_AGARF_CARBON = 26, /* FieldAgar[level] (box_x*box_z_agar)        */
+    BCG_F_AGARF_OXYGEN = 27,
+    BCG_F_AGARF_ACETATE = 28,
+    BCG_F_MG_SOL_CARBON = 29, /* Multigrid::Aga[level] ((nx+1)*(nz+1))     */
+    BCG_F_MG_SOL_OXYGEN = 30,
+    BCG_F_MG_SOL_ACETATE = 31,
+    BCG_F_MG_RES_CARBON = 32, /* Multigrid::AgaRes[level]                  */
+    BCG_F_MG_RES_OXYGEN = 33,
+    BCG_F_MG_RES_ACETATE = 34,
+    BCG_F_MG_ERR_CARBON = 35, /* Multigrid::AgaErr[level]                  */
+    BCG_F_MG_ERR_OXYGEN = 36,
+    BCG_F_MG_ERR_ACETATE = 37,
+    BCG_F_DENSITY = 38,       /* Density (BoxAverage of RoughDensity)      */
+    BCG_F_ROUGH_DENSITY = 39, /* RoughDensity (GetDensity)                 */
+    BCG_F_COUNT = 40
+} bcg_field_id;
+
+/* Number of doubles of a field at a level (x-major, z fastest, matching
+ * Array2D/Array3D indexing x*(Y*Z)+y*Z+z with Y=1). */
+int bcg_field_size(bcg_ctx* ctx, int field, int level, size_t* n);
+int bcg_get_field(bcg_ctx* ctx, int field, int level, double* out, size_t n);
+int bcg_set_field(bcg_ctx* ctx, int field, int level, const double* in, size_t n);
+/* Bounding box used by the field chain: minx, maxx, maxz after the +-5
+ * widening of Compute.cpp:250-252 (written by the deposition calls). */
+int bcg_get_bbox(bcg_ctx* ctx, int* minx, int* maxx, int* maxz);
+
+/* GetDensity + ShiftDensity + 6x BoxAverage + Height_Average + Smooth +
+ * GetSurfaceNormal (Simulation.cpp:266-280; Compute.cpp:120-253, 344-605,
+ * 669-738, 466-491). */
+int bcg_update_density(bcg_ctx* ctx);
+/* GetHeight + Height_Average + Smooth + GetSurfaceNormal (Simulation.cpp:
+ * 302-306; Compute.cpp:256-340). */
+int bcg_update_height(bcg_ctx* ctx);
+/* The initial-condition variant of the deposition chain at
+ * Simulation.cpp:186-210 (no height smoothing). */
+int bcg_initial_density(bcg_ctx* ctx);
+
+/* UpdateEnvArrayMG_OxygenAcetate (Multigrid.cpp:984-1125): n solves, each
+ * one Multigrid::solve followed by `sweeps` colony/interface Jacobi sweeps.
+ * n <= 0 selects params.solves_per_update; sweeps < 0 selects
+ * params.sweeps_per_solve. */
+int bcg_nutrient_update(bcg_ctx* ctx, int n, int sweeps);
+/* One Multigrid::solve (Multigrid.cpp:864-889) with `vcycles` V-cycles
+ * (<=0: params.mg_vcycles): copyToMG, setup, V-cycles, reset, copyFromMG. */
+int bcg_mg_solve(bcg_ctx* ctx, int vcycles);
+/* `sweeps` colony/interface sweeps (the inner loop of Multigrid.cpp:
+ * 1017-1120) starting at sweep parity `count0`. */
+int bcg_colony_sweeps(bcg_ctx* ctx, int sweeps, int count0);
+
+/* ------------------------------------------------------------------ */
+/* mixed precision multigrid (FP32 smoothing/restriction/prolongation in */
+/* an FP64 iterative-refinement loop); no reference counterpart.         */
+/* ------------------------------------------------------------------ */
+/* Solve the backward-Euler agar step (the system Multigrid::solve
+ * iterates on) until the FP64 residual max-norm falls below
+ * rel_tol * (max-norm of the right-hand side), with V-cycles on the inner
+ * correction run in precision `precision` (32 or 64).  *iters receives the
+ * outer iterations used and *rel_res the final relative residual. */
+int bcg_mg_solve_tol(bcg_ctx* ctx, double rel_tol, int precision, int max_iters,
+                     int* iters, double* rel_res);
+
+/* ------------------------------------------------------------------ */
+/* timing: device time of the kernels queued by the last call of each    */
+/* kind (CUDA events on the context stream), in milliseconds.            */
+/* ------------------------------------------------------------------ */
+typedef enum bcg_timer_id {
+    BCG_T_MOVE_GROW = 0, BCG_T_DIVIDE = 1, BCG_T_NEIGHBOURS = 2,
+    BCG_T_MG_SOLVE = 3, BCG_T_SWEEPS = 4, BCG_T_DENSITY = 5, BCG_T_COUNT = 6
+} bcg_timer_id;
+int bcg_enable_timers(bcg_ctx* ctx, int on);
+int bcg_get_timer(bcg_ctx* ctx, int timer, double* ms, int64_t* launches);
+
+/* ------------------------------------------------------------------ */
+/* host helpers                                                         */
+/* ------------------------------------------------------------------ */
+/* glibc-compatible rand() stream owned by the host (the reference seeds
+ * the process-wide rand() with srand, CellMD3D.cpp:23).  Implemented from
+ * the published TYPE_3 additive-feedback description; bcg_rng_skip uses a
+ * polynomial jump-ahead so skipping the F_cw draws costs O(31^2 log k). */
+typedef struct bcg_rng { uint32_t r[34]; int32_t pos; } bcg_rng;
+void    bcg_rng_seed(bcg_rng* g, uint32_t seed);
+int32_t bcg_rng_next(bcg_rng* g);
+void    bcg_rng_skip(bcg_rng* g, int64_t k);
+
+/* Seeded synthetic colony (2-D x-z half-ellipse dome on the agar,
+ * random sequential placement, no overlaps); see the generator notes in
+ * the design document.  Returns the cell count in *n.  width/height in um. */
+int bcg_synth_colony(uint64_t seed, int n_target, double width, double height,
+                     double radius, double len_lo, double len_hi,
+                     double l_divide, double div_phase_spread,
+                     bcg_cell* out, int capacity, int* n);
+
+/* ------------------------------------------------------------------ */
+/* C++ host loop (rewrite of SimSingleThread, Simulation.cpp:42-434)     */
+/* ------------------------------------------------------------------ */
+typedef struct bcg_sim bcg_sim;
+/* Build a simulation from params and n cells; seeds the host rand() stream
+ * with `seed`, draws the rough wall (Simulation.cpp:161-168) and runs the
+ * initial field block (Simulation.cpp:185-217) if run_initial_fields. */
+int bcg_sim_create(const bcg_params* p, const bcg_cell* cells, int n, uint32_t seed,
+                   int run_initial_fields, bcg_sim** out);
+int bcg_sim_destroy(bcg_sim* sim);
+/* Advance `steps` iterations of the while loop (Simulation.cpp:254-431),
+ * honouring UpdateFlag / HeightDensityUpdateFlag; output steps are skipped
+ * (OutFlag handling stays with the caller). */
+int bcg_sim_run(bcg_sim* sim, int steps);
+bcg_ctx* bcg_sim_ctx(bcg_sim* sim);
+int bcg_sim_time(bcg_sim* sim, double* t, int* n_cells, int64_t* divisions);
+/* Lineage pairs recorded so far (parent, daughter), up to capacity pairs. */
+int bcg_sim_lineage(bcg_sim* sim, int* pairs, int capacity, int* n);
+/* Per-step mode used by benchmarks: each step runs the mechanics step and
+ * `vcycles` V-cycles of the agar solve instead of the reference's field
+ * cadence (0 = mechanics only). */
+int bcg_sim_set_step_mode(bcg_sim* sim, int field_cadence_reference, int vcycles_per_step);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BCG_H_ */
