@@ -26,7 +26,7 @@ def synth_colony(n, width, height, seed=20261203, radius=0.5, len_lo=2.0, len_hi
     return out[:got.value]
 
 
-def workload_colony(name, seed=None, phi=0.4, div_phase_spread=1.0, n=None):
+def workload_colony(name, seed=None, phi=0.45, div_phase_spread=1.0, n=None):
     """Cells of a named workload (params.WORKLOADS)."""
     cells, aspect, *_ = _params.WORKLOADS[name]
     n = n or cells

@@ -146,8 +146,10 @@ __device__ __forceinline__ V3 wall_locus(const Cst& c, V3 cm, V3 pole, double wa
 
 /* Array2D<double>::linear_interp at y = 0 with float weights (Array.h:282-288).
  * The two y+1 terms carry weight exactly 0 and are omitted. */
-__device__ __forceinline__ double height_interp(const double* __restrict__ h, int x0, double dx)
+__device__ __forceinline__ double height_interp(const double* __restrict__ h, int x0, double dx, int xh)
 {
+    /* a cell outside the grid is reported by the binning; keep reads in bounds */
+    x0 = x0 < 0 ? 0 : (x0 > xh - 2 ? xh - 2 : x0);
     float x = dx < 0 ? 1 + dx : dx;
     float y = 0.0f;
     return h[x0] * (1 - x) * (1 - y) + h[x0 + 1] * x * (1 - y);
@@ -163,16 +165,17 @@ __device__ __forceinline__ void surface_tension(const Cst& c, V3 cm, const Field
     int i_ht = (int)(c.p.x / hb + half);
     double dxp = c.p.x / hb - (i_ht - half + 0.5);
     i_ht = (int)ceil(dxp) + i_ht - 1;
-    double height_p = height_interp(fp.height, i_ht, dxp);
+    double height_p = height_interp(fp.height, i_ht, dxp, mp.xh);
     i_ht = (int)(c.q.x / hb + half);
     double dxq = c.q.x / hb - (i_ht - half + 0.5);
     i_ht = (int)ceil(dxq) + i_ht - 1;
-    double height_q = height_interp(fp.height, i_ht, dxq);
+    double height_q = height_interp(fp.height, i_ht, dxq, mp.xh);
     i_ht = (int)(cm.x / hb + half);
     double dxc = cm.x / hb - (i_ht - half + 0.5);
     i_ht = (int)ceil(dxc) + i_ht - 1;
-    double height_cm = height_interp(fp.height, i_ht, dxc);
+    double height_cm = height_interp(fp.height, i_ht, dxc, mp.xh);
     if (height_cm > (cm.z + mp.box_length)) { F = mk(0, 0, 0); T = mk(0, 0, 0); return; }
+    xa = xa < 0 ? 0 : (xa > mp.xh - 1 ? mp.xh - 1 : xa);
     V3 N = mk(fp.nx[xa], fp.ny[xa], fp.nz[xa]);
     V3 F1 = mk(0, 0, 0), F2 = mk(0, 0, 0);
     double dh = c.p.z - (height_p - mp.delta_h / N.z);

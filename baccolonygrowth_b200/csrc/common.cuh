@@ -37,6 +37,7 @@ struct DevStatus {
 /* Parameters the kernels read, copied by value into each launch. */
 struct MechParams {
     int box_x, box_y, box_z, rgh;
+    int xh;             /* Height/Normal length, box_x*rgh */
     int kmax, box_cap;
     double box_length, rc, cell_radius, l_divide;
     double k_cc, k_wc, var_l, var_angle, var_pos, viscosity, gamma_t, cell_mu, wall_mu;

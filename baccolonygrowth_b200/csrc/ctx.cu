@@ -34,6 +34,7 @@ MechParams mech_params(const bcg_ctx* c)
     MechParams m;
     const bcg_params& P = c->P;
     m.box_x = P.box_x; m.box_y = P.box_y; m.box_z = P.box_z; m.rgh = P.refinement_grid_height;
+    m.xh = P.box_x * P.refinement_grid_height;
     m.kmax = c->kmax; m.box_cap = P.max_cells_per_box;
     m.box_length = P.box_length; m.rc = P.rc; m.cell_radius = P.cell_radius; m.l_divide = P.l_divide;
     m.k_cc = P.k_cc; m.k_wc = P.k_wc; m.var_l = P.var_l; m.var_angle = P.var_angle; m.var_pos = P.var_pos;

@@ -1,0 +1,519 @@
+/*
+ * mg.cu -- the composite-grid agar multigrid (class Multigrid,
+ * AgentBasedModel-BacColonyGrowth/Multigrid.cpp:5-981) on the device.
+ *
+ * Each level holds Sol/Res/Err for carbon (0), oxygen (1), acetate (2),
+ * (nx+1) x (nz+1) points, row k contiguous in i with a padded pitch.
+ * Composite levels l < agarLevels are full size and each covers twice the
+ * extent of the previous one at half the resolution; levels >= agarLevels
+ * are plain coarsenings.  The smoother is the reference's zebra-column
+ * Gauss-Seidel: all even columns, then all odd columns, each column swept
+ * bottom to top in place (one thread per column and species).
+ */
+#include "ctx.cuh"
+#include "mg.cuh"
+
+__device__ __forceinline__ double dmaxd(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmind(double a, double b) { return a < b ? a : b; }
+
+#define AT(arr, L, i, k) (arr)[(size_t)(k) * (L).pitch + (i)]
+
+MgConst mg_const(const bcg_ctx* c, double dt)
+{
+    MgConst m;
+    const bcg_params& P = c->P;
+    m.A = P.max_levels_mg; m.levels = c->mg_levels; m.box_x = P.box_x; m.box_z_agar = P.box_z_agar;
+    m.bl2 = P.box_length * P.box_length;
+    m.dt = dt;
+    m.D[0] = P.diff_agar_carbon; m.D[1] = P.diff_agar_o2; m.D[2] = P.diff_agar_ace;
+    m.max_carbon = P.max_carbon; m.max_o2_agar = P.max_o2_agar;
+    m.box_z = P.box_z;
+    return m;
+}
+
+MgLvl mg_lvl(const bcg_ctx* c, int l)
+{
+    MgLvl v;
+    const MgLevel& L = c->mg[l];
+    v.nx = L.nx; v.nz = L.nz; v.pitch = L.pitch;
+    for (int s = 0; s < 3; s++) { v.s[s] = L.sol[s]; v.r[s] = L.res[s]; v.e[s] = L.err[s]; }
+    return v;
+}
+
+/* ------------------------------------------------------------------------ */
+/* relaxationAgarElementwise, Multigrid.cpp:160-249, for one species        */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ void relax_point(const MgConst& m, const MgLvl& L, int l, int sp, int i, int k,
+                                            const double* __restrict__ inside0, double& e_below, bool have_below)
+{
+    const int nx = L.nx, nz = L.nz;
+    const double h2 = m.bl2 * (double)(1 << (2 * l));
+    const double dt = m.dt, D = m.D[sp];
+    double* E = L.e[sp];
+    const double* R = L.r[sp];
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    double r = AT(R, L, i, k);
+    double e_dn = have_below ? e_below : (k > 0 ? AT(E, L, i, k - 1) : 0.0);
+    double out;
+    bool write = true;
+    if (k == 0) {
+        int d = 1 << l;
+        int i0 = (i - nx / 2) * d + m.box_x / 2;
+        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+        if (inside0[(size_t)i0 * m.box_z] > 0) out = r;
+        else if (i == 0 || i == nx) {
+            if (top_levels) {
+                if (oxy) out = r;
+                else {
+                    double s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
+                    double up = AT(E, L, i, 1);
+                    out = (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
+                }
+            } else write = false;
+        } else {
+            if (oxy) out = r;
+            else {
+                double up = AT(E, L, i, 1), xm = AT(E, L, i - 1, 0), xp = AT(E, L, i + 1, 0);
+                out = (r * h2 / dt / D + up + 0.5 * xm + 0.5 * xp) / (h2 / dt / D + 2);
+            }
+        }
+    } else if (k == nz) {
+        if (top_levels) {
+            if (i == 0 || i == nx) {
+                if (oxy) out = r;
+                else {
+                    double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                    out = (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
+                }
+            } else {
+                double xp = AT(E, L, i + 1, k), xm = AT(E, L, i - 1, k);
+                out = (r * h2 / dt / D + e_dn + 0.5 * xp + 0.5 * xm) / (h2 / dt / D + 2);
+            }
+        } else write = false;
+    } else if (i == 0 || i == nx) {
+        if (top_levels) {
+            if (oxy) out = r;
+            else {
+                double up = AT(E, L, i, k + 1);
+                double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + s1) / (h2 / dt / D + 2);
+            }
+        } else write = false;
+    } else {
+        double up = AT(E, L, i, k + 1), xm = AT(E, L, i - 1, k), xp = AT(E, L, i + 1, k);
+        out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + 0.5 * xm + 0.5 * xp) / (h2 / dt / D + 2);
+    }
+    if (write) AT(E, L, i, k) = out;
+    e_below = write ? out : AT(E, L, i, k);
+}
+
+/* one thread per (column of the given parity, species), bottom to top */
+__global__ void k_mg_relax(MgConst m, MgLvl L, int l, int parity, const double* __restrict__ inside0)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int ncol = (L.nx + 1 - parity + 1) / 2;
+    int sp = blockIdx.y;
+    if (t >= ncol) return;
+    int i = 2 * t + parity;
+    double below = 0.0;
+    for (int k = 0; k <= L.nz; k++) relax_point(m, L, l, sp, i, k, inside0, below, k > 0);
+}
+
+/* ------------------------------------------------------------------------ */
+/* restrictionAgaElementwise, Multigrid.cpp:269-405 (level l from l-1)       */
+/* ------------------------------------------------------------------------ */
+__global__ void k_mg_restrict(MgConst m, MgLvl Lc, MgLvl Lf, int l, const double* __restrict__ inside0)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    const int nx = Lc.nx, nz = Lc.nz;
+    if (idx >= (nx + 1) * (nz + 1)) return;
+    int i = idx % (nx + 1), k = idx / (nx + 1);
+    const int X = m.box_x, ZA = m.box_z_agar;
+    int d = 1 << l, d0 = 1 << m.A;
+    int nxp = X * d0 / d < X ? X * d0 / d : X;
+    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    double h2 = m.bl2 * d * d;
+    const double dt = m.dt, D = m.D[sp];
+    const bool oxy = sp == 1;
+    int i0 = (i - nx / 2) * d + X / 2;
+    i0 = i0 < 0 ? 0 : (i0 > X ? X : i0);
+    int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
+    const double* EP = Lf.e[sp];
+    const double* RP = Lf.r[sp];
+    const double* AP = Lf.s[sp];
+    const double* AL = Lc.s[sp];
+    double* R = &AT(Lc.r[sp], Lc, i, k);
+#define EPv(a, b) AT(EP, Lf, a, b)
+#define RPv(a, b) AT(RP, Lf, a, b)
+#define APv(a, b) AT(AP, Lf, a, b)
+#define ALv(a, b) AT(AL, Lc, a, b)
+    if (i == 0 || i == nx || k == nz) {
+        if (l >= m.A) {
+            if (k == nz && (i > 0) && (i < nx)) {
+                /* carbon uses (ip,kp), oxygen/acetate (2i,2k): equal for l >= A */
+                *R = (RPv(ip, kp) + 0.5 * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + 2 * EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+            } else {
+                int sx = (i == 0) ? 1 : -1;
+                if (oxy) *R = RPv(ip, kp) - EPv(ip, kp);
+                else if (k == 0)
+                    *R = (RPv(ip, kp) + 0.5 * (2 * EPv(ip + sx, kp) + 2 * EPv(ip, kp + 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+                else if (k == nz)
+                    *R = (RPv(ip, kp) + 0.5 * (2 * EPv(ip + sx, kp) + 2 * EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+                else
+                    *R = (RPv(ip, kp) + 0.5 * (2 * EPv(ip + sx, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+            }
+        }
+    } else if (k == 0) {
+        if (inside0[(size_t)i0 * m.box_z] > 0) *R = 0;
+        else if (ip > 0 && ip < nxp) {
+            if (oxy) *R = (RPv(ip, 0) - EPv(ip, 0)) * 0.5;
+            else *R = (RPv(ip, 0) + 0.5 * (EPv(ip + 1, 0) + EPv(ip - 1, 0) + 2 * EPv(ip, 1) - 4 * EPv(ip, 0)) * D * dt * 4 / h2 - EPv(ip, 0)) * 0.5;
+        } else if ((l < m.A) && (ip >= 0 && ip <= nxp) && ((ip == 0) || (ip == nxp))) {
+            if (oxy) *R = m.max_o2_agar - ALv(i, 0);
+            else if (ip == 0) *R = (APv(ip + 2, 0) + 0.5 * EPv(ip + 2, 0) + ALv(i - 1, 0) + 2 * ALv(i, 1) - 4 * ALv(i, 0)) * D * dt / h2;
+            else *R = (ALv(i + 1, 0) + 0.5 * EPv(ip - 2, 0) + APv(ip - 2, 0) + 2 * ALv(i, 1) - 4 * ALv(i, 0)) * dt * D / h2;
+        }
+    } else if (l < m.A && ip >= 0 && ip <= nxp && kp <= nzp) {
+        if (kp == nzp) {
+            if (ip == 0 || ip == nxp)
+                *R = (ALv(i + 1, k) + ALv(i - 1, k) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
+            else
+                *R = (ALv(i + 1, k) + ALv(i - 1, k) + ALv(i, k + 1) + APv(ip, kp - 2) + 0.5 * EPv(ip, kp - 2) - 4 * ALv(i, k)) * D * dt / h2;
+        } else if (ip == 0) {
+            *R = (APv(ip + 2, kp) + 0.5 * EPv(ip + 2, kp) + ALv(i - 1, k) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
+        } else if (ip == nxp) {
+            *R = (ALv(i + 1, k) + 0.5 * EPv(ip - 2, kp) + APv(ip - 2, kp) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
+        } else {
+            *R = (RPv(ip, kp) + 0.5 * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt / h2 * 4 - EPv(ip, kp)) * 0.5;
+        }
+    } else if (l >= m.A) {
+        *R = (RPv(ip, kp) + 0.5 * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt / h2 * 4 - EPv(ip, kp)) * 0.5;
+    }
+#undef EPv
+#undef RPv
+#undef APv
+#undef ALv
+}
+
+/* interpolationAga, Multigrid.cpp:407-467 (Err of level l += from l+1) */
+__global__ void k_mg_interp(MgConst m, MgLvl Lf, MgLvl Lc, int l)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    const int nx = Lf.nx, nz = Lf.nz;
+    if (idx >= (nx + 1) * (nz + 1)) return;
+    int i = idx % (nx + 1), k = idx / (nx + 1);
+    const int X = m.box_x;
+    int d = 1 << l, d0 = 1 << m.A;
+    int nxp = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
+    const double* C = Lc.e[sp];
+    double& e = AT(Lf.e[sp], Lf, i, k);
+    if (i % 2 == 0) {
+        int ip = nxp / 2 - nx / 4 + i / 2;
+        if (k % 2 == 0) e += AT(C, Lc, ip, k / 2);
+        else { int kp = (k - 1) / 2; e += 0.5 * (AT(C, Lc, ip, kp) + AT(C, Lc, ip, kp + 1)); }
+    } else {
+        int ip = nxp / 2 - nx / 4 + (i - 1) / 2;
+        if (k % 2 == 0) { int kp = k / 2; e += 0.5 * (AT(C, Lc, ip, kp) + AT(C, Lc, ip + 1, kp)); }
+        else {
+            int kp = (k - 1) / 2;
+            e += 0.25 * (AT(C, Lc, ip, kp) + AT(C, Lc, ip, kp + 1) + AT(C, Lc, ip + 1, kp) + AT(C, Lc, ip + 1, kp + 1));
+        }
+    }
+}
+
+/* resetZero, Multigrid.cpp:47-82 */
+__global__ void k_mg_reset_zero(MgLvl L, int zero_res)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    if (idx >= (L.nx + 1) * (L.nz + 1)) return;
+    int i = idx % (L.nx + 1), k = idx / (L.nx + 1);
+    AT(L.e[sp], L, i, k) = 0;
+    if (zero_res) AT(L.r[sp], L, i, k) = 0;
+}
+
+/* updateSolAgaElementwise, Multigrid.cpp:544-568 */
+__global__ void k_mg_update_sol(MgConst m, MgLvl L, int l)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    const int nx = L.nx, nz = L.nz;
+    if (idx >= (nx + 1) * (nz + 1)) return;
+    int i = idx % (nx + 1), k = idx / (nx + 1);
+    const int X = m.box_x, ZA = m.box_z_agar;
+    int d = 1 << l, d0 = 1 << m.A;
+    int nxp = X * d0 / d < X ? X * d0 / d : X;
+    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    AT(L.r[sp], L, i, k) = 0;
+    int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
+    double& e = AT(L.e[sp], L, i, k);
+    if (l < m.A && (l == 0 || ip <= 0 || ip >= nxp || kp >= nzp)) {
+        double& a = AT(L.s[sp], L, i, k);
+        a += e;
+        if (sp == 0) a = dmaxd(dmind(a, m.max_carbon), 0.0);
+        else if (sp == 1) a = dmaxd(dmind(a, m.max_o2_agar), 0.0);
+        else a = dmaxd(a, 0.0);
+    }
+    e = 0;
+}
+
+/* updateResAgaElementwise, Multigrid.cpp:570-701 */
+__global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const double* __restrict__ inside0)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    const int nx = L.nx, nz = L.nz;
+    if (idx >= (nx + 1) * (nz + 1) || l >= m.A) return;
+    int i = idx % (nx + 1), k = idx / (nx + 1);
+    const int X = m.box_x, ZA = m.box_z_agar;
+    int d = 1 << l, d0 = 1 << m.A;
+    int nxp = X * d0 / d < X ? X * d0 / d : X;
+    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    double h2 = m.bl2 * d * d;
+    const double dt = m.dt, D = m.D[sp];
+    const bool oxy = sp == 1;
+    int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
+    const double* A = L.s[sp];
+    double* R = &AT(L.r[sp], L, i, k);
+#define AL(a, b) AT(A, L, a, b)
+#define APv(a, b) AT(Lp.s[sp], Lp, a, b)
+    if (i == 0 || i == nx) {
+        if (l == m.A - 1) {
+            int sx = (i == 0) ? 1 : -1;
+            if (oxy) *R = 0;
+            else if (k == 0) *R = (2 * AL(i + sx, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
+            else if (k == nz) *R = (2 * AL(i + sx, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D * dt / h2;
+            else *R = (2 * AL(i + sx, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
+        }
+    } else if (k == nz) {
+        if (l == m.A - 1) {
+            /* oxygen omits dt here, as the reference does (Multigrid.cpp:634) */
+            if (oxy) *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D / h2;
+            else *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * dt * D / h2;
+        }
+    } else if (k == 0) {
+        if (l == 0) {
+            if (inside0[(size_t)i * m.box_z] > 0) *R = 0;
+            else if (oxy) *R = m.max_o2_agar - AL(i, k);
+            else *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+        } else if ((ip > 0 && ip < nxp) != 1) {
+            if (oxy) *R = m.max_o2_agar - AL(i, k);
+            else if (ip == 0) *R = (APv(ip + 2, kp) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else if (ip == nxp) *R = (APv(ip - 2, kp) + AL(i + 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+        }
+    } else {
+        if (l > 0) {
+            if (kp == nzp && ip > 0 && ip < nxp)
+                *R = (AL(i + 1, k) + AL(i - 1, k) + APv(ip, kp - 2) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else if (ip == 0 && kp < nzp)
+                *R = (APv(ip + 2, kp) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else if (ip == nxp && kp < nzp)
+                *R = (AL(i + 1, k) + APv(ip - 2, kp) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else if (ip <= 0 || ip >= nxp || kp >= nzp)
+                *R = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+        } else {
+            *R = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+        }
+    }
+#undef AL
+#undef APv
+}
+
+/* rewriteSolBdryAga, Multigrid.cpp:469-503 (top row, then the side columns) */
+__global__ void k_mg_rewrite_bdry(MgConst m, MgLvl L, MgLvl Lc, int l)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    const int X = m.box_x;
+    int d = 1 << l, d0 = 1 << m.A;
+    const int nx = L.nx, nz = L.nz;
+    int nx2 = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
+    const double* C = Lc.s[sp];
+    if (t < nx + 1) {
+        int i = t, k2 = nz / 2;
+        int i2 = nx2 / 2 + i / 2 - nx / 4, i2p1 = nx2 / 2 + (i + 1) / 2 - nx / 4;
+        AT(L.s[sp], L, i, nz) = (AT(C, Lc, i2, k2) + AT(C, Lc, i2p1, k2)) / 2;
+    } else if (t < nx + 1 + 2 * nz) {
+        int u = t - (nx + 1);
+        int k = u >> 1, side = u & 1;
+        int i = side ? nx : 0;
+        int i2 = nx2 / 2 + i / 2 - nx / 4;
+        AT(L.s[sp], L, i, k) = (AT(C, Lc, i2, k / 2) + AT(C, Lc, i2, (k + 1) / 2)) / 2;
+    }
+}
+
+/* NestSolAgaElementwise, Multigrid.cpp:724-737 */
+__global__ void k_mg_nest(MgConst m, MgLvl L, MgLvl Lf, int l)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    const int nx = L.nx, nz = L.nz;
+    if (idx >= (nx + 1) * (nz + 1)) return;
+    int i = idx % (nx + 1), k = idx / (nx + 1);
+    const int X = m.box_x, ZA = m.box_z_agar;
+    int d = 1 << l, d0 = 1 << m.A;
+    int nxp = X * d0 / d < X ? X * d0 / d : X;
+    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
+    if (ip > 0 && ip < nxp && kp < nzp) AT(L.s[sp], L, i, k) = AT(Lf.s[sp], Lf, ip, kp);
+}
+
+/* copyToMG, Multigrid.cpp:891-907: wall-under-colony values into level 0,
+ * then the periodic copy of column 0 into column BoxX on the last
+ * composite level */
+__global__ void k_mg_copy_to(MgConst m, MgLvl L0, const double* __restrict__ wC, const double* __restrict__ wO,
+                             const double* __restrict__ wA, const double* __restrict__ inside0)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 1 && i <= m.box_x - 1 && inside0[(size_t)i * m.box_z] > 0) {
+        AT(L0.s[0], L0, i, 0) = wC[i];
+        AT(L0.s[1], L0, i, 0) = wO[i];
+        AT(L0.s[2], L0, i, 0) = wA[i];
+    }
+}
+__global__ void k_mg_copy_edge(MgLvl L)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    if (k > L.nz) return;
+    AT(L.s[sp], L, L.nx, k) = AT(L.s[sp], L, 0, k);
+}
+/* copyFromMG, Multigrid.cpp:958-981: wall rows of both buffers (the agar
+ * field is read straight from the solution rows 1..BoxZAgar) */
+__global__ void k_mg_copy_from(MgLvl L, int X, double* cC, double* cO, double* cA, double* pC, double* pO, double* pA)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= X) return;
+    double c = AT(L.s[0], L, i, 0), o = AT(L.s[1], L, i, 0), a = AT(L.s[2], L, i, 0);
+    cC[i] = c; cO[i] = o; cA[i] = a;
+    pC[i] = c; pO[i] = o; pA[i] = a;
+}
+
+/* ------------------------------------------------------------------------ */
+static inline dim3 grid2(int n, int threads) { return dim3((unsigned)((n + threads - 1) / threads), 3); }
+
+static void relax_level(bcg_ctx* c, const MgConst& m, int l)
+{
+    MgLvl L = mg_lvl(c, l);
+    for (int par = 0; par < 2; par++) {
+        int ncol = (L.nx + 1 - par + 1) / 2;
+        k_mg_relax<<<grid2(ncol, 64), 64, 0, c->stream>>>(m, L, l, par, c->inside);
+    }
+    c->launches += 2;
+}
+
+void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
+{
+    const int Lv = c->mg_levels;
+    for (int l = 0; l < Lv - 1; l++) {
+        for (int j = 0; j < mu1; j++) relax_level(c, m, l);
+        MgLvl Lc = mg_lvl(c, l + 1), Lf = mg_lvl(c, l);
+        k_mg_restrict<<<grid2((Lc.nx + 1) * (Lc.nz + 1), 256), 256, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
+        c->launches++;
+    }
+    for (int j = 0; j < mu2; j++) relax_level(c, m, Lv - 1);
+    for (int l = Lv - 2; l >= 0; l--) {
+        MgLvl Lf = mg_lvl(c, l), Lc = mg_lvl(c, l + 1);
+        k_mg_interp<<<grid2((Lf.nx + 1) * (Lf.nz + 1), 256), 256, 0, c->stream>>>(m, Lf, Lc, l);
+        c->launches++;
+        for (int j = 0; j < mu1; j++) relax_level(c, m, l);
+    }
+}
+
+static void reset_zero(bcg_ctx* c)
+{
+    for (int l = 0; l < c->mg_levels; l++) {
+        MgLvl L = mg_lvl(c, l);
+        k_mg_reset_zero<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(L, l > 0);
+        c->launches++;
+    }
+}
+static void update_sol(bcg_ctx* c, const MgConst& m, int l)
+{
+    MgLvl L = mg_lvl(c, l);
+    k_mg_update_sol<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, l);
+    c->launches++;
+}
+static void update_res(bcg_ctx* c, const MgConst& m, int l)
+{
+    MgLvl L = mg_lvl(c, l), Lp = mg_lvl(c, l > 0 ? l - 1 : 0);
+    k_mg_update_res<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    c->launches++;
+}
+
+/* setup(), Multigrid.cpp:818-825 */
+void mg_setup(bcg_ctx* c, const MgConst& m)
+{
+    reset_zero(c);
+    for (int l = 0; l <= m.A - 1; l++) update_sol(c, m, l);
+    for (int l = 0; l <= m.A - 1; l++) update_res(c, m, l);
+}
+
+/* reset(), Multigrid.cpp:827-841 (evalUpdateRes's result is discarded there) */
+void mg_reset(bcg_ctx* c, const MgConst& m)
+{
+    for (int l = 0; l <= m.A - 1; l++) update_sol(c, m, l);
+    for (int l = 0; l < m.A - 1; l++) {
+        MgLvl L = mg_lvl(c, l), Lc = mg_lvl(c, l + 1);
+        int n = L.nx + 1 + 2 * L.nz;
+        k_mg_rewrite_bdry<<<grid2(n, 256), 256, 0, c->stream>>>(m, L, Lc, l);
+        c->launches++;
+    }
+    for (int l = 0; l <= m.A - 1; l++) update_res(c, m, l);
+    reset_zero(c);
+    for (int l = 1; l < m.A; l++) {
+        MgLvl L = mg_lvl(c, l), Lf = mg_lvl(c, l - 1);
+        k_mg_nest<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lf, l);
+        c->launches++;
+    }
+}
+
+void mg_copy_to(bcg_ctx* c, const MgConst& m, int wall_buf)
+{
+    MgLvl L0 = mg_lvl(c, 0);
+    const WallBuf& w = c->wal[wall_buf];
+    k_mg_copy_to<<<(m.box_x + 255) / 256, 256, 0, c->stream>>>(m, L0, w.C[0], w.O[0], w.A[0], c->inside);
+    MgLvl La = mg_lvl(c, m.A - 1);
+    k_mg_copy_edge<<<grid2(La.nz + 1, 256), 256, 0, c->stream>>>(La);
+    c->launches += 2;
+}
+
+void mg_copy_from(bcg_ctx* c, const MgConst& m, int cur_wall)
+{
+    for (int l = 0; l < m.A; l++) {
+        MgLvl L = mg_lvl(c, l);
+        const WallBuf& cw = c->wal[cur_wall];
+        const WallBuf& pw = c->wal[cur_wall ^ 1];
+        k_mg_copy_from<<<(m.box_x + 255) / 256, 256, 0, c->stream>>>(L, m.box_x, cw.C[l], cw.O[l], cw.A[l], pw.C[l], pw.O[l], pw.A[l]);
+        c->launches++;
+    }
+}
+
+/* Multigrid::solve (Multigrid.cpp:864-889) with the given V-cycle count;
+ * `wall_buf` is the wall buffer the caller's loop currently calls current */
+int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf)
+{
+    MgConst m = mg_const(c, c->P.mg_dt);
+    mg_copy_to(c, m, wall_buf);
+    mg_setup(c, m);
+    for (int v = 0; v < vcycles; v++) mg_vcycle(c, m, c->P.mg_mu1, c->P.mg_mu2);
+    mg_reset(c, m);
+    mg_copy_from(c, m, wall_buf);
+    return cudaGetLastError() == cudaSuccess ? BCG_OK : BCG_E_CUDA;
+}
+
+extern "C" int bcg_mg_solve(bcg_ctx* c, int vcycles)
+{
+    if (!c) return BCG_E_ARG;
+    if (vcycles <= 0) vcycles = c->P.mg_vcycles;
+    timer_begin(c, BCG_T_MG_SOLVE);
+    long long l0 = c->launches;
+    int rc = mg_solve_impl(c, vcycles, 0);
+    if (rc) return rc;
+    timer_end(c, BCG_T_MG_SOLVE, (int)(c->launches - l0));
+    return ctx_check_status(c);
+}

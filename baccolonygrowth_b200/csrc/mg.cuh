@@ -1,0 +1,29 @@
+/* mg.cuh -- shared declarations of the multigrid and sweep translation units */
+#pragma once
+#include "ctx.cuh"
+
+struct MgConst {
+    int A;            /* composite (agar) levels, maxLevelsMG */
+    int levels;       /* multigrid levels (8 in the reference) */
+    int box_x, box_z_agar, box_z;
+    double bl2;       /* BoxLength^2 */
+    double dt;        /* the solve's time step (100 in the reference) */
+    double D[3];      /* agar diffusivities: carbon, oxygen, acetate */
+    double max_carbon, max_o2_agar;
+};
+
+struct MgLvl {
+    int nx, nz, pitch;
+    double* s[3];
+    double* r[3];
+    double* e[3];
+};
+
+MgConst mg_const(const bcg_ctx* c, double dt);
+MgLvl mg_lvl(const bcg_ctx* c, int l);
+void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2);
+void mg_setup(bcg_ctx* c, const MgConst& m);
+void mg_reset(bcg_ctx* c, const MgConst& m);
+void mg_copy_to(bcg_ctx* c, const MgConst& m, int wall_buf);
+void mg_copy_from(bcg_ctx* c, const MgConst& m, int cur_wall);
+int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf);

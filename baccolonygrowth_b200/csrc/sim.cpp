@@ -1,0 +1,168 @@
+/*
+ * sim.cpp -- the C++ host loop: a rewrite of SimSingleThread
+ * (AgentBasedModel-BacColonyGrowth/Simulation.cpp:42-434) over the C ABI.
+ *
+ * The host keeps what the reference keeps on the host: the glibc rand()
+ * stream, the time and the three loop flags, and the lineage record.  All
+ * cell and field state stays on the device; per step the host reads back
+ * two counters (dividing cells, F_cw draws) and uploads 9 draws per
+ * division.
+ */
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+#include "../../include/bcg.h"
+
+struct bcg_sim {
+    bcg_params P;
+    bcg_ctx* ctx;
+    bcg_rng rng;
+    double t, dt;
+    double next_out, next_update, hd_next_update, hd_update_time;
+    bool update_flag, hd_update_flag;
+    bool reference_cadence;
+    int vcycles_per_step;
+    bool first_step;
+    long long divisions;
+    std::vector<int> lineage;
+    std::vector<float> draws;
+};
+
+static float frand(bcg_rng* g) { return (float)bcg_rng_next(g) / (float)2147483647; }
+
+extern "C" int bcg_sim_create(const bcg_params* p, const bcg_cell* cells, int n, uint32_t seed,
+                              int run_initial_fields, bcg_sim** out)
+{
+    if (!p || !out || (n > 0 && !cells)) return BCG_E_ARG;
+    *out = nullptr;
+    bcg_sim* s = new bcg_sim();
+    s->P = *p;
+    int rc = bcg_create(p, &s->ctx);
+    if (rc) { delete s; return rc; }
+    rc = bcg_upload_cells(s->ctx, cells, n);
+    if (rc) { bcg_destroy(s->ctx); delete s; return rc; }
+    /* srand(seed) (CellMD3D.cpp:23) then the rough wall (Simulation.cpp:161-168) */
+    bcg_rng_seed(&s->rng, seed);
+    std::vector<double> wall((size_t)p->box_x * p->box_y);
+    for (int ii = 0; ii < p->box_x; ii++)
+        for (int jj = 0; jj < p->box_y; jj++)
+            wall[(size_t)ii * p->box_y + jj] = ((double)frand(&s->rng) - 0.5) * p->wall_rough;
+    rc = bcg_set_field(s->ctx, BCG_F_WALL, 0, wall.data(), wall.size());
+    if (rc == BCG_OK && run_initial_fields) {
+        /* Simulation.cpp:186-217 */
+        rc = bcg_initial_density(s->ctx);
+        if (rc == BCG_OK) rc = bcg_nutrient_update(s->ctx, 0, -1);
+    }
+    if (rc) { bcg_destroy(s->ctx); delete s; return rc; }
+    s->t = p->t0;
+    s->dt = p->dt;
+    s->next_out = p->output_time;
+    s->next_update = p->update_time;
+    s->hd_next_update = p->update_time / 10.0;
+    s->hd_update_time = p->update_time / 10.0;
+    s->update_flag = true;
+    s->hd_update_flag = true;
+    s->reference_cadence = true;
+    s->vcycles_per_step = 0;
+    s->first_step = true;
+    s->divisions = 0;
+    *out = s;
+    return BCG_OK;
+}
+
+extern "C" int bcg_sim_destroy(bcg_sim* s)
+{
+    if (!s) return BCG_OK;
+    bcg_destroy(s->ctx);
+    delete s;
+    return BCG_OK;
+}
+
+extern "C" bcg_ctx* bcg_sim_ctx(bcg_sim* s) { return s ? s->ctx : nullptr; }
+
+extern "C" int bcg_sim_set_step_mode(bcg_sim* s, int field_cadence_reference, int vcycles_per_step)
+{
+    if (!s || vcycles_per_step < 0) return BCG_E_ARG;
+    s->reference_cadence = field_cadence_reference != 0;
+    s->vcycles_per_step = vcycles_per_step;
+    return BCG_OK;
+}
+
+/* One iteration of while (t <= t_max), Simulation.cpp:254-431, without the
+ * output block. */
+static int sim_step(bcg_sim* s)
+{
+    int rc;
+    if (s->reference_cadence) {
+        if (s->update_flag) {
+            s->update_flag = false;
+            if ((rc = bcg_update_density(s->ctx))) return rc;
+            if ((rc = bcg_nutrient_update(s->ctx, 0, -1))) return rc;
+            if ((rc = bcg_rebuild_neighbours(s->ctx))) return rc;
+        }
+        if (s->hd_update_flag) {
+            s->hd_update_flag = false;
+            if ((rc = bcg_update_height(s->ctx))) return rc;
+        }
+    } else {
+        /* benchmark cadence: neighbour lists follow the reference's
+         * UpdateTime period; every step also runs the agar solve */
+        if (s->update_flag || s->first_step) {
+            s->update_flag = false;
+            if ((rc = bcg_rebuild_neighbours(s->ctx))) return rc;
+        }
+        if (s->vcycles_per_step > 0 && (rc = bcg_mg_solve(s->ctx, s->vcycles_per_step))) return rc;
+    }
+    s->first_step = false;
+    int nd = 0;
+    int64_t calls = 0;
+    if ((rc = bcg_move_grow(s->ctx, s->dt, &nd, &calls))) return rc;
+    bcg_rng_skip(&s->rng, calls);
+    s->draws.resize((size_t)9 * (nd > 0 ? nd : 1));
+    for (int i = 0; i < 9 * nd; i++) s->draws[i] = frand(&s->rng);
+    size_t base = s->lineage.size();
+    s->lineage.resize(base + 2 * (size_t)(nd > 0 ? nd : 0));
+    int done = 0;
+    rc = bcg_divide(s->ctx, s->draws.data(), nd, s->t, &done, nd > 0 ? s->lineage.data() + base : nullptr);
+    s->lineage.resize(base + 2 * (size_t)done);
+    s->divisions += done;
+    if (rc) return rc;
+    s->t += s->dt;
+    bool out = (s->next_out <= 0);
+    s->next_out = (out ? s->P.output_time : s->next_out) - s->dt;
+    s->update_flag = (s->next_update <= 0);
+    s->next_update = (s->update_flag ? s->P.update_time : s->next_update) - s->dt;
+    s->hd_update_flag = (s->hd_next_update <= 0);
+    s->hd_next_update = (s->hd_update_flag ? s->hd_update_time : s->hd_next_update) - s->dt;
+    return BCG_OK;
+}
+
+extern "C" int bcg_sim_run(bcg_sim* s, int steps)
+{
+    if (!s || steps < 0) return BCG_E_ARG;
+    for (int i = 0; i < steps; i++) {
+        int rc = sim_step(s);
+        if (rc) return rc;
+    }
+    return BCG_OK;
+}
+
+extern "C" int bcg_sim_time(bcg_sim* s, double* t, int* n_cells, int64_t* divisions)
+{
+    if (!s) return BCG_E_ARG;
+    if (t) *t = s->t;
+    if (n_cells) bcg_num_cells(s->ctx, n_cells);
+    if (divisions) *divisions = s->divisions;
+    return BCG_OK;
+}
+
+extern "C" int bcg_sim_lineage(bcg_sim* s, int* pairs, int capacity, int* n)
+{
+    if (!s) return BCG_E_ARG;
+    int total = (int)(s->lineage.size() / 2);
+    if (n) *n = total;
+    int m = total < capacity ? total : capacity;
+    if (m > 0 && pairs) memcpy(pairs, s->lineage.data(), sizeof(int) * 2 * (size_t)m);
+    return BCG_OK;
+}

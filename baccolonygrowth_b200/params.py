@@ -125,8 +125,8 @@ def read_parameters(path, p=None):
 WORKLOADS = {
     # name: (cells, dome aspect height/width, box_x, box_z, box_z_agar, agar levels)
     "small_4k": (4096, 6.0 / 40.0, 256, 50, 32, 2),
-    "scale_262k": (262144, 15.0 / 300.0, 2048, 128, 512, 3),
-    "mixed_1m": (1048576, 25.0 / 600.0, 4096, 192, 1024, 3),
+    "scale_262k": (262144, 15.0 / 300.0, 2304, 128, 512, 3),
+    "mixed_1m": (1048576, 25.0 / 600.0, 4608, 200, 1024, 3),
 }
 
 
@@ -150,7 +150,7 @@ def workload_params(name, max_cells=None):
     return finalize(p)
 
 
-def dome_size(n_cells, aspect, phi=0.4, radius=0.5, mean_len=3.0):
+def dome_size(n_cells, aspect, phi=0.45, radius=0.5, mean_len=3.0):
     """Half-ellipse width/height (um) holding n cells at area fraction phi."""
     area = n_cells * (2 * radius) * (mean_len + 2 * radius) / phi
     w = math.sqrt(area / (math.pi / 4.0 * aspect))

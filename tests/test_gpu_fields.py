@@ -1,0 +1,133 @@
+"""Parity of the CUDA field chain with the C restatement in oracle/:
+deposition and surface fields (Compute.cpp), the composite-grid multigrid
+(Multigrid.cpp) and the colony/interface sweeps (Nutrients.cpp).
+
+Tolerance: 1e-12 relative (the sums over a box run in a different order
+than the reference's box lists; everything else keeps the reference's
+operation order).  The level > 0 wall interior, where the reference reads
+uninitialised locals, is excluded.
+"""
+import numpy as np
+import pytest
+
+from baccolonygrowth_b200 import _abi, params
+from baccolonygrowth_b200.colony import Colony, workload_colony
+
+import checkers as ck
+
+F = _abi.FIELDS
+TOL = 1e-12
+pytestmark = pytest.mark.gpu
+
+
+def make(n=4096, workload="small_4k", seed=12345):
+    p = params.workload_params(workload)
+    cells = workload_colony(workload, n=n)
+    orc = ck.Oracle(p, seed=seed)
+    orc.load(cells)
+    col = Colony(p, cells)
+    col.set_field("WALL", orc.field(F["WALL"]))
+    return p, orc, col
+
+
+def close(a, b, tol=TOL, mask=None):
+    a = np.asarray(a); b = np.asarray(b)
+    if mask is not None:
+        a = a[mask]; b = b[mask]
+    scale = max(np.abs(a).max(), 1e-300)
+    return np.abs(a - b).max() / scale
+
+
+def bbox_mask(p, bbox, nz=None):
+    minx, maxx, maxz = bbox
+    Z = p.box_z
+    m = np.zeros((p.box_x, Z), dtype=bool)
+    m[max(minx, 0):max(maxx, 0), :min(maxz, Z)] = True
+    return m.reshape(-1)
+
+
+def wall_mask(p, level):
+    m = np.ones(p.box_x, dtype=bool)
+    if level > 0:
+        m[p.box_x // 4: p.box_x * 3 // 4] = False
+    return m
+
+
+def test_density_chain(gpu):
+    p, orc, col = make()
+    orc.update_density()
+    col.update_density()
+    assert orc.bbox() == col.bbox()
+    for f in ("INSIDE", "HEIGHT", "NORMAL_X", "NORMAL_Z"):
+        assert np.array_equal(orc.field(F[f]), col.field(f)), f
+    m = bbox_mask(p, orc.bbox())
+    for f in ("ROUGH_DENSITY", "DENSITY_SHIFT", "DENSITY"):
+        assert close(orc.field(F[f]), col.field(f), mask=m) <= TOL, f
+
+
+def test_height_chain(gpu):
+    p, orc, col = make()
+    orc.update_height()
+    col.update_height()
+    assert orc.bbox() == col.bbox()
+    for f in ("HEIGHT", "NORMAL_X", "NORMAL_Z"):
+        assert np.array_equal(orc.field(F[f]), col.field(f)), f
+
+
+def test_mg_solve(gpu):
+    p, orc, col = make()
+    orc.update_density()
+    col.update_density()
+    orc.mg_solve(3, p.mg_dt)
+    col.mg_solve(3)
+    for l in range(p.mg_levels):
+        for sp in ("CARBON", "OXYGEN", "ACETATE"):
+            for kind in ("SOL", "RES", "ERR"):
+                f = "MG_%s_%s" % (kind, sp)
+                a, b = orc.field(F[f], l), col.field(f, l)
+                if kind == "SOL":
+                    assert close(a, b) <= TOL, (f, l)
+                else:
+                    assert np.abs(a - b).max() <= TOL * max(1.0, np.abs(a).max()), (f, l)
+    for l in range(p.max_levels_mg):
+        for sp in ("CARBON", "OXYGEN", "ACETATE"):
+            f = "WALLF_" + sp
+            assert close(orc.field(F[f], l), col.field(f, l)) <= TOL, (f, l)
+            f = "AGARF_" + sp
+            assert close(orc.field(F[f], l), col.field(f, l)) <= TOL, (f, l)
+
+
+def test_nutrient_update(gpu):
+    p, orc, col = make()
+    orc.update_density()
+    col.update_density()
+    orc.nutrient_update(2)
+    col.nutrient_update(2)
+    m = bbox_mask(p, orc.bbox())
+    for f in ("ENV_CARBON", "ENV_WASTE", "ENV_OXYGEN", "ENV_ACETATE", "ENV_GROWTH1", "ENV_GROWTH2",
+              "OLDENV_CARBON", "OLDENV_WASTE", "OLDENV_OXYGEN", "OLDENV_ACETATE"):
+        assert close(orc.field(F[f]), col.field(f), mask=m) <= 1e-11, f
+    inside = orc.field(F["INSIDE"]) > 0.5
+    assert close(orc.field(F["ENV_PH"]), col.field("ENV_PH"), mask=inside & m) <= 1e-9
+    for l in range(p.max_levels_mg):
+        wm = wall_mask(p, l)
+        for f in ("WALLF_CARBON", "WALLF_WASTE", "WALLF_OXYGEN", "WALLF_ACETATE",
+                  "OLDWALLF_CARBON", "OLDWALLF_WASTE", "OLDWALLF_OXYGEN", "OLDWALLF_ACETATE"):
+            a, b = orc.field(F[f], l)[wm], col.field(f, l)[wm]
+            assert np.abs(a - b).max() <= 1e-11 * max(1.0, np.abs(a).max()), (f, l)
+    for l in range(p.mg_levels):
+        for sp in ("CARBON", "OXYGEN", "ACETATE"):
+            f = "MG_SOL_" + sp
+            assert close(orc.field(F[f], l), col.field(f, l)) <= 1e-11, (f, l)
+
+
+def test_colony_sweeps_odd_count(gpu):
+    p, orc, col = make(n=2048)
+    for m in (orc, col):
+        m.update_density()
+        m.mg_solve(1) if m is col else m.mg_solve(1, p.mg_dt)
+    orc.colony_sweeps(7, 1)
+    col.colony_sweeps(7, 1)
+    mk = bbox_mask(p, orc.bbox())
+    for f in ("ENV_CARBON", "OLDENV_CARBON", "ENV_ACETATE", "OLDENV_OXYGEN"):
+        assert close(orc.field(F[f]), col.field(f), mask=mk) <= 1e-11, f

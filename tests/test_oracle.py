@@ -1,0 +1,127 @@
+"""The checker itself: the C restatement (oracle/liboracle.so) reproduces
+the reference bit for bit on the committed golden vectors (made from the
+reference by tests/golden/make_golden.py), and, where the reference tree is
+built here (oracle/_ref), on live runs of the reference."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from baccolonygrowth_b200 import _abi, params
+from baccolonygrowth_b200.colony import workload_colony
+
+import checkers as ck
+
+F = _abi.FIELDS
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load_params(js):
+    p = _abi.Params()
+    for k, v in json.loads(str(js)).items():
+        setattr(p, k, v)
+    return p
+
+
+def unpack(counts, flat):
+    out, o = [], 0
+    for c in counts:
+        out.append(flat[o:o + c])
+        o += c
+    return out
+
+
+def test_oracle_matches_golden_mechanics():
+    g = np.load(os.path.join(GOLD, "mech_small.npz"))
+    p = load_params(g["params"])
+    orc = ck.Oracle(p, seed=12345)
+    orc.load(g["cells_in"])
+    orc.update_height()
+    orc.set_field(F["ENV_GROWTH1"], np.full(p.box_x * p.box_z, 0.9))
+    orc.rebuild()
+    for f, key in (("HEIGHT", "height"), ("NORMAL_X", "normal_x"), ("NORMAL_Z", "normal_z"), ("WALL", "wall")):
+        assert np.array_equal(orc.field(F[f]), g[key]), f
+    nb = orc.neighbours()
+    want = unpack(g["nbr0_counts"], g["nbr0_flat"])
+    assert all(np.array_equal(a, b) for a, b in zip(nb, want))
+    divs = unpack(g["div_counts"], g["div_flat"])
+    lins = unpack(g["lineage_counts"], g["lineage"])
+    t = 0.0
+    for s in range(len(g["rand_calls"])):
+        ids, calls, lin = orc.step(p.dt, t)
+        t += p.dt
+        assert calls == g["rand_calls"][s]
+        assert np.array_equal(ids, divs[s])
+        assert np.array_equal(lin.reshape(-1), lins[s])
+    assert orc.cells().tobytes() == g["cells_out"].tobytes()
+    nb = orc.neighbours()
+    want = unpack(g["nbr_counts"], g["nbr_flat"])
+    assert all(np.array_equal(a, b) for a, b in zip(nb, want))
+
+
+def test_oracle_matches_golden_fields():
+    g = np.load(os.path.join(GOLD, "fields_small.npz"))
+    p = load_params(g["params"])
+    orc = ck.Oracle(p, seed=12345)
+    orc.load(g["cells_in"])
+    orc.update_density()
+    assert tuple(orc.bbox()) == tuple(g["bbox"])
+    for f in ("ROUGH_DENSITY", "INSIDE", "DENSITY_SHIFT", "DENSITY", "HEIGHT", "NORMAL_X", "NORMAL_Z", "WALL"):
+        assert np.array_equal(orc.field(F[f]), g["d_" + f]), f
+    orc.mg_solve(3, p.mg_dt)
+    for l in range(p.mg_levels):
+        for sp in ("CARBON", "OXYGEN", "ACETATE"):
+            assert np.array_equal(orc.field(F["MG_SOL_" + sp], l), g["mg_%d_%s" % (l, sp)]), (l, sp)
+    orc.nutrient_update(1)
+    for f in ("ENV_CARBON", "ENV_WASTE", "ENV_OXYGEN", "ENV_ACETATE", "ENV_GROWTH1", "ENV_PH",
+              "OLDENV_CARBON", "OLDENV_WASTE", "OLDENV_OXYGEN", "OLDENV_ACETATE"):
+        assert np.array_equal(orc.field(F[f]), g["n_" + f]), f
+    X = p.box_x
+    for l in range(p.max_levels_mg):
+        keep = np.ones(X, dtype=bool)
+        if l > 0:   # the reference reads uninitialised locals for these points
+            keep[X // 4:X * 3 // 4] = False
+        for f in ("WALLF_CARBON", "WALLF_WASTE", "WALLF_OXYGEN", "WALLF_ACETATE", "OLDWALLF_CARBON"):
+            assert np.array_equal(orc.field(F[f], l)[keep], g["n_%s_%d" % (f, l)][keep]), (f, l)
+        for sp in ("CARBON", "OXYGEN", "ACETATE"):
+            assert np.array_equal(orc.field(F["MG_SOL_" + sp], l), g["n_mg_%d_%s" % (l, sp)]), (l, sp)
+
+
+needs_ref = pytest.mark.skipif(not ck.have_ref(), reason="reference harness (oracle/_ref) not built here")
+
+
+@needs_ref
+def test_oracle_matches_reference_live_loop():
+    """The whole while-loop body (Simulation.cpp:256-430) including the
+    UpdateFlag field block, with a short nutrient schedule."""
+    p = params.workload_params("small_4k")
+    p.solves_per_update = 1
+    p.update_time = 0.0004   # field update every 4 steps
+    cells = workload_colony("small_4k", n=1024)
+    ref = ck.Reference(p, seed=777)
+    orc = ck.Oracle(p, seed=777)
+    ref.load(cells)
+    orc.load(cells)
+    # the loop body's field / neighbour / mechanics sequence, one solve per update
+    ref.initial_fields(False)
+    orc.initial_fields(False)
+    for s in range(6):
+        ref.update_density(); orc.update_density()
+        ref.nutrient_update(1); orc.nutrient_update(1)
+        ref.rebuild(); orc.rebuild()
+        ref.update_height(); orc.update_height()
+        r1, r2 = ref.step(p.dt, 0.0001 * s), orc.step(p.dt, 0.0001 * s)
+        assert r1[1] == r2[1] and np.array_equal(r1[2], r2[2])
+    assert ref.cells().tobytes() == orc.cells().tobytes()
+    # outside the bounding box BoxAverage leaves the reference's scratch
+    # array uninitialised; compare inside it
+    minx, maxx, maxz = ref.bbox()
+    box = np.zeros((p.box_x, p.box_z), dtype=bool)
+    box[minx:maxx, :maxz] = True
+    box = box.reshape(-1)
+    for f in ("ENV_CARBON", "ENV_GROWTH1", "DENSITY_SHIFT", "HEIGHT"):
+        a, b = ref.field(F[f]), orc.field(F[f])
+        if a.size == box.size:
+            a, b = a[box], b[box]
+        assert np.array_equal(a, b), f
