@@ -215,6 +215,7 @@ EXTRA_PROTOTYPES = {
     "bcg_set_force_group": (_I, [_I]),
     "bcg_kernel_launches": (ctypes.c_longlong, [_VP]),
     "bcg_set_bbox": (_I, [_VP, _I, _I, _I]),
+    "bcg_set_relax_mode": (_I, [_I]),
 }
 
 _lib = None

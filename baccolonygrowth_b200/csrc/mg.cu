@@ -18,6 +18,20 @@ __device__ __forceinline__ double dmind(double a, double b) { return a < b ? a :
 
 #define AT(arr, L, i, k) (arr)[(size_t)(k) * (L).pitch + (i)]
 
+/* Read (i, k) with the reference's flat index i*(nz+1)+k: on levels with
+ * nz <= 1 the stencils reach k = -1 or k = nz+1, which the reference's
+ * Array3D maps onto the neighbouring column; an index past either end of
+ * the array (undefined in the reference) reads as 0.  In range it is AT. */
+__device__ __forceinline__ double at_ref(const double* a, const MgLvl& L, int i, int k)
+{
+    if (k >= 0 && k <= L.nz) return AT(a, L, i, k);
+    long f = (long)i * (L.nz + 1) + k;
+    long n = (long)(L.nx + 1) * (L.nz + 1);
+    if (f < 0 || f >= n) return 0.0;
+    int i2 = (int)(f / (L.nz + 1)), k2 = (int)(f % (L.nz + 1));
+    return AT(a, L, i2, k2);
+}
+
 MgConst mg_const(const bcg_ctx* c, double dt)
 {
     MgConst m;
@@ -67,14 +81,14 @@ __device__ __forceinline__ void relax_point(const MgConst& m, const MgLvl& L, in
                 if (oxy) out = r;
                 else {
                     double s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
-                    double up = AT(E, L, i, 1);
+                    double up = at_ref(E, L, i, 1);
                     out = (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
                 }
             } else write = false;
         } else {
             if (oxy) out = r;
             else {
-                double up = AT(E, L, i, 1), xm = AT(E, L, i - 1, 0), xp = AT(E, L, i + 1, 0);
+                double up = at_ref(E, L, i, 1), xm = AT(E, L, i - 1, 0), xp = AT(E, L, i + 1, 0);
                 out = (r * h2 / dt / D + up + 0.5 * xm + 0.5 * xp) / (h2 / dt / D + 2);
             }
         }
@@ -120,6 +134,132 @@ __global__ void k_mg_relax(MgConst m, MgLvl L, int l, int parity, const double* 
     for (int k = 0; k <= L.nz; k++) relax_point(m, L, l, sp, i, k, inside0, below, k > 0);
 }
 
+/* Segmented form of the same sweep, for tall columns.  Along a column the
+ * update is a first-order recurrence E_k = (b_k + w E_{k-1}) / (c + 2) with
+ * w/(c + 2) <= 1/4 (c = h^2/(dt D) >= 0, w <= 1), so the influence of the
+ * value carried in from below shrinks by 4x per row.  Each thread owns SEG
+ * rows of one column and first re-runs the WARM rows below them from the
+ * pre-sweep values; after WARM = 32 rows the carried-in difference is
+ * below 4^-32 ~ 5e-20 of itself, i.e. the rows are those of the sequential
+ * bottom-to-top sweep.  The pre-sweep values a thread reads from rows that
+ * another thread of its column writes (its warm-up rows' upper neighbours
+ * and the row just above its segment) are loaded before a block barrier, so
+ * every thread reads them before any thread writes.  All segments of a
+ * column live in one block: blockDim = (32 columns, nseg segments). */
+#define RELAX_WARM 32
+__global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l, int parity, int seg_len,
+                                                      const double* __restrict__ inside0)
+{
+    const int ncol = (L.nx + 1 - parity + 1) / 2;
+    const int t = blockIdx.x * 32 + threadIdx.x;
+    const int seg = threadIdx.y;
+    const int sp = blockIdx.y;
+    const bool active = t < ncol;
+    const int i = 2 * t + parity;
+    const int nz = L.nz;
+    const int k_begin = seg * seg_len;
+    const int k_end = min(k_begin + seg_len, nz + 1);
+    const int k_start = max(0, k_begin - RELAX_WARM);
+    double* E = L.e[sp];
+    /* pre-sweep values this thread needs from rows other threads write */
+    double up_w[RELAX_WARM + 1];
+    double below = 0.0, above_end = 0.0;
+    if (active && k_begin <= nz) {
+        for (int k = k_start; k < k_begin; k++) up_w[k - k_start] = AT(E, L, i, k + 1);
+        if (k_start > 0) below = AT(E, L, i, k_start - 1);
+        if (k_end <= nz) above_end = AT(E, L, i, k_end);
+    }
+    __syncthreads();
+    if (!active || k_begin > nz) return;
+    const double h2 = m.bl2 * (double)(1 << (2 * l));
+    const double dt = m.dt, D = m.D[sp];
+    const double* R = L.r[sp];
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    const int nx = L.nx;
+    const bool side = (i == 0 || i == nx);
+    double xm_, xp_;
+    for (int k = k_start; k < k_end; k++) {
+        const bool warm = k < k_begin;
+        double r = AT(R, L, i, k);
+        double up = (k < nz) ? (warm ? up_w[k - k_start] : (k + 1 == k_end ? above_end : AT(E, L, i, k + 1))) : 0.0;
+        double e_dn = below;
+        double out = 0.0;
+        bool write = true;
+        if (k == 0) {
+            int d = 1 << l;
+            int i0 = (i - nx / 2) * d + m.box_x / 2;
+            i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+            if (inside0[(size_t)i0 * m.box_z] > 0) out = r;
+            else if (side) {
+                if (top_levels) {
+                    if (oxy) out = r;
+                    else {
+                        double s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
+                        out = (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
+                    }
+                } else write = false;
+            } else {
+                if (oxy) out = r;
+                else {
+                    xm_ = AT(E, L, i - 1, 0); xp_ = AT(E, L, i + 1, 0);
+                    out = (r * h2 / dt / D + up + 0.5 * xm_ + 0.5 * xp_) / (h2 / dt / D + 2);
+                }
+            }
+        } else if (k == nz) {
+            if (top_levels) {
+                if (side) {
+                    if (oxy) out = r;
+                    else {
+                        double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                        out = (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
+                    }
+                } else {
+                    xp_ = AT(E, L, i + 1, k); xm_ = AT(E, L, i - 1, k);
+                    out = (r * h2 / dt / D + e_dn + 0.5 * xp_ + 0.5 * xm_) / (h2 / dt / D + 2);
+                }
+            } else write = false;
+        } else if (side) {
+            if (top_levels) {
+                if (oxy) out = r;
+                else {
+                    double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                    out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + s1) / (h2 / dt / D + 2);
+                }
+            } else write = false;
+        } else {
+            xm_ = AT(E, L, i - 1, k); xp_ = AT(E, L, i + 1, k);
+            out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + 0.5 * xm_ + 0.5 * xp_) / (h2 / dt / D + 2);
+        }
+        /* points that are not relaxed keep their value; those columns and
+         * rows (composite edges) are written by no thread in this sweep */
+        if (!write) out = AT(E, L, i, k);
+        if (write && !warm) AT(E, L, i, k) = out;
+        below = out;
+    }
+}
+
+/* All mu2 relaxations of a small (coarsest) level in one block: the sweep
+ * order (even columns, then odd, each bottom to top) is kept with a block
+ * barrier between half-sweeps. */
+__global__ void __launch_bounds__(1024) k_mg_relax_coarse(MgConst m, MgLvl L, int l, int sweeps,
+                                                          const double* __restrict__ inside0)
+{
+    const int nx = L.nx;
+    const int ncols = nx + 1;
+    for (int s = 0; s < sweeps; s++)
+        for (int parity = 0; parity < 2; parity++) {
+            int ncol = (ncols - parity + 1) / 2;
+            for (int w = threadIdx.x; w < 3 * ncol; w += blockDim.x) {
+                int sp = w / ncol, t = w % ncol;
+                int i = 2 * t + parity;
+                double below = 0.0;
+                for (int k = 0; k <= L.nz; k++) relax_point(m, L, l, sp, i, k, inside0, below, k > 0);
+            }
+            __syncthreads();
+        }
+}
+
 /* ------------------------------------------------------------------------ */
 /* restrictionAgaElementwise, Multigrid.cpp:269-405 (level l from l-1)       */
 /* ------------------------------------------------------------------------ */
@@ -138,17 +278,17 @@ __global__ void k_mg_restrict(MgConst m, MgLvl Lc, MgLvl Lf, int l, const double
     const double dt = m.dt, D = m.D[sp];
     const bool oxy = sp == 1;
     int i0 = (i - nx / 2) * d + X / 2;
-    i0 = i0 < 0 ? 0 : (i0 > X ? X : i0);
+    i0 = i0 < 0 ? 0 : (i0 > X ? X : i0);   /* clamped to BoxX as in the reference */
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     const double* EP = Lf.e[sp];
     const double* RP = Lf.r[sp];
     const double* AP = Lf.s[sp];
     const double* AL = Lc.s[sp];
     double* R = &AT(Lc.r[sp], Lc, i, k);
-#define EPv(a, b) AT(EP, Lf, a, b)
-#define RPv(a, b) AT(RP, Lf, a, b)
-#define APv(a, b) AT(AP, Lf, a, b)
-#define ALv(a, b) AT(AL, Lc, a, b)
+#define EPv(a, b) at_ref(EP, Lf, a, b)
+#define RPv(a, b) at_ref(RP, Lf, a, b)
+#define APv(a, b) at_ref(AP, Lf, a, b)
+#define ALv(a, b) at_ref(AL, Lc, a, b)
     if (i == 0 || i == nx || k == nz) {
         if (l >= m.A) {
             if (k == nz && (i > 0) && (i < nx)) {
@@ -166,7 +306,9 @@ __global__ void k_mg_restrict(MgConst m, MgLvl Lc, MgLvl Lf, int l, const double
             }
         }
     } else if (k == 0) {
-        if (inside0[(size_t)i0 * m.box_z] > 0) *R = 0;
+        /* i0 == BoxX lies one row past insideColonyDen (Multigrid.cpp:279);
+         * it counts as outside the colony */
+        if (i0 < X && inside0[(size_t)i0 * m.box_z] > 0) *R = 0;
         else if (ip > 0 && ip < nxp) {
             if (oxy) *R = (RPv(ip, 0) - EPv(ip, 0)) * 0.5;
             else *R = (RPv(ip, 0) + 0.5 * (EPv(ip + 1, 0) + EPv(ip - 1, 0) + 2 * EPv(ip, 1) - 4 * EPv(ip, 0)) * D * dt * 4 / h2 - EPv(ip, 0)) * 0.5;
@@ -210,18 +352,20 @@ __global__ void k_mg_interp(MgConst m, MgLvl Lf, MgLvl Lc, int l)
     int nxp = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
     const double* C = Lc.e[sp];
     double& e = AT(Lf.e[sp], Lf, i, k);
+#define CV(a, b) at_ref(C, Lc, a, b)
     if (i % 2 == 0) {
         int ip = nxp / 2 - nx / 4 + i / 2;
-        if (k % 2 == 0) e += AT(C, Lc, ip, k / 2);
-        else { int kp = (k - 1) / 2; e += 0.5 * (AT(C, Lc, ip, kp) + AT(C, Lc, ip, kp + 1)); }
+        if (k % 2 == 0) e += CV(ip, k / 2);
+        else { int kp = (k - 1) / 2; e += 0.5 * (CV(ip, kp) + CV(ip, kp + 1)); }
     } else {
         int ip = nxp / 2 - nx / 4 + (i - 1) / 2;
-        if (k % 2 == 0) { int kp = k / 2; e += 0.5 * (AT(C, Lc, ip, kp) + AT(C, Lc, ip + 1, kp)); }
+        if (k % 2 == 0) { int kp = k / 2; e += 0.5 * (CV(ip, kp) + CV(ip + 1, kp)); }
         else {
             int kp = (k - 1) / 2;
-            e += 0.25 * (AT(C, Lc, ip, kp) + AT(C, Lc, ip, kp + 1) + AT(C, Lc, ip + 1, kp) + AT(C, Lc, ip + 1, kp + 1));
+            e += 0.25 * (CV(ip, kp) + CV(ip, kp + 1) + CV(ip + 1, kp) + CV(ip + 1, kp + 1));
         }
     }
+#undef CV
 }
 
 /* resetZero, Multigrid.cpp:47-82 */
@@ -396,14 +540,41 @@ __global__ void k_mg_copy_from(MgLvl L, int X, double* cC, double* cO, double* c
 /* ------------------------------------------------------------------------ */
 static inline dim3 grid2(int n, int threads) { return dim3((unsigned)((n + threads - 1) / threads), 3); }
 
+static int g_relax_mode = 1;   /* 0 = one thread per column, 1 = segmented */
+extern "C" int bcg_set_relax_mode(int mode) { if (mode < 0 || mode > 1) return BCG_E_ARG; g_relax_mode = mode; return BCG_OK; }
+
 static void relax_level(bcg_ctx* c, const MgConst& m, int l)
 {
     MgLvl L = mg_lvl(c, l);
-    for (int par = 0; par < 2; par++) {
-        int ncol = (L.nx + 1 - par + 1) / 2;
-        k_mg_relax<<<grid2(ncol, 64), 64, 0, c->stream>>>(m, L, l, par, c->inside);
+    const int rows = L.nz + 1;
+    if (g_relax_mode == 0 || rows <= 96) {
+        for (int par = 0; par < 2; par++) {
+            int ncol = (L.nx + 1 - par + 1) / 2;
+            k_mg_relax<<<grid2(ncol, 64), 64, 0, c->stream>>>(m, L, l, par, c->inside);
+        }
+    } else {
+        int nseg = (rows + 63) / 64;
+        if (nseg > 16) nseg = 16;
+        int seg_len = (rows + nseg - 1) / nseg;
+        for (int par = 0; par < 2; par++) {
+            int ncol = (L.nx + 1 - par + 1) / 2;
+            dim3 grid((unsigned)((ncol + 31) / 32), 3);
+            k_mg_relax_seg<<<grid, dim3(32, nseg), 0, c->stream>>>(m, L, l, par, seg_len, c->inside);
+        }
     }
     c->launches += 2;
+}
+
+/* mu2 sweeps on the coarsest level: fused when it fits one block */
+static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
+{
+    MgLvl L = mg_lvl(c, l);
+    if (g_relax_mode == 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
+        k_mg_relax_coarse<<<1, 1024, 0, c->stream>>>(m, L, l, sweeps, c->inside);
+        c->launches++;
+    } else {
+        for (int j = 0; j < sweeps; j++) relax_level(c, m, l);
+    }
 }
 
 void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
@@ -415,7 +586,7 @@ void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
         k_mg_restrict<<<grid2((Lc.nx + 1) * (Lc.nz + 1), 256), 256, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
         c->launches++;
     }
-    for (int j = 0; j < mu2; j++) relax_level(c, m, Lv - 1);
+    relax_coarsest(c, m, Lv - 1, mu2);
     for (int l = Lv - 2; l >= 0; l--) {
         MgLvl Lf = mg_lvl(c, l), Lc = mg_lvl(c, l + 1);
         k_mg_interp<<<grid2((Lf.nx + 1) * (Lf.nz + 1), 256), 256, 0, c->stream>>>(m, Lf, Lc, l);

@@ -1,0 +1,388 @@
+"""Benchmark of the BacColonyGrowth hot path on B200.
+
+One step = one pass of the hot path over the colony: MoveCell + GrowCell for
+every cell (two-stage integration with forces from the neighbour lists,
+growth), the division loop with its partial neighbour rebuilds, the full
+neighbour rebuild on the reference's UpdateTime cadence (every 100 steps),
+and one agar solve (Multigrid::solve with `--vcycles` V-cycles) -- the
+"1,000 mechanics steps with one V-cycle nutrient solve per step" schedule,
+on the 1,048,576-cell workload restated in the reference's 2-D x-z geometry.
+
+Metric: cell-steps/s (cells x steps / time), with the multigrid DOF/s of
+the solve reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+  python bench.py --impl reference      # the reference's own CPU code
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="mixed_1m")
+    ap.add_argument("--vcycles", type=int, default=1)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def mg_dof(p):
+    """3 species x the finest composite levels' points (the work unit of one
+    V-cycle; coarser levels count as work, not DOF)."""
+    A = p.max_levels_mg
+    return 3 * A * (p.box_x + 1) * (p.box_z_agar + 1)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own code (oracle/_ref) or, where it is not built,
+# the C restatement, on a bounded sample of the same workload
+# ---------------------------------------------------------------------------
+def cpu_run(p, cells, steps, threads, sample_cells=131072):
+    """Time the CPU implementation on a bounded sample of the workload: the
+    mechanics on a central x-window of `sample_cells` cells (per-cell cost
+    does not depend on the colony size), the agar solve on the full grid.
+    Returns per-step time for the whole workload (cells / mechanics rate +
+    one 1-V-cycle solve + the neighbour rebuild amortised over 100 steps)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+    import checkers
+    from baccolonygrowth_b200 import _abi, params as _params
+    kind = "reference" if checkers.have_ref() else "port"
+    n = len(cells)
+    m_cells = min(n, sample_cells)
+    order = np.argsort(np.abs(0.5 * (cells["p"][:, 0] + cells["q"][:, 0])), kind="stable")
+    sample = np.ascontiguousarray(cells[np.sort(order[:m_cells])])
+    ps = p.copy()
+    ps.max_cells = int(m_cells * 1.1) + 1024
+
+    def model(pp):
+        if kind == "reference":
+            return checkers.Reference(pp, seed=12345, threads=threads)
+        return checkers.Oracle(pp, seed=12345)
+
+    m = model(ps)
+    m.load(sample)
+    m.set_field(_abi.FIELDS["ENV_GROWTH1"], np.full(p.box_x * p.box_z, 0.9))
+    t0 = time.perf_counter()
+    m.rebuild()
+    t_rebuild = time.perf_counter() - t0
+    t = 0.0
+    t0 = time.perf_counter()
+    for s in range(steps):
+        m.step(p.dt, t)
+        t += p.dt
+    t_mech = (time.perf_counter() - t0) / steps
+    m.close()
+    del m
+    pg = p.copy()
+    pg.max_cells = 4096
+    g = model(pg)
+    t0 = time.perf_counter()
+    g.mg_solve(1, p.mg_dt)
+    t_solve = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    g.mg_solve(3, p.mg_dt)
+    t_v = max((time.perf_counter() - t0 - t_solve) / 2.0, 1e-9)
+    g.close()
+    rate = m_cells / (t_mech + t_rebuild / 100.0)
+    per_step = n / rate + t_solve
+    return dict(kind=kind, threads=threads if kind == "reference" else 1, per_step=per_step,
+                t_mech=t_mech, t_solve=t_solve, t_vcycle=t_v, cell_steps=n / per_step,
+                mg_dof_s=mg_dof(p) / t_v,
+                sample="mechanics: %d of the %d cells (central x-window), %d steps + 1 full neighbour rebuild "
+                       "(amortised over 100 steps); agar: Multigrid::solve with 1 and 3 V-cycles on the full "
+                       "%dx%d composite grid; per step = cells/mechanics rate + one 1-V-cycle solve"
+                       % (m_cells, n, steps, p.box_x + 1, p.box_z_agar + 1))
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from baccolonygrowth_b200 import params
+    from baccolonygrowth_b200.colony import workload_colony
+    p = params.workload_params(args.workload)
+    cells = workload_colony(args.workload)
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, args.cpu_sample_steps))
+    # warm-up sample (page-in), then the timed samples
+    r = None
+    for i in range(max(1, min(args.warmup, 1))):
+        cpu_run(p, cells[:4096], 1, threads)
+    r = cpu_run(p, cells, steps, threads)
+    v = r["cell_steps"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "cells": len(cells), "box": [p.box_x, p.box_y, p.box_z],
+                   "box_z_agar": p.box_z_agar, "agar_levels": p.max_levels_mg, "vcycles_per_step": 1},
+        "mg_dof_per_s": r["mg_dof_s"],
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": r["threads"], "kind": r["kind"],
+                         "sample": r["sample"]},
+        "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def b200_arm(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from baccolonygrowth_b200 import _abi, params
+    from baccolonygrowth_b200.colony import workload_colony
+    lib = _abi.load()
+    p = params.workload_params(args.workload)
+    # replicas: every rank runs its own colony (different seed), no
+    # data-path collective
+    cells = workload_colony(args.workload, seed=20261205 + rank)
+    n0 = len(cells)
+    cells = np.ascontiguousarray(cells)
+    pinned = torch.empty(cells.nbytes, dtype=torch.uint8, pin_memory=True)
+    hostbuf = pinned.numpy().view(_abi.CELL_DTYPE)
+    hostbuf[:] = cells
+
+    def make_sim():
+        sim = ctypes.c_void_p()
+        _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(hostbuf), n0, 12345 + rank, 0, ctypes.byref(sim)), "bcg_sim_create")
+        _abi.check(lib.bcg_sim_set_step_mode(sim, 0, args.vcycles), "bcg_sim_set_step_mode")
+        ctx = lib.bcg_sim_ctx(sim)
+        # growth field of a colony in steady nutrient supply (no field update
+        # runs inside the timed steps)
+        g = np.full(p.box_x * p.box_z, 0.9)
+        _abi.check(lib.bcg_set_field(ctx, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size), "set growth")
+        _abi.check(lib.bcg_update_density(ctx), "bcg_update_density")
+        return sim, ctx
+
+    sim, ctx = make_sim()
+    stream = torch.cuda.ExternalStream(lib.bcg_stream(ctx))
+    _abi.check(lib.bcg_sim_run(sim, args.warmup), "warmup")
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = int(lib.bcg_kernel_launches(ctx))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    _abi.check(lib.bcg_sim_run(sim, args.steps), "timed steps")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = int(lib.bcg_kernel_launches(ctx)) - launches0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    t_ = ctypes.c_double(); n_ = ctypes.c_int(); d_ = ctypes.c_int64()
+    lib.bcg_sim_time(sim, ctypes.byref(t_), ctypes.byref(n_), ctypes.byref(d_))
+    n_end = n_.value
+    cells_mean = 0.5 * (n0 + n_end)
+
+    # per-kernel device time of the same schedule with timers on (separate run,
+    # so the event syncs of the timers do not enter the timed region above)
+    _abi.check(lib.bcg_enable_timers(ctx, 1), "timers")
+    kt_steps = min(20, args.steps)
+    _abi.check(lib.bcg_sim_run(sim, kt_steps), "timer steps")
+    timers = {}
+    for name, tid in _abi.TIMERS.items():
+        msx = ctypes.c_double(); nl = ctypes.c_int64()
+        lib.bcg_get_timer(ctx, tid, ctypes.byref(msx), ctypes.byref(nl))
+        timers[name] = msx.value / kt_steps
+    _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
+    n_now = ctypes.c_int()
+    lib.bcg_num_cells(ctx, ctypes.byref(n_now))
+    lib.bcg_sim_destroy(sim)
+
+    # end to end through the C ABI with host buffers: upload of the colony
+    # from pinned host memory, the steps (each reads two counters back and
+    # uploads the division draws), download of the final colony
+    sim2 = ctypes.c_void_p()
+    _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(hostbuf), 0, 12345 + rank, 0, ctypes.byref(sim2)), "sim2")
+    _abi.check(lib.bcg_sim_set_step_mode(sim2, 0, args.vcycles), "mode2")
+    ctx2 = lib.bcg_sim_ctx(sim2)
+    g = np.full(p.box_x * p.box_z, 0.9)
+    lib.bcg_set_field(ctx2, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size)
+    out_pinned = torch.empty((n0 + n0 // 4) * 208, dtype=torch.uint8, pin_memory=True)
+    outbuf = out_pinned.numpy().view(_abi.CELL_DTYPE)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    _abi.check(lib.bcg_upload_cells(ctx2, _abi.ptr(hostbuf), n0), "upload")
+    _abi.check(lib.bcg_update_density(ctx2), "density")
+    _abi.check(lib.bcg_sim_run(sim2, args.steps), "e2e steps")
+    got = ctypes.c_int()
+    _abi.check(lib.bcg_download_cells(ctx2, _abi.ptr(outbuf), len(outbuf), ctypes.byref(got)), "download")
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - w0
+    t2 = ctypes.c_double(); n2 = ctypes.c_int(); d2 = ctypes.c_int64()
+    lib.bcg_sim_time(sim2, ctypes.byref(t2), ctypes.byref(n2), ctypes.byref(d2))
+    lib.bcg_sim_destroy(sim2)
+    h2d = (n0 * 208 + 9 * 4 * d2.value) / args.steps
+    d2h = (got.value * 208 + 16 * args.steps + 8 * d2.value) / args.steps
+    e2e_value = 0.5 * (n0 + got.value) * args.steps / e2e_s
+
+    # max over ranks
+    vals = torch.tensor([ms, e2e_s, cells_mean * args.steps, 0.5 * (n0 + got.value) * args.steps], dtype=torch.float64, device="cuda")
+    if world > 1:
+        mx = vals.clone()
+        dist.all_reduce(mx[:2], op=dist.ReduceOp.MAX)
+        tot = vals.clone()
+        dist.all_reduce(tot[2:], op=dist.ReduceOp.SUM)
+        ms_max, e2e_max = float(mx[0]), float(mx[1])
+        work, work_e2e = float(tot[2]), float(tot[3])
+    else:
+        ms_max, e2e_max = ms, e2e_s
+        work, work_e2e = cells_mean * args.steps, 0.5 * (n0 + got.value) * args.steps
+
+    value = work / (ms_max / 1e3)
+    e2e_value = work_e2e / e2e_max
+
+    # roofline of the dominant kernel group
+    peak_gbs, peak_src = measured_peaks()
+    dof = mg_dof(p)
+    mg_ms = timers["MG_SOLVE"]
+    mech_ms = timers["MOVE_GROW"]
+    # algorithmic bytes: per finest DOF per V-cycle ~245 B (2*mu1 relaxations
+    # of 24 B, residual/restriction 24 B, prolongation 16 B, x 4/3 for the
+    # coarse levels); per cell-step 280 B of state + 4 B per list entry
+    mg_bytes = 245.0 * dof * args.vcycles
+    k_mean = float(os.environ.get("BCG_K_MEAN", "0")) or None
+    mech_bytes = (280.0 + 4.0 * (k_mean or 2.0)) * cells_mean
+    mg_gbs = mg_bytes / (mg_ms / 1e3) / 1e9 if mg_ms > 0 else 0.0
+    mech_gbs = mech_bytes / (mech_ms / 1e3) / 1e9 if mech_ms > 0 else 0.0
+    if mg_ms >= mech_ms:
+        roof = {"kernel": "multigrid solve (Multigrid::solve, %d V-cycle)" % args.vcycles, "bound": "hbm",
+                "achieved": mg_gbs, "peak": peak_gbs, "unit": "GB/s", "frac": mg_gbs / peak_gbs,
+                "traffic": None, "peak_source": peak_src, "algorithmic_bytes_per_launch": mg_bytes,
+                "launch_ms": mg_ms}
+    else:
+        roof = {"kernel": "k_move_grow (MoveCell+GrowCell)", "bound": "hbm", "achieved": mech_gbs,
+                "peak": peak_gbs, "unit": "GB/s", "frac": mech_gbs / peak_gbs, "traffic": None,
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": mech_bytes, "launch_ms": mech_ms}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            r = cpu_run(p, cells, args.cpu_sample_steps, os.cpu_count() or 1)
+            cpu = {"value": r["cell_steps"], "unit": "cell-steps/s", "cores": r["threads"], "kind": r["kind"],
+                   "sample": r["sample"], "mg_dof_per_s": r["mg_dof_s"]}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port", "sample": "failed: %s" % e}
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "cells": n0, "cells_end": n_end,
+                   "box": [p.box_x, p.box_y, p.box_z], "box_z_agar": p.box_z_agar,
+                   "agar_levels": p.max_levels_mg, "mg_levels": p.mg_levels, "mg_dof": dof,
+                   "vcycles_per_step": args.vcycles, "neighbour_rebuild_every": 100,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (cell records 2x%d MB + fields)" % (n0 * 128 // 2 ** 20)},
+        "mg_dof_per_s": dof * args.vcycles / (mg_ms / 1e3) if mg_ms > 0 else None,
+        "kernel_ms_per_step": timers,
+        "divisions": d_.value,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    a = parse()
+    sys.exit(reference_arm(a) if a.impl == "reference" else b200_arm(a))

@@ -1160,10 +1160,24 @@ static void sweeps(orc_state* s, int nsweeps, env_t** cur, env_t** prev, aga_t**
 /* class Multigrid, Multigrid.cpp:5-981.  Arrays are (nx+1) x (nz+1),
  * x-major; the three species are carbon (C), oxygen (O), acetate (A). */
 #define MI(l, i, k) ((long)(i) * (mg_nz(s, l) + 1) + (k))
-#define AG(l, i, k) s->mgA[l][MI(l, i, k)]
-#define RS(l, i, k) s->mgR[l][MI(l, i, k)]
-#define ER(l, i, k) s->mgE[l][MI(l, i, k)]
-static double ins0(orc_state* s, int i) { return s->inside[IX3(i, 0)]; }
+/* Reads go through the reference's flat index i*(nz+1)+k: on levels with
+ * nz <= 1 the stencils reach k = -1 or k = nz+1, which Array3D maps onto
+ * the neighbouring column (Multigrid.cpp:160-249, 269-467); an index past
+ * either end of the array (undefined in the reference) reads as 0. */
+static aga_t g_zero_aga;
+static aga_t* mg_ref(orc_state* s, aga_t** arr, int l, int i, int k)
+{
+    long n = (long)(mg_nx(s, l) + 1) * (mg_nz(s, l) + 1);
+    long f = MI(l, i, k);
+    if (f < 0 || f >= n) { memset(&g_zero_aga, 0, sizeof(g_zero_aga)); return &g_zero_aga; }
+    return &arr[l][f];
+}
+#define AG(l, i, k) (*mg_ref(s, s->mgA, l, i, k))
+#define RS(l, i, k) (*mg_ref(s, s->mgR, l, i, k))
+#define ER(l, i, k) (*mg_ref(s, s->mgE, l, i, k))
+/* insideColonyDen(i, 0, 0).  The restriction clamps i to BoxX, one x-row
+ * past the array (Multigrid.cpp:279); that row counts as outside (0). */
+static double ins0(orc_state* s, int i) { return i < s->P.box_x ? s->inside[IX3(i, 0)] : 0.0; }
 
 /* relaxationAgarElementwise, Multigrid.cpp:160-249 */
 static void relax_point(orc_state* s, int l, int i, int k, int nx, int nz)

@@ -18,7 +18,14 @@
 #include <stdlib.h>
 #include <math.h>
 #include <algorithm>
+#include <sstream>
+#include <string>
+#include <fstream>
+#include <iostream>
+#include <cmath>
 
+#define private public   /* the harness reads Multigrid's private arrays and dt,
+                            and pads Array3D storage (see ref_init) */
 #include "tools.h"
 #include "Cell.h"
 #include "Constants.h"
@@ -29,7 +36,6 @@
 #include "Cells.h"
 #include "Compute.h"
 #include "Forces.h"
-#define private public   /* the harness reads Multigrid's private arrays and dt */
 #include "Multigrid.h"
 #undef private
 
@@ -145,8 +151,31 @@ void ref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : omp_get_max_thread
 /* Allocate as main() + the top of SimSingleThread do (CellMD3D.cpp:46-142,
  * Simulation.cpp:44-169).  The rough wall consumes BoxX*BoxY rand() draws
  * right after srand(seed), as in the reference when make_wall != 0. */
+/* free the previous scenario (the harness keeps one at a time) */
+static void ref_release(void)
+{
+    if (!S.old_cells) return;
+    delete[] S.old_cells; delete[] S.new_cells;
+    if (S.nbr) { for (int i = 0; i < maxCells; i++) delete[] S.nbr[i]; delete[] S.nbr; }
+    delete S.grid; delete S.Height; delete S.Density; delete S.Density1; delete S.Density2;
+    delete S.WallDensity; delete S.WallDensity1; delete S.WallDensity2; delete S.Env; delete S.oldEnv;
+    for (int i = 0; i < maxLevelsMG; i++) { delete S.FieldAgar[i]; delete S.oldFieldAgar[i]; delete S.FieldWall[i]; delete S.oldFieldWall[i]; }
+    delete[] S.FieldAgar; delete[] S.oldFieldAgar; delete[] S.FieldWall; delete[] S.oldFieldWall;
+    delete S.Normal; delete S.Wall; delete S.Filter; delete S.Filter3D;
+    DoubleArray3D* a3s[] = {S.RoughDensity, S.RoughDensity1, S.RoughDensity2, S.insideColonyDen, S.RoughDensityShiftP,
+        S.RoughDensity1ShiftP, S.RoughDensity2ShiftP, S.DensityShiftP, S.Density1ShiftP, S.Density2ShiftP};
+    for (auto* a : a3s) delete a;
+    DoubleArray2D* a2s[] = {S.RoughWallDensity, S.RoughWallDensity1, S.RoughWallDensity2, S.RoughWallDensityShiftP,
+        S.RoughWallDensity1ShiftP, S.RoughWallDensity2ShiftP, S.WallDensityShiftP, S.WallDensity1ShiftP, S.WallDensity2ShiftP, S.RoughHeight};
+    for (auto* a : a2s) delete a;
+    /* S.mg holds padded arrays (see ref_init) and is not deleted */
+    delete[] S.dividingCells; delete[] S.IDlist;
+    S = RefState();
+}
+
 int ref_init(const bcg_params* p, unsigned seed, int make_wall, int threads)
 {
+    ref_release();
     set_globals(p);
     ref_set_threads(threads);
     srand(seed);
@@ -193,8 +222,36 @@ int ref_init(const bcg_params* p, unsigned seed, int make_wall, int threads)
         S.WallDensityShiftP, S.WallDensity1ShiftP, S.WallDensity2ShiftP, S.WallDensity,
         S.WallDensity1, S.WallDensity2};
     for (auto* a : zero2) a->Initialize(0.0);
+    /* Multigrid::restrictionAgaElementwise clamps its column to BoxX and so
+     * reads insideColonyDen one x-row past the end (Multigrid.cpp:279, 335);
+     * give that row defined storage (0 = outside the colony) so runs are
+     * reproducible.  The array's own elements are unchanged. */
+    {
+        double* padded = new double[(size_t)(BoxX + 1) * BoxY * BoxZ]();
+        delete[] S.insideColonyDen->Data;
+        S.insideColonyDen->Data = padded;
+    }
     S.mg = new Multigrid(maxLevelsMG, p->mg_levels, BoxX, BoxY, BoxZAgar);
     S.mg->setInsideColony(S.insideColonyDen);
+    /* On levels with nz <= 1 the smoother and the transfers index k = -1 and
+     * k = nz+1, which the flat Array3D index maps onto the neighbouring
+     * column, or one element before/after the array at the ends
+     * (Multigrid.cpp:160-249, 269-467).  Give those two elements defined
+     * storage (0) so runs are reproducible; the array itself is unchanged.
+     * The padded arrays are never handed back to Array3D's delete[]
+     * (ref_release leaks the Multigrid). */
+    for (int l = 0; l < p->mg_levels; l++) {
+        AgaArray3D* arrs[3] = {S.mg->Aga[l], S.mg->AgaRes[l], S.mg->AgaErr[l]};
+        for (AgaArray3D* a : arrs) {
+            size_t n = (size_t)a->m_Size.x * a->m_Size.y * a->m_Size.z;
+            LocalAga* base = new LocalAga[n + 2];
+            memcpy(base + 1, a->Data, n * sizeof(LocalAga));
+            memset(base, 0, sizeof(LocalAga));
+            memset(base + n + 1, 0, sizeof(LocalAga));
+            delete[] a->Data;
+            a->Data = base + 1;
+        }
+    }
     S.Wall = new DoubleArray2D(BoxX, BoxY);
     for (int ii = 0; ii < BoxX; ii++)
         for (int jj = 0; jj < BoxY; jj++)

@@ -131,3 +131,22 @@ def test_colony_sweeps_odd_count(gpu):
     mk = bbox_mask(p, orc.bbox())
     for f in ("ENV_CARBON", "OLDENV_CARBON", "ENV_ACETATE", "OLDENV_OXYGEN"):
         assert close(orc.field(F[f]), col.field(f), mask=mk) <= 1e-11, f
+
+
+def test_segmented_smoother_matches_sequential(gpu):
+    """The segmented zebra sweep (default) reproduces the one-thread-per-
+    column sweep to rounding on a grid tall enough to be segmented."""
+    lib = _abi.load()
+    p = params.workload_params("scale_262k")
+    cells = workload_colony("scale_262k", n=20000)
+    out = []
+    for mode in (0, 1):
+        assert lib.bcg_set_relax_mode(mode) == 0
+        col = Colony(p, cells)
+        col.update_density()
+        col.mg_solve(2)
+        out.append([col.field("MG_SOL_" + sp, l) for l in range(3) for sp in ("CARBON", "OXYGEN", "ACETATE")])
+        col.close()
+    lib.bcg_set_relax_mode(1)
+    for a, b in zip(*out):
+        assert close(a, b) <= 1e-14
