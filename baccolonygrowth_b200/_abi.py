@@ -208,6 +208,9 @@ PROTOTYPES = {
     "bcg_sim_time": (_I, [_VP, _PD, _PI, _PI64]),
     "bcg_sim_lineage": (_I, [_VP, _PI, _I, _PI]),
     "bcg_sim_set_step_mode": (_I, [_VP, _I, _I]),
+    "bcg_save_restart": (_I, [ctypes.c_char_p, _D, _D, _VP, _I]),
+    "bcg_load_restart": (_I, [ctypes.c_char_p, _PD, _PD, _VP, _I, _PI]),
+    "bcg_mean_stress": (_I, [_VP, _PD, _PD, _PI64]),
 }
 
 # library entry points outside include/bcg.h, used by tests and the benchmark

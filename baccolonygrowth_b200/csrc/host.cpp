@@ -4,6 +4,7 @@
  * jump-ahead, and the seeded synthetic colony generator.
  */
 #include <math.h>
+#include <stdio.h>
 #include <string.h>
 #include <stdint.h>
 #include <random>
@@ -274,6 +275,37 @@ int bcg_synth_colony(uint64_t seed, int n_target, double width, double height,
     }
     *n = n_target;
     return BCG_OK;
+}
+
+/* SaveCells / LoadCells (InputOutput.cpp:394-448): {double t, double dt,
+ * Cell[N]} raw; the record count follows from the file size. */
+int bcg_save_restart(const char* path, double t, double dt, const bcg_cell* cells, int n)
+{
+    if (!path || n < 0 || (n > 0 && !cells)) return BCG_E_ARG;
+    FILE* f = fopen(path, "wb");
+    if (!f) return BCG_E_ARG;
+    int ok = fwrite(&t, sizeof(double), 1, f) == 1 && fwrite(&dt, sizeof(double), 1, f) == 1 &&
+             (n == 0 || fwrite(cells, sizeof(bcg_cell), (size_t)n, f) == (size_t)n);
+    ok = (fclose(f) == 0) && ok;
+    return ok ? BCG_OK : BCG_E_ARG;
+}
+
+int bcg_load_restart(const char* path, double* t, double* dt, bcg_cell* cells, int capacity, int* n)
+{
+    if (!path || !t || !dt || !n) return BCG_E_ARG;
+    FILE* f = fopen(path, "rb");
+    if (!f) return BCG_E_ARG;
+    fseek(f, 0, SEEK_END);
+    long size = ftell(f);
+    rewind(f);
+    if (size < (long)(2 * sizeof(double))) { fclose(f); return BCG_E_ARG; }
+    long count = (size - 2 * (long)sizeof(double)) / (long)sizeof(bcg_cell);
+    if (fread(t, sizeof(double), 1, f) != 1 || fread(dt, sizeof(double), 1, f) != 1) { fclose(f); return BCG_E_ARG; }
+    *n = (int)count;
+    int m = count < capacity ? (int)count : capacity;
+    if (m > 0 && (!cells || fread(cells, sizeof(bcg_cell), (size_t)m, f) != (size_t)m)) { fclose(f); return BCG_E_ARG; }
+    fclose(f);
+    return count <= capacity ? BCG_OK : BCG_E_ARG;
 }
 
 } // extern "C"

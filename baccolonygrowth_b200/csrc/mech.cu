@@ -612,3 +612,93 @@ extern "C" int bcg_divide(bcg_ctx* c, const float* draws, int n_draw_sets, doubl
     if (n_done) *n_done = 0;
     return BCG_OK;
 }
+
+/* ======================================================================= */
+/* mean_stress (Compute.cpp:18-117)                                         */
+/* ======================================================================= */
+__global__ void k_mean_stress(int n, const CellRec* __restrict__ rec, const int* __restrict__ nbr,
+                              const int* __restrict__ ncount, FieldPtrs fp, MechParams mp,
+                              double* __restrict__ stress, double* __restrict__ fnet,
+                              unsigned long long* fcw_count, DevStatus* st)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int near = 0;
+    if (i < n) {
+        Cst c = load_cst(&rec[i]);
+        double V = c.L * BCG_PI * c.R * c.R + 4.0 / 3.0 * BCG_PI * c.R * c.R * c.R;
+        V3 CM = avg_pq(c.p, c.q);
+        int xi, yi, zi;
+        if (box_address(CM, mp, xi, yi, zi) < 0) { dev_error(st, BCG_E_OUT_OF_GRID, i); xi = 0; yi = 0; }
+        double sxx = 0, syy = 0, szz = 0;
+        V3 Fn = mk(0, 0, 0);
+        const int* list = nbr + (size_t)i * mp.kmax;
+        int cnt = ncount[i];
+        for (int j = 0; j < cnt; j++) {
+            Cst b = load_cst(&rec[list[j]]);
+            V3 F, r;
+            if (!pair_force(c, CM, b, mp, F, r)) { F = mk(0, 0, 0); continue; }
+            Fn = add3(Fn, F);
+            r = sub3(r, CM);
+            sxx -= F.x * r.x; syy -= F.y * r.y; szz -= F.z * r.z;
+        }
+        if (dmin_(c.q.z, c.p.z) < 1.2 * c.R) {
+            near = 1;
+            double wall_z = fp.wall[xi * mp.box_y + yi];
+            V3 r1, r2, sf = mk(0, 0, 0), df = mk(0, 0, 0);
+            V3 F1 = wall_locus(c, CM, c.p, wall_z, mp, r1, sf, df);
+            V3 F2 = wall_locus(c, CM, c.q, wall_z, mp, r2, sf, df);
+            Fn = add3(Fn, F1);
+            r1 = sub3(r1, CM);
+            sxx -= F1.x * r1.x; syy -= F1.y * r1.y; szz -= F1.z * r1.z;
+            Fn = add3(Fn, F2);
+            r2 = sub3(r2, CM);
+            sxx -= F2.x * r2.x; syy -= F2.y * r2.y; szz -= F2.z * r2.z;
+        }
+        V3 F, T;
+        surface_tension(c, CM, fp, mp, F, T);
+        Fn = add3(Fn, F);
+        V3 r = sub3(c.p, CM); r.z += c.R;
+        V3 r2 = sub3(c.q, CM); r2.z += c.R;
+        sxx -= F.x * r.x * 0.5 - F.x * r2.x * 0.5;
+        syy -= F.y * r.y * 0.5 - F.y * r2.y * 0.5;
+        szz -= F.z * r.z * 0.5 - F.z * r2.z * 0.5;
+        sxx /= V; syy /= V; szz /= V;
+        double rr, tt;
+        double Lcm = sqrt(CM.x * CM.x + CM.y * CM.y);
+        if (Lcm > DBL_EPSILON) {
+            V3 uv = scl3(CM, 1.0 / Lcm);
+            rr = sxx * uv.x + syy * uv.y;
+            tt = -sxx * uv.y + syy * uv.x;
+        } else { rr = (sxx + syy); tt = 0.0; }
+        stress[5 * (size_t)i + 0] = sxx; stress[5 * (size_t)i + 1] = syy; stress[5 * (size_t)i + 2] = szz;
+        stress[5 * (size_t)i + 3] = rr; stress[5 * (size_t)i + 4] = tt;
+        if (fnet) { fnet[3 * (size_t)i] = Fn.x; fnet[3 * (size_t)i + 1] = Fn.y; fnet[3 * (size_t)i + 2] = Fn.z; }
+    }
+    unsigned long long v = near;
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(fcw_count, v);
+}
+
+extern "C" int bcg_mean_stress(bcg_ctx* c, double* stress, double* fnet, int64_t* fcw_calls)
+{
+    if (!c || !stress) return BCG_E_ARG;
+    int n = c->n;
+    BCG_CUDA_TRY(cudaMemsetAsync(c->fcw_count, 0, sizeof(unsigned long long), c->stream));
+    if (n > 0) {
+        double *ds = nullptr, *df = nullptr;
+        BCG_CUDA_TRY(cudaMallocAsync((void**)&ds, sizeof(double) * 5 * (size_t)n, c->stream));
+        if (fnet) BCG_CUDA_TRY(cudaMallocAsync((void**)&df, sizeof(double) * 3 * (size_t)n, c->stream));
+        k_mean_stress<<<(n + 127) / 128, 128, 0, c->stream>>>(n, c->rec[c->cur], c->nbr, c->ncount, field_ptrs(c),
+                                                              mech_params(c), ds, df, c->fcw_count, c->status);
+        c->launches++;
+        BCG_CUDA_TRY(cudaMemcpyAsync(stress, ds, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+        if (fnet) BCG_CUDA_TRY(cudaMemcpyAsync(fnet, df, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+        BCG_CUDA_TRY(cudaFreeAsync(ds, c->stream));
+        if (df) BCG_CUDA_TRY(cudaFreeAsync(df, c->stream));
+    }
+    unsigned long long h = 0;
+    BCG_CUDA_TRY(cudaMemcpyAsync(&h, c->fcw_count, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    int rc = ctx_check_status(c);
+    if (fcw_calls) *fcw_calls = (int64_t)h;
+    return rc;
+}

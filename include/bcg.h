@@ -320,6 +320,18 @@ int bcg_synth_colony(uint64_t seed, int n_target, double width, double height,
                      double l_divide, double div_phase_spread,
                      bcg_cell* out, int capacity, int* n);
 
+/* Binary restart files in the reference's format: double t, double dt,
+ * then the Cell records (SaveCells / LoadCells, InputOutput.cpp:394-448).
+ * bcg_load_restart returns the record count in *n (at most capacity). */
+int bcg_save_restart(const char* path, double t, double dt, const bcg_cell* cells, int n);
+int bcg_load_restart(const char* path, double* t, double* dt, bcg_cell* cells, int capacity, int* n);
+
+/* mean_stress for every cell (Compute.cpp:18-117, called on output steps at
+ * Simulation.cpp:316-327): stress receives 5 doubles per cell (xx, yy, zz,
+ * rr, tt of the Tensor), fnet (optional) 3 per cell; *fcw_calls = the
+ * rand() draws the reference makes here (one per wall-near cell). */
+int bcg_mean_stress(bcg_ctx* ctx, double* stress, double* fnet, int64_t* fcw_calls);
+
 /* ------------------------------------------------------------------ */
 /* C++ host loop (rewrite of SimSingleThread, Simulation.cpp:42-434)     */
 /* ------------------------------------------------------------------ */

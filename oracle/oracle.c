@@ -1621,6 +1621,53 @@ void orc_colony_sweeps(orc_state* s, int nsweeps, int count0)
     sweeps(s, nsweeps, &cur, &prev, &ca, &pa, &cw, &pw, &count);
 }
 
+/* mean_stress, Compute.cpp:18-117, for every cell in id order (the output
+ * step, Simulation.cpp:320-326); returns the rand() draws made. */
+long long orc_mean_stress(orc_state* s, double* stress, double* fnet)
+{
+    long long r0 = s->rand_calls;
+    for (int i = 0; i < s->N; i++) {
+        const bcg_cell* c = &s->oldc[i];
+        double V = c->length * PI * c->radius * c->radius + 4.0 / 3.0 * PI * c->radius * c->radius * c->radius;
+        int xi, yi, zi;
+        get_address(s, avg(c), &xi, &yi, &zi);
+        const int* nb = nbr_row(s, i);
+        double sxx = 0, syy = 0, szz = 0;
+        V3 Fn = v3(0, 0, 0), CM = avg(c), F, r, F2, r2, df, sf;
+        double d;
+        for (int k = 1; k < nb[0] + 1; k++) {
+            F_cc(s, c, &s->oldc[nb[k]], &F, &r, &d);
+            Fn = vsum(Fn, F);
+            r = vdiff(r, CM);
+            sxx -= F.x * r.x; syy -= F.y * r.y; szz -= F.z * r.z;
+        }
+        if (dmin(c->q.z, c->p.z) < 1.2 * c->radius) {
+            double wall_y = s->wall[xi * s->P.box_y + yi];
+            df = v3(0, 0, 0); sf = v3(0, 0, 0);
+            F_cw(s, c, wall_y, &F, &F2, &r, &r2, &df, &sf);
+            Fn = vsum(Fn, F); r = vdiff(r, CM);
+            sxx -= F.x * r.x; syy -= F.y * r.y; szz -= F.z * r.z;
+            Fn = vsum(Fn, F2); r2 = vdiff(r2, CM);
+            sxx -= F2.x * r2.x; syy -= F2.y * r2.y; szz -= F2.z * r2.z;
+        }
+        V3 T;
+        F_surf(s, c, &F, &T);
+        Fn = vsum(Fn, F);
+        r = vdiff(c->p, CM); r.z += c->radius;
+        r2 = vdiff(c->q, CM); r2.z += c->radius;
+        sxx -= F.x * r.x * 0.5 - F.x * r2.x * 0.5;
+        syy -= F.y * r.y * 0.5 - F.y * r2.y * 0.5;
+        szz -= F.z * r.z * 0.5 - F.z * r2.z * 0.5;
+        sxx /= V; syy /= V; szz /= V;
+        double rr, tt, Lcm = sqrt(CM.x * CM.x + CM.y * CM.y);
+        if (Lcm > DBL_EPSILON) { V3 uv = vscale(CM, 1.0 / Lcm); rr = sxx * uv.x + syy * uv.y; tt = -sxx * uv.y + syy * uv.x; }
+        else { rr = (sxx + syy); tt = 0.0; }
+        stress[5 * i] = sxx; stress[5 * i + 1] = syy; stress[5 * i + 2] = szz; stress[5 * i + 3] = rr; stress[5 * i + 4] = tt;
+        if (fnet) { fnet[3 * i] = Fn.x; fnet[3 * i + 1] = Fn.y; fnet[3 * i + 2] = Fn.z; }
+    }
+    return s->rand_calls - r0;
+}
+
 /* One iteration of the while loop, Simulation.cpp:256-430, without output. */
 int orc_loop_step(orc_state* s, int* lineage)
 {

@@ -39,6 +39,7 @@ void orc_nutrient_update(orc_state* s, int n);
 void orc_mg_solve(orc_state* s, int vcycles, double dt);
 void orc_colony_sweeps(orc_state* s, int sweeps, int count0);
 int  orc_loop_step(orc_state* s, int* lineage);
+long long orc_mean_stress(orc_state* s, double* stress, double* fnet);
 double orc_time(orc_state* s);
 
 #ifdef __cplusplus

@@ -440,6 +440,21 @@ int ref_loop_step(int* lineage)
     return done;
 }
 
+/* mean_stress for every cell in id order, as on an output step
+ * (Simulation.cpp:320-326); returns the rand() draws made */
+long long ref_mean_stress(double* stress, double* fnet)
+{
+    long long r0 = g_rand_calls;
+    Tensor T;
+    DoubleCoord F;
+    for (int i = 0; i < S.N; i++) {
+        mean_stress(S.old_cells[i], S.old_cells, S.nbr[i], *S.grid, *S.Wall, *S.Height, *S.Normal, T, F);
+        stress[5 * i] = T.xx; stress[5 * i + 1] = T.yy; stress[5 * i + 2] = T.zz; stress[5 * i + 3] = T.rr; stress[5 * i + 4] = T.tt;
+        if (fnet) { fnet[3 * i] = F.x; fnet[3 * i + 1] = F.y; fnet[3 * i + 2] = F.z; }
+    }
+    return g_rand_calls - r0;
+}
+
 double ref_time(void) { return S.t; }
 void ref_bbox(int* mnx, int* mxx, int* mxz) { *mnx = S.minx; *mxx = S.maxx; *mxz = S.maxz; }
 void ref_set_bbox(int mnx, int mxx, int mxz) { S.minx = mnx; S.maxx = mxx; S.maxz = mxz; }

@@ -65,6 +65,7 @@ def oracle_lib():
         _proto(lib, "orc_colony_sweeps", None, [_VP, ctypes.c_int, ctypes.c_int])
         _proto(lib, "orc_loop_step", ctypes.c_int, [_VP, _PI])
         _proto(lib, "orc_time", ctypes.c_double, [_VP])
+        _proto(lib, "orc_mean_stress", ctypes.c_longlong, [_VP, _PD, _PD])
         _oracle = lib
     return _oracle
 
@@ -100,6 +101,7 @@ def ref_lib():
         _proto(lib, "ref_mg_solve", None, [ctypes.c_int, ctypes.c_double])
         _proto(lib, "ref_loop_step", ctypes.c_int, [_PI])
         _proto(lib, "ref_time", ctypes.c_double, [])
+        _proto(lib, "ref_mean_stress", ctypes.c_longlong, [_PD, _PD])
         _ref = lib
     return _ref
 
@@ -233,6 +235,11 @@ class Oracle(_Model):
     def time(self):
         return self.lib.orc_time(self.h)
 
+    def mean_stress(self):
+        st = np.zeros(5 * self.n_cells()); fn = np.zeros(3 * self.n_cells())
+        calls = self.lib.orc_mean_stress(self.h, _abi.ptr(st, ctypes.c_double), _abi.ptr(fn, ctypes.c_double))
+        return st.reshape(-1, 5), fn.reshape(-1, 3), calls
+
 
 class Reference(_Model):
     """The reference compiled from its sources (one process-wide instance)."""
@@ -309,3 +316,8 @@ class Reference(_Model):
 
     def time(self):
         return self.lib.ref_time()
+
+    def mean_stress(self):
+        st = np.zeros(5 * self.n_cells()); fn = np.zeros(3 * self.n_cells())
+        calls = self.lib.ref_mean_stress(_abi.ptr(st, ctypes.c_double), _abi.ptr(fn, ctypes.c_double))
+        return st.reshape(-1, 5), fn.reshape(-1, 3), calls

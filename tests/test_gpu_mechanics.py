@@ -134,3 +134,19 @@ def test_out_of_grid_is_reported(gpu):
     cells["q"][5, 0] = 2.0
     col.upload(cells)
     col.rebuild_neighbours()
+
+
+def test_mean_stress(gpu):
+    import ctypes
+    p, orc, col, rng = setup_pair(n=2048)
+    col.rebuild_neighbours()
+    orc.step(p.dt, 0.0)
+    col.step(p.dt, 0.0, rng)
+    st_o, fn_o, calls_o = orc.mean_stress()
+    n = col.n_cells()
+    st = np.zeros(5 * n); fn = np.zeros(3 * n); calls = ctypes.c_int64()
+    lib = _abi.load()
+    assert lib.bcg_mean_stress(col.h, _abi.ptr(st, ctypes.c_double), _abi.ptr(fn, ctypes.c_double), ctypes.byref(calls)) == 0
+    assert calls.value == calls_o
+    assert rel_err(st_o.reshape(-1), st) <= 1e-10
+    assert rel_err(fn_o.reshape(-1), fn) <= 1e-10

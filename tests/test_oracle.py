@@ -133,3 +133,35 @@ def test_oracle_matches_reference_live_loop():
         if a.size == box.size:
             a, b = a[box], b[box]
         assert np.array_equal(a, b), f
+
+
+@needs_ref
+def test_oracle_mean_stress_matches_reference():
+    p = params.workload_params("small_4k")
+    cells = workload_colony("small_4k", n=1024)
+    ref, orc = ck.Reference(p, seed=99), ck.Oracle(p, seed=99)
+    for m in (ref, orc):
+        m.load(cells)
+        m.update_height()
+        m.rebuild()
+        m.step(p.dt, 0.0)     # some contacts and velocities
+    a, b = ref.mean_stress(), orc.mean_stress()
+    assert a[2] == b[2]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_restart_roundtrip(tmp_path):
+    import ctypes
+    lib = _abi.load()
+    cells = workload_colony("small_4k", n=300)
+    path = str(tmp_path / "8.txt").encode()
+    assert lib.bcg_save_restart(path, 9.001, 1e-4, _abi.ptr(cells), len(cells)) == 0
+    out = np.zeros(400, dtype=_abi.CELL_DTYPE)
+    t, dt, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    assert lib.bcg_load_restart(path, ctypes.byref(t), ctypes.byref(dt), _abi.ptr(out), 400, ctypes.byref(n)) == 0
+    assert (t.value, dt.value, n.value) == (9.001, 1e-4, 300)
+    assert out[:300].tobytes() == cells.tobytes()
+    # the file is exactly the reference's SaveCells layout: two doubles then 208-byte records
+    raw = open(path.decode(), "rb").read()
+    assert len(raw) == 16 + 208 * 300
+    assert np.frombuffer(raw[:16], dtype=np.float64).tolist() == [9.001, 1e-4]
