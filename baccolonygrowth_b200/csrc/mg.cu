@@ -12,6 +12,7 @@
  */
 #include "ctx.cuh"
 #include "mg.cuh"
+#include <string.h>
 
 __device__ __forceinline__ double dmaxd(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double dmind(double a, double b) { return a < b ? a : b; }
@@ -22,12 +23,13 @@ __device__ __forceinline__ double dmind(double a, double b) { return a < b ? a :
  * nz <= 1 the stencils reach k = -1 or k = nz+1, which the reference's
  * Array3D maps onto the neighbouring column; an index past either end of
  * the array (undefined in the reference) reads as 0.  In range it is AT. */
-__device__ __forceinline__ double at_ref(const double* a, const MgLvl& L, int i, int k)
+template <class P, class LV>
+__device__ __forceinline__ P at_ref(const P* a, const LV& L, int i, int k)
 {
     if (k >= 0 && k <= L.nz) return AT(a, L, i, k);
     long f = (long)i * (L.nz + 1) + k;
     long n = (long)(L.nx + 1) * (L.nz + 1);
-    if (f < 0 || f >= n) return 0.0;
+    if (f < 0 || f >= n) return P(0);
     int i2 = (int)(f / (L.nz + 1)), k2 = (int)(f % (L.nz + 1));
     return AT(a, L, i2, k2);
 }
@@ -54,22 +56,33 @@ MgLvl mg_lvl(const bcg_ctx* c, int l)
     return v;
 }
 
+MgLvlF mg_lvl_f(const bcg_ctx* c, int l)
+{
+    MgLvlF v;
+    const MgLevel& L = c->mg[l];
+    v.nx = L.nx; v.nz = L.nz; v.pitch = L.pitch;
+    for (int s = 0; s < 3; s++) { v.s[s] = L.sol[s]; v.r[s] = L.resf[s]; v.e[s] = L.errf[s]; }
+    return v;
+}
+
 /* ------------------------------------------------------------------------ */
 /* relaxationAgarElementwise, Multigrid.cpp:160-249, for one species        */
 /* ------------------------------------------------------------------------ */
-__device__ __forceinline__ void relax_point(const MgConst& m, const MgLvl& L, int l, int sp, int i, int k,
-                                            const double* __restrict__ inside0, double& e_below, bool have_below)
+template <class T>
+__device__ __forceinline__ void relax_point(const MgConst& m, const MgLvlT<T>& L, int l, int sp, int i, int k,
+                                            const double* __restrict__ inside0, T& e_below, bool have_below)
 {
     const int nx = L.nx, nz = L.nz;
-    const double h2 = m.bl2 * (double)(1 << (2 * l));
-    const double dt = m.dt, D = m.D[sp];
-    double* E = L.e[sp];
-    const double* R = L.r[sp];
+    const T h2 = (T)(m.bl2 * (double)(1 << (2 * l)));
+    const T dt = (T)m.dt, D = (T)m.D[sp];
+    const T half = (T)0.5;
+    T* E = L.e[sp];
+    const T* R = L.r[sp];
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
-    double r = AT(R, L, i, k);
-    double e_dn = have_below ? e_below : (k > 0 ? AT(E, L, i, k - 1) : 0.0);
-    double out;
+    T r = AT(R, L, i, k);
+    T e_dn = have_below ? e_below : (k > 0 ? AT(E, L, i, k - 1) : T(0));
+    T out;
     bool write = true;
     if (k == 0) {
         int d = 1 << l;
@@ -80,16 +93,16 @@ __device__ __forceinline__ void relax_point(const MgConst& m, const MgLvl& L, in
             if (top_levels) {
                 if (oxy) out = r;
                 else {
-                    double s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
-                    double up = at_ref(E, L, i, 1);
+                    T s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
+                    T up = at_ref(E, L, i, 1);
                     out = (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
                 }
             } else write = false;
         } else {
             if (oxy) out = r;
             else {
-                double up = at_ref(E, L, i, 1), xm = AT(E, L, i - 1, 0), xp = AT(E, L, i + 1, 0);
-                out = (r * h2 / dt / D + up + 0.5 * xm + 0.5 * xp) / (h2 / dt / D + 2);
+                T up = at_ref(E, L, i, 1), xm = AT(E, L, i - 1, 0), xp = AT(E, L, i + 1, 0);
+                out = (r * h2 / dt / D + up + half * xm + half * xp) / (h2 / dt / D + 2);
             }
         }
     } else if (k == nz) {
@@ -97,40 +110,91 @@ __device__ __forceinline__ void relax_point(const MgConst& m, const MgLvl& L, in
             if (i == 0 || i == nx) {
                 if (oxy) out = r;
                 else {
-                    double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                    T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
                     out = (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
                 }
             } else {
-                double xp = AT(E, L, i + 1, k), xm = AT(E, L, i - 1, k);
-                out = (r * h2 / dt / D + e_dn + 0.5 * xp + 0.5 * xm) / (h2 / dt / D + 2);
+                T xp = AT(E, L, i + 1, k), xm = AT(E, L, i - 1, k);
+                out = (r * h2 / dt / D + e_dn + half * xp + half * xm) / (h2 / dt / D + 2);
             }
         } else write = false;
     } else if (i == 0 || i == nx) {
         if (top_levels) {
             if (oxy) out = r;
             else {
-                double up = AT(E, L, i, k + 1);
-                double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
-                out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + s1) / (h2 / dt / D + 2);
+                T up = AT(E, L, i, k + 1);
+                T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                out = (r * h2 / dt / D + half * e_dn + half * up + s1) / (h2 / dt / D + 2);
             }
         } else write = false;
     } else {
-        double up = AT(E, L, i, k + 1), xm = AT(E, L, i - 1, k), xp = AT(E, L, i + 1, k);
-        out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + 0.5 * xm + 0.5 * xp) / (h2 / dt / D + 2);
+        T up = AT(E, L, i, k + 1), xm = AT(E, L, i - 1, k), xp = AT(E, L, i + 1, k);
+        out = (r * h2 / dt / D + half * e_dn + half * up + half * xm + half * xp) / (h2 / dt / D + 2);
     }
     if (write) AT(E, L, i, k) = out;
     e_below = write ? out : AT(E, L, i, k);
 }
 
+/* Value the smoother would give point (i, k) of species sp (no write), and
+ * whether the point is relaxed and how its update is scaled:
+ * kind 0 = not relaxed, 1 = Dirichlet (E = R), 2 = E = (R c + N(E)) / (c + 2). */
+template <class T>
+__device__ __forceinline__ double relax_eval(const MgConst& m, const MgLvlT<T>& L, const double* __restrict__ R64,
+                                             int l, int sp, int i, int k,
+                                             const double* __restrict__ inside0, int& kind, double& cfac)
+{
+    const int nx = L.nx, nz = L.nz;
+    const double h2 = m.bl2 * (double)(1 << (2 * l));
+    const double dt = m.dt, D = m.D[sp];
+    const T* E = L.e[sp];
+    const double r = AT(R64, L, i, k);
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    cfac = h2 / dt / D;
+    kind = 2;
+    if (k == 0) {
+        int d = 1 << l;
+        int i0 = (i - nx / 2) * d + m.box_x / 2;
+        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+        if (inside0[(size_t)i0 * m.box_z] > 0) { kind = 1; return r; }
+        if (i == 0 || i == nx) {
+            if (!top_levels) { kind = 0; return 0.0; }
+            if (oxy) { kind = 1; return r; }
+            double s1 = (i == 0) ? (double)AT(E, L, i + 1, 0) : (double)AT(E, L, i - 1, 0);
+            return (r * h2 / dt / D + (s1 + (double)at_ref(E, L, i, 1))) / (h2 / dt / D + 2);
+        }
+        if (oxy) { kind = 1; return r; }
+        return (r * h2 / dt / D + (double)at_ref(E, L, i, 1) + 0.5 * (double)AT(E, L, i - 1, 0) + 0.5 * (double)AT(E, L, i + 1, 0)) / (h2 / dt / D + 2);
+    }
+    const double e_dn = (double)AT(E, L, i, k - 1);
+    if (k == nz) {
+        if (!top_levels) { kind = 0; return 0.0; }
+        if (i == 0 || i == nx) {
+            if (oxy) { kind = 1; return r; }
+            double s1 = (i == 0) ? (double)AT(E, L, i + 1, k) : (double)AT(E, L, i - 1, k);
+            return (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
+        }
+        return (r * h2 / dt / D + e_dn + 0.5 * (double)AT(E, L, i + 1, k) + 0.5 * (double)AT(E, L, i - 1, k)) / (h2 / dt / D + 2);
+    }
+    if (i == 0 || i == nx) {
+        if (!top_levels) { kind = 0; return 0.0; }
+        if (oxy) { kind = 1; return r; }
+        double s1 = (i == 0) ? (double)AT(E, L, i + 1, k) : (double)AT(E, L, i - 1, k);
+        return (r * h2 / dt / D + 0.5 * e_dn + 0.5 * (double)AT(E, L, i, k + 1) + s1) / (h2 / dt / D + 2);
+    }
+    return (r * h2 / dt / D + 0.5 * e_dn + 0.5 * (double)AT(E, L, i, k + 1) + 0.5 * (double)AT(E, L, i - 1, k) + 0.5 * (double)AT(E, L, i + 1, k)) / (h2 / dt / D + 2);
+}
+
 /* one thread per (column of the given parity, species), bottom to top */
-__global__ void k_mg_relax(MgConst m, MgLvl L, int l, int parity, const double* __restrict__ inside0)
+template <class T>
+__global__ void k_mg_relax(MgConst m, MgLvlT<T> L, int l, int parity, const double* __restrict__ inside0)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int ncol = (L.nx + 1 - parity + 1) / 2;
     int sp = blockIdx.y;
     if (t >= ncol) return;
     int i = 2 * t + parity;
-    double below = 0.0;
+    T below = T(0);
     for (int k = 0; k <= L.nz; k++) relax_point(m, L, l, sp, i, k, inside0, below, k > 0);
 }
 
@@ -147,7 +211,8 @@ __global__ void k_mg_relax(MgConst m, MgLvl L, int l, int parity, const double* 
  * every thread reads them before any thread writes.  All segments of a
  * column live in one block: blockDim = (32 columns, nseg segments). */
 #define RELAX_WARM 32
-__global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l, int parity, int seg_len,
+template <class T>
+__global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvlT<T> L, int l, int parity, int seg_len,
                                                       const double* __restrict__ inside0)
 {
     const int ncol = (L.nx + 1 - parity + 1) / 2;
@@ -160,10 +225,10 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l,
     const int k_begin = seg * seg_len;
     const int k_end = min(k_begin + seg_len, nz + 1);
     const int k_start = max(0, k_begin - RELAX_WARM);
-    double* E = L.e[sp];
+    T* E = L.e[sp];
     /* pre-sweep values this thread needs from rows other threads write */
-    double up_w[RELAX_WARM + 1];
-    double below = 0.0, above_end = 0.0;
+    T up_w[RELAX_WARM + 1];
+    T below = T(0), above_end = T(0);
     if (active && k_begin <= nz) {
         for (int k = k_start; k < k_begin; k++) up_w[k - k_start] = AT(E, L, i, k + 1);
         if (k_start > 0) below = AT(E, L, i, k_start - 1);
@@ -171,20 +236,21 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l,
     }
     __syncthreads();
     if (!active || k_begin > nz) return;
-    const double h2 = m.bl2 * (double)(1 << (2 * l));
-    const double dt = m.dt, D = m.D[sp];
-    const double* R = L.r[sp];
+    const T h2 = (T)(m.bl2 * (double)(1 << (2 * l)));
+    const T dt = (T)m.dt, D = (T)m.D[sp];
+    const T half = (T)0.5;
+    const T* R = L.r[sp];
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
     const int nx = L.nx;
     const bool side = (i == 0 || i == nx);
-    double xm_, xp_;
+    T xm_, xp_;
     for (int k = k_start; k < k_end; k++) {
         const bool warm = k < k_begin;
-        double r = AT(R, L, i, k);
-        double up = (k < nz) ? (warm ? up_w[k - k_start] : (k + 1 == k_end ? above_end : AT(E, L, i, k + 1))) : 0.0;
-        double e_dn = below;
-        double out = 0.0;
+        T r = AT(R, L, i, k);
+        T up = (k < nz) ? (warm ? up_w[k - k_start] : (k + 1 == k_end ? above_end : AT(E, L, i, k + 1))) : T(0);
+        T e_dn = below;
+        T out = T(0);
         bool write = true;
         if (k == 0) {
             int d = 1 << l;
@@ -195,7 +261,7 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l,
                 if (top_levels) {
                     if (oxy) out = r;
                     else {
-                        double s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
+                        T s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
                         out = (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
                     }
                 } else write = false;
@@ -203,7 +269,7 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l,
                 if (oxy) out = r;
                 else {
                     xm_ = AT(E, L, i - 1, 0); xp_ = AT(E, L, i + 1, 0);
-                    out = (r * h2 / dt / D + up + 0.5 * xm_ + 0.5 * xp_) / (h2 / dt / D + 2);
+                    out = (r * h2 / dt / D + up + half * xm_ + half * xp_) / (h2 / dt / D + 2);
                 }
             }
         } else if (k == nz) {
@@ -211,25 +277,25 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l,
                 if (side) {
                     if (oxy) out = r;
                     else {
-                        double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                        T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
                         out = (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
                     }
                 } else {
                     xp_ = AT(E, L, i + 1, k); xm_ = AT(E, L, i - 1, k);
-                    out = (r * h2 / dt / D + e_dn + 0.5 * xp_ + 0.5 * xm_) / (h2 / dt / D + 2);
+                    out = (r * h2 / dt / D + e_dn + half * xp_ + half * xm_) / (h2 / dt / D + 2);
                 }
             } else write = false;
         } else if (side) {
             if (top_levels) {
                 if (oxy) out = r;
                 else {
-                    double s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
-                    out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + s1) / (h2 / dt / D + 2);
+                    T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
+                    out = (r * h2 / dt / D + half * e_dn + half * up + s1) / (h2 / dt / D + 2);
                 }
             } else write = false;
         } else {
             xm_ = AT(E, L, i - 1, k); xp_ = AT(E, L, i + 1, k);
-            out = (r * h2 / dt / D + 0.5 * e_dn + 0.5 * up + 0.5 * xm_ + 0.5 * xp_) / (h2 / dt / D + 2);
+            out = (r * h2 / dt / D + half * e_dn + half * up + half * xm_ + half * xp_) / (h2 / dt / D + 2);
         }
         /* points that are not relaxed keep their value; those columns and
          * rows (composite edges) are written by no thread in this sweep */
@@ -242,7 +308,8 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvl L, int l,
 /* All mu2 relaxations of a small (coarsest) level in one block: the sweep
  * order (even columns, then odd, each bottom to top) is kept with a block
  * barrier between half-sweeps. */
-__global__ void __launch_bounds__(1024) k_mg_relax_coarse(MgConst m, MgLvl L, int l, int sweeps,
+template <class T>
+__global__ void __launch_bounds__(1024) k_mg_relax_coarse(MgConst m, MgLvlT<T> L, int l, int sweeps,
                                                           const double* __restrict__ inside0)
 {
     const int nx = L.nx;
@@ -253,7 +320,7 @@ __global__ void __launch_bounds__(1024) k_mg_relax_coarse(MgConst m, MgLvl L, in
             for (int w = threadIdx.x; w < 3 * ncol; w += blockDim.x) {
                 int sp = w / ncol, t = w % ncol;
                 int i = 2 * t + parity;
-                double below = 0.0;
+                T below = T(0);
                 for (int k = 0; k <= L.nz; k++) relax_point(m, L, l, sp, i, k, inside0, below, k > 0);
             }
             __syncthreads();
@@ -263,7 +330,8 @@ __global__ void __launch_bounds__(1024) k_mg_relax_coarse(MgConst m, MgLvl L, in
 /* ------------------------------------------------------------------------ */
 /* restrictionAgaElementwise, Multigrid.cpp:269-405 (level l from l-1)       */
 /* ------------------------------------------------------------------------ */
-__global__ void k_mg_restrict(MgConst m, MgLvl Lc, MgLvl Lf, int l, const double* __restrict__ inside0)
+template <class T>
+__global__ void k_mg_restrict(MgConst m, MgLvlT<T> Lc, MgLvlT<T> Lf, int l, const double* __restrict__ inside0)
 {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     int sp = blockIdx.y;
@@ -274,35 +342,36 @@ __global__ void k_mg_restrict(MgConst m, MgLvl Lc, MgLvl Lf, int l, const double
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d < X ? X * d0 / d : X;
     int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
-    double h2 = m.bl2 * d * d;
-    const double dt = m.dt, D = m.D[sp];
+    const T h2 = (T)(m.bl2 * d * d);
+    const T dt = (T)m.dt, D = (T)m.D[sp];
+    const T half = (T)0.5;
     const bool oxy = sp == 1;
     int i0 = (i - nx / 2) * d + X / 2;
     i0 = i0 < 0 ? 0 : (i0 > X ? X : i0);   /* clamped to BoxX as in the reference */
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
-    const double* EP = Lf.e[sp];
-    const double* RP = Lf.r[sp];
+    const T* EP = Lf.e[sp];
+    const T* RP = Lf.r[sp];
     const double* AP = Lf.s[sp];
     const double* AL = Lc.s[sp];
-    double* R = &AT(Lc.r[sp], Lc, i, k);
+    T* R = &AT(Lc.r[sp], Lc, i, k);
 #define EPv(a, b) at_ref(EP, Lf, a, b)
 #define RPv(a, b) at_ref(RP, Lf, a, b)
-#define APv(a, b) at_ref(AP, Lf, a, b)
-#define ALv(a, b) at_ref(AL, Lc, a, b)
+#define APv(a, b) ((T)at_ref(AP, Lf, a, b))
+#define ALv(a, b) ((T)at_ref(AL, Lc, a, b))
     if (i == 0 || i == nx || k == nz) {
         if (l >= m.A) {
             if (k == nz && (i > 0) && (i < nx)) {
                 /* carbon uses (ip,kp), oxygen/acetate (2i,2k): equal for l >= A */
-                *R = (RPv(ip, kp) + 0.5 * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + 2 * EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+                *R = (RPv(ip, kp) + half * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + 2 * EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
             } else {
                 int sx = (i == 0) ? 1 : -1;
                 if (oxy) *R = RPv(ip, kp) - EPv(ip, kp);
                 else if (k == 0)
-                    *R = (RPv(ip, kp) + 0.5 * (2 * EPv(ip + sx, kp) + 2 * EPv(ip, kp + 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+                    *R = (RPv(ip, kp) + half * (2 * EPv(ip + sx, kp) + 2 * EPv(ip, kp + 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
                 else if (k == nz)
-                    *R = (RPv(ip, kp) + 0.5 * (2 * EPv(ip + sx, kp) + 2 * EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+                    *R = (RPv(ip, kp) + half * (2 * EPv(ip + sx, kp) + 2 * EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
                 else
-                    *R = (RPv(ip, kp) + 0.5 * (2 * EPv(ip + sx, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
+                    *R = (RPv(ip, kp) + half * (2 * EPv(ip + sx, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt * 4 / h2 - EPv(ip, kp)) / 2;
             }
         }
     } else if (k == 0) {
@@ -310,28 +379,28 @@ __global__ void k_mg_restrict(MgConst m, MgLvl Lc, MgLvl Lf, int l, const double
          * it counts as outside the colony */
         if (i0 < X && inside0[(size_t)i0 * m.box_z] > 0) *R = 0;
         else if (ip > 0 && ip < nxp) {
-            if (oxy) *R = (RPv(ip, 0) - EPv(ip, 0)) * 0.5;
-            else *R = (RPv(ip, 0) + 0.5 * (EPv(ip + 1, 0) + EPv(ip - 1, 0) + 2 * EPv(ip, 1) - 4 * EPv(ip, 0)) * D * dt * 4 / h2 - EPv(ip, 0)) * 0.5;
+            if (oxy) *R = (RPv(ip, 0) - EPv(ip, 0)) * half;
+            else *R = (RPv(ip, 0) + half * (EPv(ip + 1, 0) + EPv(ip - 1, 0) + 2 * EPv(ip, 1) - 4 * EPv(ip, 0)) * D * dt * 4 / h2 - EPv(ip, 0)) * half;
         } else if ((l < m.A) && (ip >= 0 && ip <= nxp) && ((ip == 0) || (ip == nxp))) {
-            if (oxy) *R = m.max_o2_agar - ALv(i, 0);
-            else if (ip == 0) *R = (APv(ip + 2, 0) + 0.5 * EPv(ip + 2, 0) + ALv(i - 1, 0) + 2 * ALv(i, 1) - 4 * ALv(i, 0)) * D * dt / h2;
-            else *R = (ALv(i + 1, 0) + 0.5 * EPv(ip - 2, 0) + APv(ip - 2, 0) + 2 * ALv(i, 1) - 4 * ALv(i, 0)) * dt * D / h2;
+            if (oxy) *R = (T)m.max_o2_agar - ALv(i, 0);
+            else if (ip == 0) *R = (APv(ip + 2, 0) + half * EPv(ip + 2, 0) + ALv(i - 1, 0) + 2 * ALv(i, 1) - 4 * ALv(i, 0)) * D * dt / h2;
+            else *R = (ALv(i + 1, 0) + half * EPv(ip - 2, 0) + APv(ip - 2, 0) + 2 * ALv(i, 1) - 4 * ALv(i, 0)) * dt * D / h2;
         }
     } else if (l < m.A && ip >= 0 && ip <= nxp && kp <= nzp) {
         if (kp == nzp) {
             if (ip == 0 || ip == nxp)
                 *R = (ALv(i + 1, k) + ALv(i - 1, k) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
             else
-                *R = (ALv(i + 1, k) + ALv(i - 1, k) + ALv(i, k + 1) + APv(ip, kp - 2) + 0.5 * EPv(ip, kp - 2) - 4 * ALv(i, k)) * D * dt / h2;
+                *R = (ALv(i + 1, k) + ALv(i - 1, k) + ALv(i, k + 1) + APv(ip, kp - 2) + half * EPv(ip, kp - 2) - 4 * ALv(i, k)) * D * dt / h2;
         } else if (ip == 0) {
-            *R = (APv(ip + 2, kp) + 0.5 * EPv(ip + 2, kp) + ALv(i - 1, k) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
+            *R = (APv(ip + 2, kp) + half * EPv(ip + 2, kp) + ALv(i - 1, k) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
         } else if (ip == nxp) {
-            *R = (ALv(i + 1, k) + 0.5 * EPv(ip - 2, kp) + APv(ip - 2, kp) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
+            *R = (ALv(i + 1, k) + half * EPv(ip - 2, kp) + APv(ip - 2, kp) + ALv(i, k + 1) + ALv(i, k - 1) - 4 * ALv(i, k)) * D * dt / h2;
         } else {
-            *R = (RPv(ip, kp) + 0.5 * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt / h2 * 4 - EPv(ip, kp)) * 0.5;
+            *R = (RPv(ip, kp) + half * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt / h2 * 4 - EPv(ip, kp)) * half;
         }
     } else if (l >= m.A) {
-        *R = (RPv(ip, kp) + 0.5 * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt / h2 * 4 - EPv(ip, kp)) * 0.5;
+        *R = (RPv(ip, kp) + half * (EPv(ip + 1, kp) + EPv(ip - 1, kp) + EPv(ip, kp + 1) + EPv(ip, kp - 1) - 4 * EPv(ip, kp)) * D * dt / h2 * 4 - EPv(ip, kp)) * half;
     }
 #undef EPv
 #undef RPv
@@ -340,7 +409,8 @@ __global__ void k_mg_restrict(MgConst m, MgLvl Lc, MgLvl Lf, int l, const double
 }
 
 /* interpolationAga, Multigrid.cpp:407-467 (Err of level l += from l+1) */
-__global__ void k_mg_interp(MgConst m, MgLvl Lf, MgLvl Lc, int l)
+template <class T>
+__global__ void k_mg_interp(MgConst m, MgLvlT<T> Lf, MgLvlT<T> Lc, int l)
 {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     int sp = blockIdx.y;
@@ -350,26 +420,28 @@ __global__ void k_mg_interp(MgConst m, MgLvl Lf, MgLvl Lc, int l)
     const int X = m.box_x;
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
-    const double* C = Lc.e[sp];
-    double& e = AT(Lf.e[sp], Lf, i, k);
+    const T* C = Lc.e[sp];
+    T& e = AT(Lf.e[sp], Lf, i, k);
+    const T half = (T)0.5, quarter = (T)0.25;
 #define CV(a, b) at_ref(C, Lc, a, b)
     if (i % 2 == 0) {
         int ip = nxp / 2 - nx / 4 + i / 2;
         if (k % 2 == 0) e += CV(ip, k / 2);
-        else { int kp = (k - 1) / 2; e += 0.5 * (CV(ip, kp) + CV(ip, kp + 1)); }
+        else { int kp = (k - 1) / 2; e += half * (CV(ip, kp) + CV(ip, kp + 1)); }
     } else {
         int ip = nxp / 2 - nx / 4 + (i - 1) / 2;
-        if (k % 2 == 0) { int kp = k / 2; e += 0.5 * (CV(ip, kp) + CV(ip + 1, kp)); }
+        if (k % 2 == 0) { int kp = k / 2; e += half * (CV(ip, kp) + CV(ip + 1, kp)); }
         else {
             int kp = (k - 1) / 2;
-            e += 0.25 * (CV(ip, kp) + CV(ip, kp + 1) + CV(ip + 1, kp) + CV(ip + 1, kp + 1));
+            e += quarter * (CV(ip, kp) + CV(ip, kp + 1) + CV(ip + 1, kp) + CV(ip + 1, kp + 1));
         }
     }
 #undef CV
 }
 
 /* resetZero, Multigrid.cpp:47-82 */
-__global__ void k_mg_reset_zero(MgLvl L, int zero_res)
+template <class T>
+__global__ void k_mg_reset_zero(MgLvlT<T> L, int zero_res)
 {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     int sp = blockIdx.y;
@@ -543,14 +615,19 @@ static inline dim3 grid2(int n, int threads) { return dim3((unsigned)((n + threa
 static int g_relax_mode = 1;   /* 0 = one thread per column, 1 = segmented */
 extern "C" int bcg_set_relax_mode(int mode) { if (mode < 0 || mode > 1) return BCG_E_ARG; g_relax_mode = mode; return BCG_OK; }
 
+template <class T> static MgLvlT<T> lvl(const bcg_ctx* c, int l);
+template <> MgLvlT<double> lvl<double>(const bcg_ctx* c, int l) { return mg_lvl(c, l); }
+template <> MgLvlT<float> lvl<float>(const bcg_ctx* c, int l) { return mg_lvl_f(c, l); }
+
+template <class T>
 static void relax_level(bcg_ctx* c, const MgConst& m, int l)
 {
-    MgLvl L = mg_lvl(c, l);
+    MgLvlT<T> L = lvl<T>(c, l);
     const int rows = L.nz + 1;
     if (g_relax_mode == 0 || rows <= 96) {
         for (int par = 0; par < 2; par++) {
             int ncol = (L.nx + 1 - par + 1) / 2;
-            k_mg_relax<<<grid2(ncol, 64), 64, 0, c->stream>>>(m, L, l, par, c->inside);
+            k_mg_relax<T><<<grid2(ncol, 64), 64, 0, c->stream>>>(m, L, l, par, c->inside);
         }
     } else {
         int nseg = (rows + 63) / 64;
@@ -559,47 +636,54 @@ static void relax_level(bcg_ctx* c, const MgConst& m, int l)
         for (int par = 0; par < 2; par++) {
             int ncol = (L.nx + 1 - par + 1) / 2;
             dim3 grid((unsigned)((ncol + 31) / 32), 3);
-            k_mg_relax_seg<<<grid, dim3(32, nseg), 0, c->stream>>>(m, L, l, par, seg_len, c->inside);
+            k_mg_relax_seg<T><<<grid, dim3(32, nseg), 0, c->stream>>>(m, L, l, par, seg_len, c->inside);
         }
     }
     c->launches += 2;
 }
 
 /* mu2 sweeps on the coarsest level: fused when it fits one block */
+template <class T>
 static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
-    MgLvl L = mg_lvl(c, l);
+    MgLvlT<T> L = lvl<T>(c, l);
     if (g_relax_mode == 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
-        k_mg_relax_coarse<<<1, 1024, 0, c->stream>>>(m, L, l, sweeps, c->inside);
+        k_mg_relax_coarse<T><<<1, 1024, 0, c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
     } else {
-        for (int j = 0; j < sweeps; j++) relax_level(c, m, l);
+        for (int j = 0; j < sweeps; j++) relax_level<T>(c, m, l);
     }
 }
 
-void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
+/* Vcycle, Multigrid.cpp:843-862 */
+template <class T>
+void mg_vcycle_t(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
 {
     const int Lv = c->mg_levels;
     for (int l = 0; l < Lv - 1; l++) {
-        for (int j = 0; j < mu1; j++) relax_level(c, m, l);
-        MgLvl Lc = mg_lvl(c, l + 1), Lf = mg_lvl(c, l);
-        k_mg_restrict<<<grid2((Lc.nx + 1) * (Lc.nz + 1), 256), 256, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
+        for (int j = 0; j < mu1; j++) relax_level<T>(c, m, l);
+        MgLvlT<T> Lc = lvl<T>(c, l + 1), Lf = lvl<T>(c, l);
+        k_mg_restrict<T><<<grid2((Lc.nx + 1) * (Lc.nz + 1), 256), 256, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
         c->launches++;
     }
-    relax_coarsest(c, m, Lv - 1, mu2);
+    relax_coarsest<T>(c, m, Lv - 1, mu2);
     for (int l = Lv - 2; l >= 0; l--) {
-        MgLvl Lf = mg_lvl(c, l), Lc = mg_lvl(c, l + 1);
-        k_mg_interp<<<grid2((Lf.nx + 1) * (Lf.nz + 1), 256), 256, 0, c->stream>>>(m, Lf, Lc, l);
+        MgLvlT<T> Lf = lvl<T>(c, l), Lc = lvl<T>(c, l + 1);
+        k_mg_interp<T><<<grid2((Lf.nx + 1) * (Lf.nz + 1), 256), 256, 0, c->stream>>>(m, Lf, Lc, l);
         c->launches++;
-        for (int j = 0; j < mu1; j++) relax_level(c, m, l);
+        for (int j = 0; j < mu1; j++) relax_level<T>(c, m, l);
     }
 }
+template void mg_vcycle_t<double>(bcg_ctx*, const MgConst&, int, int);
+template void mg_vcycle_t<float>(bcg_ctx*, const MgConst&, int, int);
+
+void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2) { mg_vcycle_t<double>(c, m, mu1, mu2); }
 
 static void reset_zero(bcg_ctx* c)
 {
     for (int l = 0; l < c->mg_levels; l++) {
         MgLvl L = mg_lvl(c, l);
-        k_mg_reset_zero<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(L, l > 0);
+        k_mg_reset_zero<double><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(L, l > 0);
         c->launches++;
     }
 }
@@ -686,5 +770,153 @@ extern "C" int bcg_mg_solve(bcg_ctx* c, int vcycles)
     int rc = mg_solve_impl(c, vcycles, 0);
     if (rc) return rc;
     timer_end(c, BCG_T_MG_SOLVE, (int)(c->launches - l0));
+    return ctx_check_status(c);
+}
+
+
+/* ======================================================================== */
+/* Tolerance-driven solve, FP64 and mixed precision (no reference           */
+/* counterpart: the reference runs a fixed 3 V-cycles and discards its      */
+/* residual, Multigrid.cpp:835, 869).                                       */
+/* ======================================================================== */
+/* Defect of the relaxation equations at the relaxed, uncovered points of a
+ * composite level (the points updateSolAga updates, Multigrid.cpp:553-561):
+ * for E = (R c + N(E)) / (c + 2) points it is R - ((c+2) E - N(E)) / c, for
+ * Dirichlet points R - E.  Computed in FP64 from the FP64 right-hand side
+ * and the current correction (FP64 or FP32 storage).  Max-norms of the
+ * defect and of R go to out[0], out[1] as ordered bit patterns. */
+template <class T>
+__global__ void k_mg_defect(MgConst m, MgLvlT<T> L, MgLvl L64, int l, const double* __restrict__ inside0,
+                            unsigned long long* out)
+{
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int sp = blockIdx.y;
+    double dmax = 0.0, rmax = 0.0;
+    if (idx < (L.nx + 1) * (L.nz + 1)) {
+        int i = idx % (L.nx + 1), k = idx / (L.nx + 1);
+        const int X = m.box_x, ZA = m.box_z_agar;
+        int d = 1 << l, d0 = 1 << m.A;
+        int nxp = X * d0 / d < X ? X * d0 / d : X;
+        int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+        int ip = 2 * i - L.nx + nxp / 2, kp = 2 * k;
+        bool uncovered = (l == 0 || ip <= 0 || ip >= nxp || kp >= nzp);
+        if (uncovered) {
+            int kind; double cfac;
+            double v = relax_eval<T>(m, L, L64.r[sp], l, sp, i, k, inside0, kind, cfac);
+            if (kind != 0) {
+                double e = (double)AT(L.e[sp], L, i, k);
+                double def = (kind == 1) ? (v - e) : (v - e) * (cfac + 2) / cfac;
+                dmax = fabs(def);
+                rmax = fabs(AT(L64.r[sp], L64, i, k));
+            }
+        }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+        rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        /* non-negative doubles order like their bit patterns */
+        if (dmax > 0) atomicMax(&out[0], (unsigned long long)__double_as_longlong(dmax));
+        if (rmax > 0) atomicMax(&out[1], (unsigned long long)__double_as_longlong(rmax));
+    }
+}
+
+template <class A, class B>
+__global__ void k_mg_convert(const A* __restrict__ in, B* __restrict__ out, size_t n)
+{
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (B)in[i];
+}
+
+/* relative defect over the composite levels; syncs the stream */
+template <class T>
+static int mg_rel_defect(bcg_ctx* c, const MgConst& m, double* rel, double* rhs_norm)
+{
+    unsigned long long* d = (unsigned long long*)c->mg_scratch;
+    BCG_CUDA_TRY(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c->stream));
+    for (int l = 0; l < m.A; l++) {
+        MgLvlT<T> L = lvl<T>(c, l);
+        k_mg_defect<T><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, mg_lvl(c, l), l, c->inside, d);
+        c->launches++;
+    }
+    unsigned long long h[2];
+    BCG_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    BCG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double dm, rm;
+    memcpy(&dm, &h[0], 8);
+    memcpy(&rm, &h[1], 8);
+    if (rhs_norm) *rhs_norm = rm;
+    *rel = rm > 0 ? dm / rm : 0.0;
+    return BCG_OK;
+}
+
+static void mg_convert_levels(bcg_ctx* c, bool to_float, bool res)
+{
+    for (int l = 0; l < c->mg_levels; l++) {
+        MgLevel& L = c->mg[l];
+        size_t n = (size_t)L.pitch * (L.nz + 1);
+        for (int sp = 0; sp < 3; sp++) {
+            if (to_float) {
+                const double* src = res ? L.res[sp] : L.err[sp];
+                float* dst = res ? L.resf[sp] : L.errf[sp];
+                k_mg_convert<double, float><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(src, dst, n);
+            } else {
+                const float* src = res ? L.resf[sp] : L.errf[sp];
+                double* dst = res ? L.res[sp] : L.err[sp];
+                k_mg_convert<float, double><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(src, dst, n);
+            }
+            c->launches++;
+        }
+    }
+}
+
+extern "C" int bcg_mg_solve_tol(bcg_ctx* c, double rel_tol, int precision, int max_iters, int* iters, double* rel_res)
+{
+    if (!c || rel_tol <= 0 || max_iters < 1 || (precision != 32 && precision != 64)) return BCG_E_ARG;
+    timer_begin(c, BCG_T_MG_SOLVE);
+    long long l0 = c->launches;
+    MgConst m = mg_const(c, c->P.mg_dt);
+    mg_copy_to(c, m, 0);
+    mg_setup(c, m);
+    const int mu1 = c->P.mg_mu1, mu2 = c->P.mg_mu2;
+    double rel = 1.0, r0 = 0.0;
+    int rc = mg_rel_defect<double>(c, m, &rel, &r0);
+    if (rc) return rc;
+    int it = 0;
+    if (r0 > 0) {
+        rel = 1.0;
+        if (precision == 32) {
+            /* FP32 V-cycles on FP32 copies of Res/Err until the FP64 defect
+             * stops falling by at least 2x per cycle (the FP32 floor) */
+            mg_convert_levels(c, true, true);
+            for (int l = 0; l < c->mg_levels; l++) {
+                MgLvlF L = mg_lvl_f(c, l);
+                k_mg_reset_zero<float><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(L, 0);
+                c->launches++;
+            }
+            double best = 1.0;
+            while (it < max_iters) {
+                mg_vcycle_t<float>(c, m, mu1, mu2);
+                it++;
+                if ((rc = mg_rel_defect<float>(c, m, &rel, nullptr))) return rc;
+                if (rel < rel_tol || rel > 0.5 * best) break;
+                best = rel;
+            }
+            /* FP64 refinement continues from the FP32 correction */
+            mg_convert_levels(c, false, false);
+        }
+        while (rel >= rel_tol && it < max_iters) {
+            mg_vcycle_t<double>(c, m, mu1, mu2);
+            it++;
+            if ((rc = mg_rel_defect<double>(c, m, &rel, nullptr))) return rc;
+        }
+    } else rel = 0.0;
+    mg_reset(c, m);
+    mg_copy_from(c, m, 0);
+    BCG_CUDA_TRY(cudaGetLastError());
+    timer_end(c, BCG_T_MG_SOLVE, (int)(c->launches - l0));
+    if (iters) *iters = it;
+    if (rel_res) *rel_res = rel;
     return ctx_check_status(c);
 }

@@ -12,15 +12,22 @@ struct MgConst {
     double max_carbon, max_o2_agar;
 };
 
-struct MgLvl {
+/* one level as the kernels see it: the solution is always FP64; the
+ * correction (Err) and right-hand side (Res) are T = double or float */
+template <class T>
+struct MgLvlT {
     int nx, nz, pitch;
     double* s[3];
-    double* r[3];
-    double* e[3];
+    T* r[3];
+    T* e[3];
 };
+typedef MgLvlT<double> MgLvl;
+typedef MgLvlT<float> MgLvlF;
 
 MgConst mg_const(const bcg_ctx* c, double dt);
 MgLvl mg_lvl(const bcg_ctx* c, int l);
+MgLvlF mg_lvl_f(const bcg_ctx* c, int l);
+template <class T> void mg_vcycle_t(bcg_ctx* c, const MgConst& m, int mu1, int mu2);
 void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2);
 void mg_setup(bcg_ctx* c, const MgConst& m);
 void mg_reset(bcg_ctx* c, const MgConst& m);

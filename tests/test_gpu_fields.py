@@ -150,3 +150,34 @@ def test_segmented_smoother_matches_sequential(gpu):
     lib.bcg_set_relax_mode(1)
     for a, b in zip(*out):
         assert close(a, b) <= 1e-14
+
+
+def _solve_state(col, p):
+    return [col.field("MG_SOL_" + sp, l) for l in range(p.max_levels_mg) for sp in ("CARBON", "OXYGEN", "ACETATE")]
+
+
+def test_tolerance_solve_fixed_cycles_equals_solve(gpu):
+    """With an unreachable tolerance and max_iters = 3 the tolerance-driven
+    solve runs the same kernels as Multigrid::solve's 3 V-cycles."""
+    p = params.workload_params("small_4k")
+    cells = workload_colony("small_4k", n=2048)
+    a = Colony(p, cells); a.update_density(); a.mg_solve(3)
+    b = Colony(p, cells); b.update_density()
+    it, rel = b.mg_solve_tol(1e-300, 64, 3)
+    assert it == 3
+    for x, y in zip(_solve_state(a, p), _solve_state(b, p)):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("workload,n", [("small_4k", 4096), ("scale_262k", 40000)])
+def test_mixed_precision_reaches_fp64_tolerance(gpu, workload, n):
+    p = params.workload_params(workload)
+    cells = workload_colony(workload, n=n)
+    ref = Colony(p, cells); ref.update_density()
+    it64, rel64 = ref.mg_solve_tol(1e-8, 64, 60)
+    mix = Colony(p, cells); mix.update_density()
+    it32, rel32 = mix.mg_solve_tol(1e-8, 32, 60)
+    assert rel64 < 1e-8 and rel32 < 1e-8, (it64, rel64, it32, rel32)
+    # both solve the same system to the same tolerance
+    for x, y in zip(_solve_state(ref, p), _solve_state(mix, p)):
+        assert close(x, y) <= 1e-9
