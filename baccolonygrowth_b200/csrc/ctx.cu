@@ -219,7 +219,9 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
     for (int l = 0; l < c->mg_levels; l++) {
         MgLevel& L = c->mg[l];
         L.nx = mg_nx(*p, l); L.nz = mg_nz(*p, l);
-        if (L.nx < 2 || L.nz < 2) { bcg_destroy(c); return BCG_E_ARG; }
+        /* coarse levels may have nz = 0 (one row; the small input's coarsest
+         * level is 4 x 0), never nx < 2 */
+        if (L.nx < 2 || L.nz < 0) { bcg_destroy(c); return BCG_E_ARG; }
         L.pitch = ((L.nx + 1) + 31) / 32 * 32;
         size_t np = (size_t)L.pitch * (L.nz + 1);
         const double init[3] = {p->max_carbon, p->max_o2, 0.0};
@@ -265,6 +267,7 @@ extern "C" int bcg_destroy(bcg_ctx* c)
             void* ma[] = {c->mg[l].sol[sp], c->mg[l].res[sp], c->mg[l].err[sp], c->mg[l].errf[sp], c->mg[l].resf[sp]};
             for (void* q : ma) if (q) cudaFree(q);
         }
+    for (int g = 0; g < 2; g++) if (c->nutrient_graph[g]) cudaGraphExecDestroy(c->nutrient_graph[g]);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (int t = 0; t < BCG_T_COUNT; t++) { if (c->ev[t][0]) cudaEventDestroy(c->ev[t][0]); if (c->ev[t][1]) cudaEventDestroy(c->ev[t][1]); }
     if (c->stream) cudaStreamDestroy(c->stream);

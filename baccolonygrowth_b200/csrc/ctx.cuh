@@ -77,6 +77,11 @@ struct bcg_ctx {
     MgLevel mg[BCG_MAX_MG_LEVELS];
     int mg_levels;
     double* mg_scratch;    /* reductions */
+    /* captured [solve + sweeps] units of the nutrient update: [0] plain,
+     * [1] with the acetate buffer solve in its last two sweeps */
+    cudaGraphExec_t nutrient_graph[2];
+    int nutrient_graph_sweeps;
+    int nutrient_graph_launches[2];
     /* timers */
     int timers_on;
     cudaEvent_t ev[BCG_T_COUNT][2];

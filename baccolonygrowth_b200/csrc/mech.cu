@@ -114,7 +114,9 @@ __global__ void k_bin_sort(int nbox, const int* __restrict__ box_start, int* __r
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nbox) return;
     int s = box_start[b], e = box_start[b + 1];
-    if (e - s > box_cap - 1) dev_error(st, BCG_E_BOX_OVERFLOW, b);
+    /* an overfull box is an error (UniformGrid.h:35); leave it unsorted so
+     * that the work of this thread stays bounded */
+    if (e - s > box_cap - 1) { dev_error(st, BCG_E_BOX_OVERFLOW, b); return; }
     for (int i = s + 1; i < e; i++) {
         int v = box_ids[i], j = i - 1;
         while (j >= s && box_ids[j] > v) { box_ids[j + 1] = box_ids[j]; j--; }
@@ -187,6 +189,7 @@ __device__ void warp_rebuild_one(int me, const CellRec* rec, MechParams mp,
             for (int xa = max(xi - 1, 0); xa < min(xi + 2, mp.box_x); xa++) {
                 int b = xa * YZ + ya * mp.box_z + za;
                 int s = box_start[b], e = box_start[b + 1];
+                if (e - s > mp.box_cap) e = s + mp.box_cap;   /* overfull: error already raised by the binning */
                 for (int t = s; t < e; t += 32) {
                     int j = (t + lane < e) ? box_ids[t + lane] : -1;
                     bool keep = false;

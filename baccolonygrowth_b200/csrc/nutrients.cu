@@ -344,6 +344,38 @@ extern "C" int bcg_colony_sweeps(bcg_ctx* c, int sweeps, int count0)
     return ctx_check_status(c);
 }
 
+/* One unit of the nutrient update -- Multigrid::solve then `sweeps`
+ * sweeps -- captured once as a CUDA graph and replayed: with an even sweep
+ * count the local buffer indices and the sweep-count parity are back where
+ * they started after each unit, so every unit issues the same kernels with
+ * the same arguments. */
+static int nutrient_unit_graph(bcg_ctx* c, int sweeps, int last, cudaGraphExec_t* out)
+{
+    if (c->nutrient_graph_sweeps != sweeps) {
+        for (int g = 0; g < 2; g++)
+            if (c->nutrient_graph[g]) { cudaGraphExecDestroy(c->nutrient_graph[g]); c->nutrient_graph[g] = nullptr; }
+        c->nutrient_graph_sweeps = sweeps;
+    }
+    if (!c->nutrient_graph[last]) {
+        cudaGraph_t g;
+        BCG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        long long l0 = c->launches;
+        int ce = 0, cw = 0, count = 0;
+        int rc = mg_solve_impl(c, c->P.mg_vcycles, cw);
+        if (rc == BCG_OK) run_sweeps(c, sweeps, ce, cw, count, last ? sweeps - 2 : sweeps);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
+        c->nutrient_graph_launches[last] = (int)(c->launches - l0);
+        c->launches = l0;
+        e = cudaGraphInstantiate(&c->nutrient_graph[last], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
+    }
+    *out = c->nutrient_graph[last];
+    return BCG_OK;
+}
+
 /* UpdateEnvArrayMG_OxygenAcetate (Multigrid.cpp:984-1125) */
 extern "C" int bcg_nutrient_update(bcg_ctx* c, int n, int sweeps)
 {
@@ -354,11 +386,22 @@ extern "C" int bcg_nutrient_update(bcg_ctx* c, int n, int sweeps)
     if (sweeps < 0) sweeps = P.sweeps_per_solve;
     timer_begin(c, BCG_T_SWEEPS);
     long long l0 = c->launches;
-    int ce = 0, cw = 0, count = 0;
-    for (int i = 0; i < n; i++) {
-        int rc = mg_solve_impl(c, P.mg_vcycles, cw);
-        if (rc) return rc;
-        run_sweeps(c, sweeps, ce, cw, count, (i == n - 1) ? sweeps - 2 : sweeps);
+    if (sweeps % 2 == 0 && sweeps >= 2) {
+        for (int i = 0; i < n; i++) {
+            int last = (i == n - 1);
+            cudaGraphExec_t ge;
+            int rc = nutrient_unit_graph(c, sweeps, last, &ge);
+            if (rc) return rc;
+            BCG_CUDA_TRY(cudaGraphLaunch(ge, c->stream));
+            c->launches += c->nutrient_graph_launches[last];
+        }
+    } else {
+        int ce = 0, cw = 0, count = 0;
+        for (int i = 0; i < n; i++) {
+            int rc = mg_solve_impl(c, P.mg_vcycles, cw);
+            if (rc) return rc;
+            run_sweeps(c, sweeps, ce, cw, count, (i == n - 1) ? sweeps - 2 : sweeps);
+        }
     }
     BCG_CUDA_TRY(cudaGetLastError());
     timer_end(c, BCG_T_SWEEPS, (int)(c->launches - l0));

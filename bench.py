@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mg-tol", action="store_true")
     return ap.parse_args()
 
 
@@ -225,7 +226,8 @@ def b200_arm(args):
     p = params.workload_params(args.workload)
     # replicas: every rank runs its own colony (different seed), no
     # data-path collective
-    cells = workload_colony(args.workload, seed=20261205 + rank)
+    from baccolonygrowth_b200 import replicas as _rep
+    cells = workload_colony(args.workload, seed=_rep.replica_seed(20261205, rank))
     n0 = len(cells)
     cells = np.ascontiguousarray(cells)
     pinned = torch.empty(cells.nbytes, dtype=torch.uint8, pin_memory=True)
@@ -310,18 +312,36 @@ def b200_arm(args):
     d2h = (got.value * 208 + 16 * args.steps + 8 * d2.value) / args.steps
     e2e_value = 0.5 * (n0 + got.value) * args.steps / e2e_s
 
-    # max over ranks
-    vals = torch.tensor([ms, e2e_s, cells_mean * args.steps, 0.5 * (n0 + got.value) * args.steps], dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = vals.clone()
-        dist.all_reduce(mx[:2], op=dist.ReduceOp.MAX)
-        tot = vals.clone()
-        dist.all_reduce(tot[2:], op=dist.ReduceOp.SUM)
-        ms_max, e2e_max = float(mx[0]), float(mx[1])
-        work, work_e2e = float(tot[2]), float(tot[3])
-    else:
-        ms_max, e2e_max = ms, e2e_s
-        work, work_e2e = cells_mean * args.steps, 0.5 * (n0 + got.value) * args.steps
+    # the agar solve to a 1e-8 relative defect: plain FP64 V-cycles vs FP32
+    # V-cycles with FP64 defect checks and FP64 refinement, from the same state
+    mg_tol = None
+    if not args.no_mg_tol:
+        from baccolonygrowth_b200.colony import Colony
+        res = {}
+        sols = {}
+        for prec in (64, 32):
+            col = Colony(p, cells)
+            col.update_density()
+            col.mg_solve_tol(1e-8, prec, 2)        # warm-up (compiles graphs, pages in)
+            col.close()
+            col = Colony(p, cells)
+            col.update_density()
+            col.enable_timers(True)
+            it, rel = col.mg_solve_tol(1e-8, prec, 100)
+            msx, _ = col.timer("MG_SOLVE")
+            res["fp64" if prec == 64 else "mixed"] = {"iters": it, "ms": msx, "rel_defect": rel}
+            sols[prec] = [col.field("MG_SOL_" + sp, 0) for sp in ("CARBON", "OXYGEN", "ACETATE")]
+            col.close()
+        diff = max(float(np.abs(a - b).max() / max(np.abs(a).max(), 1e-300)) for a, b in zip(sols[64], sols[32]))
+        mg_tol = {"rel_tol": 1e-8, "fp64": res["fp64"], "mixed": res["mixed"],
+                  "speedup": res["fp64"]["ms"] / res["mixed"]["ms"] if res["mixed"]["ms"] > 0 else None,
+                  "max_rel_diff_level0": diff, "dof": mg_dof(p)}
+
+    # max over ranks (time) and sum over ranks (work); no other collective
+    from baccolonygrowth_b200 import replicas
+    (ms_max, e2e_max), (work, work_e2e) = replicas.aggregate(
+        [ms, e2e_s], [cells_mean * args.steps, 0.5 * (n0 + got.value) * args.steps],
+        device="cuda" if world > 1 else "cpu")
 
     value = work / (ms_max / 1e3)
     e2e_value = work_e2e / e2e_max
@@ -367,6 +387,7 @@ def b200_arm(args):
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (cell records 2x%d MB + fields)" % (n0 * 128 // 2 ** 20)},
         "mg_dof_per_s": dof * args.vcycles / (mg_ms / 1e3) if mg_ms > 0 else None,
+        "mg_tolerance_solve": mg_tol,
         "kernel_ms_per_step": timers,
         "divisions": d_.value,
         "roofline": roof,
