@@ -35,6 +35,28 @@ def workload_colony(name, seed=None, phi=0.45, div_phase_spread=1.0, n=None):
     return synth_colony(n, w, h, seed=s, div_phase_spread=div_phase_spread)
 
 
+def depleted_wall(p, inside, depth_c=0.6, depth_o=0.8, acetate=2.0):
+    """Level-0 wall rows (carbon, oxygen, acetate; length Box_x) of a colony
+    that has consumed nutrients: a parabolic dip under the colony footprint,
+    `depth_c` / `depth_o` of maxCarbon / Max_Oxygen at its centre, and
+    acetate up to `acetate` mM.  `inside` is the INSIDE field (Box_x x
+    Box_z, z fastest).  The agar solve copies these rows under the colony
+    into its level-0 bottom row (copyToMG, Multigrid.cpp:891-907), which
+    gives Multigrid::solve a non-zero right-hand side; from the uniform
+    initial state it has none."""
+    X = p.box_x
+    col = np.asarray(inside).reshape(X, -1)[:, 0] > 0
+    xs = np.nonzero(col)[0]
+    x = np.arange(X, dtype=np.float64)
+    if xs.size == 0:
+        u = np.zeros(X)
+    else:
+        c = 0.5 * (xs[0] + xs[-1])
+        w = max(0.5 * (xs[-1] - xs[0]), 1.0)
+        u = np.clip(1.0 - ((x - c) / w) ** 2, 0.0, 1.0)
+    return (p.max_carbon * (1.0 - depth_c * u), p.max_o2 * (1.0 - depth_o * u), acetate * u)
+
+
 class Rng:
     """The host's glibc-compatible rand() stream (bcg_rng_*)."""
 
@@ -158,6 +180,14 @@ class Colony:
         fid = _abi.FIELDS[name] if isinstance(name, str) else name
         v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
         _abi.check(self.lib.bcg_set_field(self.h, fid, level, _abi.ptr(v, ctypes.c_double), v.size), "bcg_set_field")
+
+    def deplete_wall(self, **kw):
+        """Set the level-0 wall rows to depleted_wall() of the current
+        INSIDE field (call after update_density); returns the rows."""
+        rows = depleted_wall(self.params, self.field("INSIDE"), **kw)
+        for name, v in zip(("WALLF_CARBON", "WALLF_OXYGEN", "WALLF_ACETATE"), rows):
+            self.set_field(name, v, 0)
+        return rows
 
     def bbox(self):
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -308,15 +308,18 @@ __global__ void __launch_bounds__(256) k_move_grow(int n, int nbinned, const int
 {
     int t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int gl = threadIdx.x & (G - 1);
-    bool active = t < n;
+    /* Lanes past the last cell run the body on cell 0 and write nothing:
+     * the group reduction is a full-warp shuffle, so every lane of the
+     * warp has to reach it (n > 0 at every launch). */
+    const bool active = t < n;
     int me = active ? (t < nbinned ? __ldg(&order[t]) : t) : 0;
     int near1 = 0, near2 = 0;
-    if (active) {
+    {
         Cst o = load_cst(&old[me]);
         V3 ocm = avg_pq(o.p, o.q);
         int xi, yi, zi;
         int obox = box_address(ocm, mp, xi, yi, zi);
-        if (obox < 0) { if (gl == 0) dev_error(st, BCG_E_OUT_OF_GRID, me); xi = 0; yi = 0; }
+        if (obox < 0) { if (gl == 0 && active) dev_error(st, BCG_E_OUT_OF_GRID, me); xi = 0; yi = 0; }
         double wall_z = __ldg(&fp.wall[xi * mp.box_y + yi]);
         const int* list = nbr + (size_t)me * mp.kmax;
         int cnt = __ldg(&ncount[me]);
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(256) k_move_grow(int n, int nbinned, const int
         /* grow, grow.cpp:17-102 */
         V3 ncm = avg_pq(nc.p, nc.q);
         int nbox = box_address(ncm, mp, xi, yi, zi);
-        if (nbox < 0) { if (gl == 0) dev_error(st, BCG_E_OUT_OF_GRID, me); nbox = 0; }
+        if (nbox < 0) { if (gl == 0 && active) dev_error(st, BCG_E_OUT_OF_GRID, me); nbox = 0; }
         double g;
         if (mp.cross_feeding && __ldg(&soa.type[me]) != 1) g = __ldg(&fp.gr2[nbox]);
         else g = __ldg(&fp.gr1[nbox]);
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(256) k_move_grow(int n, int nbinned, const int
         nc.L += dL;
         nc.p = sub3(nc.p, dv);
         nc.q = add3(nc.q, dv);
-        if (gl == 0) {
+        if (gl == 0 && active) {
             CellRec r;
             r.pL = make_double4(nc.p.x, nc.p.y, nc.p.z, nc.L);
             r.qR = make_double4(nc.q.x, nc.q.y, nc.q.z, nc.R);

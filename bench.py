@@ -103,6 +103,22 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def set_depleted_wall(lib, ctx, p, rows=None):
+    """Level-0 wall rows depleted under the colony, so that the agar solve
+    has a non-zero right-hand side (from the uniform start it has none).
+    Returns the rows (computed from the context's INSIDE field if not given)."""
+    import numpy as np
+    from baccolonygrowth_b200 import _abi
+    from baccolonygrowth_b200.colony import depleted_wall
+    if rows is None:
+        ins = np.zeros(p.box_x * p.box_z)
+        _abi.check(lib.bcg_get_field(ctx, _abi.FIELDS["INSIDE"], 0, _abi.ptr(ins, ctypes.c_double), ins.size), "inside")
+        rows = [np.ascontiguousarray(v) for v in depleted_wall(p, ins)]
+    for name, v in zip(("WALLF_CARBON", "WALLF_OXYGEN", "WALLF_ACETATE"), rows):
+        _abi.check(lib.bcg_set_field(ctx, _abi.FIELDS[name], 0, _abi.ptr(v, ctypes.c_double), v.size), name)
+    return rows
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -244,9 +260,10 @@ def b200_arm(args):
         g = np.full(p.box_x * p.box_z, 0.9)
         _abi.check(lib.bcg_set_field(ctx, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size), "set growth")
         _abi.check(lib.bcg_update_density(ctx), "bcg_update_density")
-        return sim, ctx
+        rows = set_depleted_wall(lib, ctx, p)
+        return sim, ctx, rows
 
-    sim, ctx = make_sim()
+    sim, ctx, wall_rows = make_sim()
     stream = torch.cuda.ExternalStream(lib.bcg_stream(ctx))
     _abi.check(lib.bcg_sim_run(sim, args.warmup), "warmup")
     torch.cuda.synchronize()
@@ -300,6 +317,7 @@ def b200_arm(args):
     w0 = time.perf_counter()
     _abi.check(lib.bcg_upload_cells(ctx2, _abi.ptr(hostbuf), n0), "upload")
     _abi.check(lib.bcg_update_density(ctx2), "density")
+    set_depleted_wall(lib, ctx2, p, wall_rows)
     _abi.check(lib.bcg_sim_run(sim2, args.steps), "e2e steps")
     got = ctypes.c_int()
     _abi.check(lib.bcg_download_cells(ctx2, _abi.ptr(outbuf), len(outbuf), ctypes.byref(got)), "download")
@@ -308,7 +326,7 @@ def b200_arm(args):
     t2 = ctypes.c_double(); n2 = ctypes.c_int(); d2 = ctypes.c_int64()
     lib.bcg_sim_time(sim2, ctypes.byref(t2), ctypes.byref(n2), ctypes.byref(d2))
     lib.bcg_sim_destroy(sim2)
-    h2d = (n0 * 208 + 9 * 4 * d2.value) / args.steps
+    h2d = (n0 * 208 + 3 * 8 * p.box_x + 9 * 4 * d2.value) / args.steps
     d2h = (got.value * 208 + 16 * args.steps + 8 * d2.value) / args.steps
     e2e_value = 0.5 * (n0 + got.value) * args.steps / e2e_s
 
@@ -322,10 +340,12 @@ def b200_arm(args):
         for prec in (64, 32):
             col = Colony(p, cells)
             col.update_density()
-            col.mg_solve_tol(1e-8, prec, 2)        # warm-up (compiles graphs, pages in)
+            col.deplete_wall()
+            col.mg_solve_tol(1e-8, prec, 2)        # warm-up (pages in)
             col.close()
             col = Colony(p, cells)
             col.update_density()
+            col.deplete_wall()
             col.enable_timers(True)
             it, rel = col.mg_solve_tol(1e-8, prec, 100)
             msx, _ = col.timer("MG_SOLVE")

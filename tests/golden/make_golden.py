@@ -9,9 +9,11 @@ outputs:
                    full neighbour rebuild, 12 MoveCell/GrowCell + division
                    steps: per-step rand() draws, dividing ids and lineage,
                    the final cells and neighbour lists.
-  fields_small.npz 2048 cells: the UpdateFlag deposition chain, one
-                   Multigrid::solve (3 V-cycles), then one nutrient update
-                   with one solve + 200 sweeps.
+  fields_small.npz 2048 cells: the UpdateFlag deposition chain, the
+                   level-0 wall rows depleted under the colony
+                   (colony.depleted_wall), one Multigrid::solve (3
+                   V-cycles), then one nutrient update with one solve +
+                   200 sweeps.
 
 Usage:  python tests/golden/make_golden.py
 """
@@ -27,7 +29,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 from baccolonygrowth_b200 import _abi, params  # noqa: E402
-from baccolonygrowth_b200.colony import workload_colony  # noqa: E402
+from baccolonygrowth_b200.colony import workload_colony, depleted_wall  # noqa: E402
 import checkers  # noqa: E402
 
 F = _abi.FIELDS
@@ -80,6 +82,9 @@ def fields():
     out["bbox"] = np.array(ref.bbox(), dtype=np.int32)
     for f in ("ROUGH_DENSITY", "INSIDE", "DENSITY_SHIFT", "DENSITY", "HEIGHT", "NORMAL_X", "NORMAL_Z", "WALL"):
         out["d_" + f] = ref.field(F[f])
+    rows = depleted_wall(p, ref.field(F["INSIDE"]))
+    for name, v in zip(("WALLF_CARBON", "WALLF_OXYGEN", "WALLF_ACETATE"), rows):
+        ref.set_field(F[name], v, 0)
     ref.mg_solve(3, p.mg_dt)
     for l in range(p.mg_levels):
         for sp in ("CARBON", "OXYGEN", "ACETATE"):

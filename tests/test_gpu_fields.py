@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from baccolonygrowth_b200 import _abi, params
-from baccolonygrowth_b200.colony import Colony, workload_colony
+from baccolonygrowth_b200.colony import Colony, workload_colony, depleted_wall
 
 import checkers as ck
 
@@ -53,6 +53,15 @@ def wall_mask(p, level):
     return m
 
 
+def deplete(p, *models):
+    """Depleted wall rows under the colony (a non-zero right-hand side for
+    the agar solve), the same on every model; after update_density."""
+    rows = depleted_wall(p, models[0].field(F["INSIDE"]))
+    for m in models:
+        for name, v in zip(("WALLF_CARBON", "WALLF_OXYGEN", "WALLF_ACETATE"), rows):
+            m.set_field(F[name], v, 0)
+
+
 def test_density_chain(gpu):
     p, orc, col = make()
     orc.update_density()
@@ -78,8 +87,11 @@ def test_mg_solve(gpu):
     p, orc, col = make()
     orc.update_density()
     col.update_density()
+    deplete(p, orc, col)
     orc.mg_solve(3, p.mg_dt)
     col.mg_solve(3)
+    # the right-hand side is not zero (the solve has work to do)
+    assert np.abs(col.field("MG_RES_CARBON", 0)).max() > 0
     for l in range(p.mg_levels):
         for sp in ("CARBON", "OXYGEN", "ACETATE"):
             for kind in ("SOL", "RES", "ERR"):
@@ -144,10 +156,12 @@ def test_segmented_smoother_matches_sequential(gpu):
         assert lib.bcg_set_relax_mode(mode) == 0
         col = Colony(p, cells)
         col.update_density()
+        col.deplete_wall()
         col.mg_solve(2)
         out.append([col.field("MG_SOL_" + sp, l) for l in range(3) for sp in ("CARBON", "OXYGEN", "ACETATE")])
         col.close()
     lib.bcg_set_relax_mode(1)
+    assert np.ptp(out[0][0]) > 0          # carbon level 0 is no longer uniform
     for a, b in zip(*out):
         assert close(a, b) <= 1e-14
 
@@ -161,10 +175,10 @@ def test_tolerance_solve_fixed_cycles_equals_solve(gpu):
     solve runs the same kernels as Multigrid::solve's 3 V-cycles."""
     p = params.workload_params("small_4k")
     cells = workload_colony("small_4k", n=2048)
-    a = Colony(p, cells); a.update_density(); a.mg_solve(3)
-    b = Colony(p, cells); b.update_density()
+    a = Colony(p, cells); a.update_density(); a.deplete_wall(); a.mg_solve(3)
+    b = Colony(p, cells); b.update_density(); b.deplete_wall()
     it, rel = b.mg_solve_tol(1e-300, 64, 3)
-    assert it == 3
+    assert it == 3 and 0 < rel < 1, (it, rel)
     for x, y in zip(_solve_state(a, p), _solve_state(b, p)):
         assert np.array_equal(x, y)
 
@@ -173,10 +187,11 @@ def test_tolerance_solve_fixed_cycles_equals_solve(gpu):
 def test_mixed_precision_reaches_fp64_tolerance(gpu, workload, n):
     p = params.workload_params(workload)
     cells = workload_colony(workload, n=n)
-    ref = Colony(p, cells); ref.update_density()
+    ref = Colony(p, cells); ref.update_density(); ref.deplete_wall()
     it64, rel64 = ref.mg_solve_tol(1e-8, 64, 60)
-    mix = Colony(p, cells); mix.update_density()
+    mix = Colony(p, cells); mix.update_density(); mix.deplete_wall()
     it32, rel32 = mix.mg_solve_tol(1e-8, 32, 60)
+    assert it64 > 1 and it32 > 1, (it64, it32)
     assert rel64 < 1e-8 and rel32 < 1e-8, (it64, rel64, it32, rel32)
     # both solve the same system to the same tolerance
     for x, y in zip(_solve_state(ref, p), _solve_state(mix, p)):

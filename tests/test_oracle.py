@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from baccolonygrowth_b200 import _abi, params
-from baccolonygrowth_b200.colony import workload_colony
+from baccolonygrowth_b200.colony import workload_colony, depleted_wall
 
 import checkers as ck
 
@@ -77,7 +77,11 @@ def test_oracle_matches_golden_fields():
         assert np.array_equal(orc.field(F[f]), g["d_" + f]), f
     for f in ("DENSITY_SHIFT", "DENSITY"):
         assert np.array_equal(orc.field(F[f])[box], g["d_" + f][box]), f
+    rows = depleted_wall(p, orc.field(F["INSIDE"]))
+    for name, v in zip(("WALLF_CARBON", "WALLF_OXYGEN", "WALLF_ACETATE"), rows):
+        orc.set_field(F[name], v, 0)
     orc.mg_solve(3, p.mg_dt)
+    assert np.ptp(orc.field(F["MG_SOL_CARBON"], 0)) > 0
     for l in range(p.mg_levels):
         for sp in ("CARBON", "OXYGEN", "ACETATE"):
             assert np.array_equal(orc.field(F["MG_SOL_" + sp], l), g["mg_%d_%s" % (l, sp)]), (l, sp)
