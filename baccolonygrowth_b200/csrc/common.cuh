@@ -35,6 +35,11 @@ struct DevStatus {
 };
 
 /* Parameters the kernels read, copied by value into each launch. */
+/* divisions per step handled by bcg_divide, and the footprint-overlap
+ * pairs its planner records before falling back to one sequential group */
+#define DIV_SORT_MAX 8192
+#define DIV_PAIR_CAP 65536
+
 struct MechParams {
     int box_x, box_y, box_z, rgh;
     int xh;             /* Height/Normal length, box_x*rgh */

@@ -106,6 +106,10 @@ extern "C" int bcg_get_timer(bcg_ctx* c, int t, double* ms, int64_t* launches)
     if (launches) *launches = c->timer_launches[t];
     return BCG_OK;
 }
+static int g_kernel_gen = 0;
+int bcg_kernel_config_generation() { return g_kernel_gen; }
+void bcg_kernel_config_changed() { g_kernel_gen++; }
+
 extern "C" void* bcg_stream(bcg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 extern "C" int bcg_synchronize(bcg_ctx* c) { return c ? ctx_check_status(c) : BCG_E_ARG; }
 extern "C" long long bcg_kernel_launches(bcg_ctx* c) { return c ? c->launches : 0; }
@@ -179,6 +183,13 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
     DALLOC(c->lineage, 2 * cap * 4);
     DALLOC(c->n_done_dev, 64);
     DALLOC(c->draws_dev, 9 * cap * 4);
+    DALLOC(c->div_rec, 2 * (size_t)DIV_SORT_MAX * sizeof(CellRec));
+    DALLOC(c->div_box, 2 * (size_t)DIV_SORT_MAX * 4);
+    DALLOC(c->div_rect, (size_t)DIV_SORT_MAX * sizeof(int4));
+    DALLOC(c->div_pairs, (size_t)DIV_PAIR_CAP * sizeof(int2));
+    DALLOC(c->div_par, (size_t)DIV_SORT_MAX * 4);
+    DALLOC(c->div_order, (size_t)DIV_SORT_MAX * 4);
+    DALLOC(c->div_grp, 2 * (size_t)DIV_SORT_MAX * 4);
     DALLOC(c->status, sizeof(DevStatus));
     BCG_CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus), c->stream));
     BCG_CUDA_TRY(cudaMemsetAsync(c->moved, 0, cap * 4, c->stream));
@@ -228,6 +239,11 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
         for (int sp = 0; sp < 3; sp++) {
             DALLOC(L.sol[sp], np * 8); DALLOC(L.res[sp], np * 8); DALLOC(L.err[sp], np * 8);
             DALLOC(L.errf[sp], np * 4); DALLOC(L.resf[sp], np * 4);
+            DALLOC(L.err2[sp], np * 8); DALLOC(L.errf2[sp], np * 4);
+            BCG_CUDA_TRY(cudaMemsetAsync(L.err2[sp], 0, np * 8, c->stream));
+            BCG_CUDA_TRY(cudaMemsetAsync(L.errf2[sp], 0, np * 4, c->stream));
+            BCG_CUDA_TRY(cudaMemsetAsync(L.errf[sp], 0, np * 4, c->stream));
+            BCG_CUDA_TRY(cudaMemsetAsync(L.resf[sp], 0, np * 4, c->stream));
             if ((rc = fill(c, L.sol[sp], init[sp], np)) || (rc = fill(c, L.res[sp], init[sp], np)) ||
                 (rc = fill(c, L.err[sp], init[sp], np))) { bcg_destroy(c); return rc; }
         }
@@ -250,7 +266,8 @@ extern "C" int bcg_destroy(bcg_ctx* c)
                     c->soa.dfx, c->soa.dfy, c->soa.dfz, c->soa.sfx, c->soa.sfy, c->soa.sfz, c->soa.type, c->soa.anc,
                     c->nbr, c->ncount, c->box_cnt, c->box_start, c->box_ids, c->cell_box, c->scan_tmp,
                     c->div_list, c->div_count, c->fcw_count, c->moved, c->delta_ids, c->delta_box, c->lineage,
-                    c->n_done_dev, c->draws_dev, c->status, c->height, c->rough_height, c->nrm_x, c->nrm_y, c->nrm_z,
+                    c->n_done_dev, c->draws_dev, c->div_rec, c->div_box, c->div_rect, c->div_pairs, c->div_par,
+                    c->div_order, c->div_grp, c->status, c->height, c->rough_height, c->nrm_x, c->nrm_y, c->nrm_z,
                     c->wall, c->rd, c->inside, c->rds, c->ds, c->dens, c->rws, c->wds, c->rw, c->wd, c->bbox, c->mg_scratch};
     for (void* q : ptrs) if (q) cudaFree(q);
     for (int b = 0; b < 2; b++) {
@@ -264,7 +281,8 @@ extern "C" int bcg_destroy(bcg_ctx* c)
     }
     for (int l = 0; l < BCG_MAX_MG_LEVELS; l++)
         for (int sp = 0; sp < 3; sp++) {
-            void* ma[] = {c->mg[l].sol[sp], c->mg[l].res[sp], c->mg[l].err[sp], c->mg[l].errf[sp], c->mg[l].resf[sp]};
+            void* ma[] = {c->mg[l].sol[sp], c->mg[l].res[sp], c->mg[l].err[sp], c->mg[l].errf[sp], c->mg[l].resf[sp],
+                          c->mg[l].err2[sp], c->mg[l].errf2[sp]};
             for (void* q : ma) if (q) cudaFree(q);
         }
     for (int g = 0; g < 2; g++) if (c->nutrient_graph[g]) cudaGraphExecDestroy(c->nutrient_graph[g]);

@@ -16,6 +16,8 @@ struct MgLevel {
     double* err[3];
     float* errf[3];   /* FP32 shadows used by the mixed-precision solve */
     float* resf[3];
+    double* err2[3];  /* second correction buffer: the fused smoother writes */
+    float* errf2[3];  /* out of place and the two buffers swap roles */
 };
 
 /* one buffer of the colony environment (LocalEnv fields kept on device) */
@@ -61,6 +63,14 @@ struct bcg_ctx {
     int* lineage;          /* 2*cap */
     int* n_done_dev;
     float* draws_dev;      /* 9*cap */
+    /* division planning (DIV_SORT_MAX divisions per step at most) */
+    CellRec* div_rec;      /* 2 per division: new mother, daughter */
+    int* div_box;          /* 2 per division */
+    int4* div_rect;        /* footprint rectangle per division */
+    int2* div_pairs;       /* overlapping footprints, DIV_PAIR_CAP */
+    int* div_par;          /* union-find parents */
+    int* div_order;        /* divisions grouped, ascending inside a group */
+    int* div_grp;          /* (start, length) per group */
     int last_ndiv;
     /* status */
     DevStatus* status;     /* device */
@@ -81,6 +91,7 @@ struct bcg_ctx {
      * [1] with the acetate buffer solve in its last two sweeps */
     cudaGraphExec_t nutrient_graph[2];
     int nutrient_graph_sweeps;
+    int nutrient_graph_gen;              /* kernel-choice generation the graphs were captured under */
     int nutrient_graph_launches[2];
     /* timers */
     int timers_on;
@@ -96,3 +107,6 @@ int ctx_check_status(bcg_ctx* c);   /* syncs, reads the device status word */
 void timer_begin(bcg_ctx* c, int t);
 void timer_end(bcg_ctx* c, int t, int launches);
 int ensure_pinned(bcg_ctx* c, size_t bytes);
+/* bumped whenever a kernel variant is switched (captured graphs go stale) */
+int bcg_kernel_config_generation();
+void bcg_kernel_config_changed();

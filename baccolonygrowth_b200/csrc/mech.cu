@@ -386,6 +386,7 @@ static int g_group = 4;   /* lanes per cell in the force loop (tunable) */
 extern "C" int bcg_set_force_group(int g)
 {
     if (g != 1 && g != 2 && g != 4 && g != 8 && g != 16) return BCG_E_ARG;
+    if (g != g_group) bcg_kernel_config_changed();
     g_group = g;
     return BCG_OK;
 }
@@ -435,12 +436,14 @@ extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_cal
 /* ======================================================================= */
 /* division loop                                                            */
 /* ======================================================================= */
-#define DIV_SORT_MAX 8192
-#define DIV_THREADS 512
 
 /* divide(), grow.cpp:107-186, for mother m into daughter d; u[0..8] are the
- * nine (float)rand()/RAND_MAX draws in call order. */
-__device__ void divide_pair(int m, int d, const float* u, double t, CellRec* rec, CellSoA soa, const MechParams& mp)
+ * nine (float)rand()/RAND_MAX draws in call order.  Reads the mother's
+ * record, writes the SoA fields of both cells (no other division reads
+ * them) and returns the two new records in out_m / out_d; the records are
+ * stored in rec[] later, in division order. */
+__device__ void divide_compute(int m, int d, const float* u, double t, const CellRec* rec, CellSoA soa,
+                               const MechParams& mp, CellRec& out_m, CellRec& out_d)
 {
     Cst M = load_cst(&rec[m]);
     double dl = ((double)u[0] - 0.5) * mp.var_l;
@@ -479,8 +482,8 @@ __device__ void divide_pair(int m, int d, const float* u, double t, CellRec* rec
     rd.qR = make_double4(dq.x, dq.y, dq.z, dR);
     rd.v = make_double4(M.v.x, M.v.y, M.v.z, 0.0);
     rd.w = make_double4(dw.x, dw.y, dw.z, 0.0);
-    rec[m] = rm;
-    rec[d] = rd;
+    out_m = rm;
+    out_d = rd;
     soa.gr[d] = soa.gr[m];
     soa.tq[d] = tq_m;
     soa.tq[m] = t;
@@ -496,24 +499,42 @@ __device__ void divide_pair(int m, int d, const float* u, double t, CellRec* rec
     soa.ldiv[d] = mp.l_divide / 2 + mp.cell_radius + dLen;
 }
 
-/* Simulation.cpp:380-404 in one CTA: divisions in ascending parent order;
- * each applies divide(), moves the mother / adds the daughter in the box
- * structure, and rebuilds the lists of {mother, mother's neighbours,
- * daughter} (Neighbours.cpp:39-55) with the warps of the block. */
-__global__ void __launch_bounds__(DIV_THREADS) k_divide(int n_start, int ndiv, int cap, double t,
-        const float* __restrict__ draws, CellRec* rec, CellSoA soa, MechParams mp,
-        const int* __restrict__ div_list, int* nbr, int* ncount,
-        const int* __restrict__ box_start, const int* __restrict__ box_ids,
-        int* moved, int* delta_ids, int* delta_box, int* lineage, int* out, DevStatus* st)
+/* Simulation.cpp:380-404.  The reference divides the parents one after
+ * another in ascending id order; each division moves the mother and adds
+ * the daughter in the box structure and rebuilds the lists of {mother,
+ * mother's neighbours, daughter} (Neighbours.cpp:39-55) against the state
+ * left by the divisions before it.
+ *
+ * Here the divisions run as independent groups.  A division's footprint is
+ * the rectangle of boxes, widened by 2, around the boxes of every cell whose
+ * list it can rebuild (the mother before and after, her listed neighbours,
+ * the daughter).  Every box a rebuild scans, and every box whose content
+ * the division changes, lies inside it.  Divisions whose footprints overlap
+ * are joined (union-find) into one group, and a group runs its divisions in
+ * ascending order on one warp.  Divisions of different groups neither
+ * change a box the other scans nor rebuild a common list, so the lists
+ * come out as in the sequential loop.
+ *
+ * k_div_plan (one CTA): sort the parents, apply the reference's MaxCells
+ * cut, compute all divisions' geometry (divide_compute; SoA fields written
+ * here), footprints, groups, and the group-ordered division list.
+ * k_div_groups (one warp per group): store the records, mark the mother
+ * moved, append both cells to the group's delta list, rebuild the lists. */
+__global__ void __launch_bounds__(1024) k_div_plan(int n_start, int ndiv, int cap, double t,
+        const float* __restrict__ draws, const CellRec* __restrict__ rec, CellSoA soa, MechParams mp,
+        const int* __restrict__ div_list, const int* __restrict__ cell_box,
+        const int* __restrict__ nbr, const int* __restrict__ ncount,
+        CellRec* __restrict__ new_rec, int* __restrict__ new_box, int4* __restrict__ rect,
+        int2* __restrict__ pairs, int* __restrict__ par, int* __restrict__ order, int* __restrict__ grp,
+        int* __restrict__ lineage, int* __restrict__ out, DevStatus* st)
 {
     __shared__ int sd[DIV_SORT_MAX];
-    __shared__ int idl[1 + 1024 + 1];
-    __shared__ int s_len;
+    __shared__ int s_npairs;
     int P2 = 1;
     while (P2 < ndiv) P2 <<= 1;
     for (int i = threadIdx.x; i < P2; i += blockDim.x) sd[i] = i < ndiv ? div_list[i] : 0x7fffffff;
+    if (threadIdx.x == 0) s_npairs = 0;
     __syncthreads();
-    /* bitonic sort, ascending */
     for (int k = 2; k <= P2; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
             for (int i = threadIdx.x; i < P2; i += blockDim.x) {
@@ -526,40 +547,118 @@ __global__ void __launch_bounds__(DIV_THREADS) k_divide(int n_start, int ndiv, i
             }
             __syncthreads();
         }
-    int N = n_start, done = 0;
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int d = 0; d < ndiv; d++) {
-        if (N > cap - 1) { if (threadIdx.x == 0) dev_error(st, BCG_E_MAXCELLS, d); break; }
-        int m = sd[d];
-        if (threadIdx.x == 0) {
-            divide_pair(m, N, draws + 9 * (size_t)d, t, rec, soa, mp);
-            int xi, yi, zi;
-            Cst a = load_cst(&rec[m]), b = load_cst(&rec[N]);
-            int bm = box_address(avg_pq(a.p, a.q), mp, xi, yi, zi);
-            int bd = box_address(avg_pq(b.p, b.q), mp, xi, yi, zi);
-            if (bm < 0) { dev_error(st, BCG_E_OUT_OF_GRID, m); bm = 0; }
-            if (bd < 0) { dev_error(st, BCG_E_OUT_OF_GRID, N); bd = 0; }
-            moved[m] = 1;
-            delta_ids[2 * d] = m; delta_box[2 * d] = bm;
-            delta_ids[2 * d + 1] = N; delta_box[2 * d + 1] = bd;
-            lineage[2 * d] = m; lineage[2 * d + 1] = N;
-            int cnt = ncount[m];
-            s_len = cnt + 2;
-            idl[0] = m;
-            idl[cnt + 1] = N;
-        }
-        __syncthreads();
-        int len = s_len;
-        for (int i = threadIdx.x; i < len - 2; i += blockDim.x) idl[1 + i] = nbr[(size_t)m * mp.kmax + i];
-        __syncthreads();
-        for (int k = warp; k < len; k += nwarps)
-            warp_rebuild_one<true>(idl[k], rec, mp, box_start, box_ids, moved, delta_ids, delta_box, 2 * (d + 1), nbr, ncount, st);
-        __syncthreads();
-        N++; done++;
+    /* the loop stops at the first division that would pass MaxCells */
+    int nd = cap - n_start;
+    if (nd < 0) nd = 0;
+    if (nd > ndiv) nd = ndiv;
+    if (nd < ndiv && threadIdx.x == 0) dev_error(st, BCG_E_MAXCELLS, nd);
+    const int YZ = mp.box_y * mp.box_z;
+    for (int d = threadIdx.x; d < nd; d += blockDim.x) {
+        const int m = sd[d], N = n_start + d;
+        CellRec rm, rd;
+        divide_compute(m, N, draws + 9 * (size_t)d, t, rec, soa, mp, rm, rd);
+        new_rec[2 * d] = rm; new_rec[2 * d + 1] = rd;
+        int xi, yi, zi;
+        int bm = box_address(avg_pq(mk(rm.pL.x, rm.pL.y, rm.pL.z), mk(rm.qR.x, rm.qR.y, rm.qR.z)), mp, xi, yi, zi);
+        int bd = box_address(avg_pq(mk(rd.pL.x, rd.pL.y, rd.pL.z), mk(rd.qR.x, rd.qR.y, rd.qR.z)), mp, xi, yi, zi);
+        if (bm < 0) { dev_error(st, BCG_E_OUT_OF_GRID, m); bm = 0; }
+        if (bd < 0) { dev_error(st, BCG_E_OUT_OF_GRID, N); bd = 0; }
+        new_box[2 * d] = bm; new_box[2 * d + 1] = bd;
+        lineage[2 * d] = m; lineage[2 * d + 1] = N;
+        int b0 = cell_box[m];
+        int x0 = b0 / YZ, z0 = b0 % mp.box_z;
+        int xlo = x0, xhi = x0, zlo = z0, zhi = z0;
+        auto grow_rect = [&](int bb) {
+            int x = bb / YZ, z = bb % mp.box_z;
+            xlo = min(xlo, x); xhi = max(xhi, x); zlo = min(zlo, z); zhi = max(zhi, z);
+        };
+        grow_rect(bm); grow_rect(bd);
+        const int cnt = ncount[m];
+        for (int j = 0; j < cnt; j++) grow_rect(cell_box[nbr[(size_t)m * mp.kmax + j]]);
+        rect[d] = make_int4(xlo - 2, xhi + 2, zlo - 2, zhi + 2);
+        par[d] = d;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 2 * done; i += blockDim.x) moved[delta_ids[i]] = 0;
-    if (threadIdx.x == 0) { out[0] = done; out[1] = N; }
+    /* overlapping footprints */
+    const long np2 = (long)nd * nd;
+    for (long q = threadIdx.x; q < np2; q += blockDim.x) {
+        int a = (int)(q / nd), b = (int)(q % nd);
+        if (a >= b) continue;
+        int4 ra = rect[a], rb = rect[b];
+        if (ra.x <= rb.y && rb.x <= ra.y && ra.z <= rb.w && rb.z <= ra.w) {
+            int k = atomicAdd(&s_npairs, 1);
+            if (k < DIV_PAIR_CAP) pairs[k] = make_int2(a, b);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int npairs = s_npairs;
+        if (npairs > DIV_PAIR_CAP) {
+            for (int d = 0; d < nd; d++) par[d] = 0;      /* too many: one sequential group */
+        } else {
+            for (int k = 0; k < npairs; k++) {
+                int a = pairs[k].x, b = pairs[k].y;
+                while (par[a] != a) a = par[a];
+                while (par[b] != b) b = par[b];
+                if (a != b) { if (a < b) par[b] = a; else par[a] = b; }
+            }
+            for (int d = 0; d < nd; d++) { int r = d; while (par[r] != r) r = par[r]; par[d] = r; }
+        }
+        /* groups in order of their first division; members ascending.
+         * grp[2g] = start in order[], grp[2g+1] = length; roots count
+         * their members in sd[] (free after the sort) */
+        int ng = 0;
+        for (int d = 0; d < nd; d++) sd[d] = 0;
+        for (int d = 0; d < nd; d++) sd[par[d]]++;
+        int pos = 0;
+        for (int d = 0; d < nd; d++)
+            if (par[d] == d) { grp[2 * ng] = pos; grp[2 * ng + 1] = sd[d]; sd[d] = ng; pos += grp[2 * ng + 1]; ng++; }
+        /* members in ascending d */
+        for (int g = 0; g < ng; g++) grp[2 * g + 1] = 0;
+        for (int d = 0; d < nd; d++) {
+            int g = sd[par[d]];
+            order[grp[2 * g] + grp[2 * g + 1]++] = d;
+        }
+        out[0] = nd; out[1] = n_start + nd; out[2] = ng;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_div_groups(int n_start, const int* __restrict__ div_out,
+        const int* __restrict__ grp, const int* __restrict__ order, const int* __restrict__ lineage,
+        const CellRec* __restrict__ new_rec, const int* __restrict__ new_box,
+        CellRec* rec, MechParams mp, int* nbr, int* ncount,
+        const int* __restrict__ box_start, const int* __restrict__ box_ids,
+        int* moved, int* delta_ids, int* delta_box, DevStatus* st)
+{
+    __shared__ int idl_all[4][1 + 1024 + 1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = blockIdx.x * 4 + w;
+    if (g >= div_out[2]) return;                       /* whole warp */
+    int* idl = idl_all[w];
+    const int gs = grp[2 * g], gl = grp[2 * g + 1];
+    int* dids = delta_ids + 2 * gs;
+    int* dbox = delta_box + 2 * gs;
+    for (int j = 0; j < gl; j++) {
+        const int d = order[gs + j];
+        const int m = lineage[2 * d], N = n_start + d;
+        if (lane == 0) {
+            rec[m] = new_rec[2 * d];
+            rec[N] = new_rec[2 * d + 1];
+            moved[m] = 1;
+            dids[2 * j] = m; dbox[2 * j] = new_box[2 * d];
+            dids[2 * j + 1] = N; dbox[2 * j + 1] = new_box[2 * d + 1];
+        }
+        const int cnt = ncount[m];
+        for (int i = lane; i < cnt; i += 32) idl[1 + i] = nbr[(size_t)m * mp.kmax + i];
+        if (lane == 0) { idl[0] = m; idl[cnt + 1] = N; }
+        __threadfence_block();
+        __syncwarp();
+        for (int k = 0; k < cnt + 2; k++)
+            warp_rebuild_one<true>(idl[k], rec, mp, box_start, box_ids, moved, dids, dbox, 2 * (j + 1), nbr, ncount, st);
+        __syncwarp();
+    }
+    __syncwarp();
+    for (int j = lane; j < gl; j += 32) moved[lineage[2 * order[gs + j]]] = 0;
 }
 
 extern "C" int bcg_get_dividing(bcg_ctx* c, int* ids, int capacity)
@@ -593,10 +692,14 @@ extern "C" int bcg_divide(bcg_ctx* c, const float* draws, int n_draw_sets, doubl
         if (rc) return rc;
         memcpy(c->pinned, draws, db);
         BCG_CUDA_TRY(cudaMemcpyAsync(c->draws_dev, c->pinned, db, cudaMemcpyHostToDevice, c->stream));
-        k_divide<<<1, DIV_THREADS, 0, c->stream>>>(c->n, ndiv, c->cap, t, c->draws_dev, c->rec[nb], c->soa,
-            mech_params(c), c->div_list, c->nbr, c->ncount, c->box_start, c->box_ids,
-            c->moved, c->delta_ids, c->delta_box, c->lineage, c->n_done_dev, c->status);
-        c->launches++;
+        MechParams mp = mech_params(c);
+        k_div_plan<<<1, 1024, 0, c->stream>>>(c->n, ndiv, c->cap, t, c->draws_dev, c->rec[nb], c->soa, mp,
+            c->div_list, c->cell_box, c->nbr, c->ncount, c->div_rec, c->div_box, c->div_rect, c->div_pairs,
+            c->div_par, c->div_order, c->div_grp, c->lineage, c->n_done_dev, c->status);
+        k_div_groups<<<(ndiv + 3) / 4, 128, 0, c->stream>>>(c->n, c->n_done_dev, c->div_grp, c->div_order,
+            c->lineage, c->div_rec, c->div_box, c->rec[nb], mp, c->nbr, c->ncount, c->box_start, c->box_ids,
+            c->moved, c->delta_ids, c->delta_box, c->status);
+        c->launches += 2;
         BCG_CUDA_TRY(cudaGetLastError());
         int* hp = (int*)c->pinned;
         BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->n_done_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -608,7 +711,7 @@ extern "C" int bcg_divide(bcg_ctx* c, const float* draws, int n_draw_sets, doubl
         c->n += done;
         c->cur ^= 1;
         c->last_ndiv = 0;
-        timer_end(c, BCG_T_DIVIDE, 6);
+        timer_end(c, BCG_T_DIVIDE, 7);
         if (n_done) *n_done = done;
         return rc;
     }

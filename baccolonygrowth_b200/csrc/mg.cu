@@ -52,7 +52,7 @@ MgLvl mg_lvl(const bcg_ctx* c, int l)
     MgLvl v;
     const MgLevel& L = c->mg[l];
     v.nx = L.nx; v.nz = L.nz; v.pitch = L.pitch;
-    for (int s = 0; s < 3; s++) { v.s[s] = L.sol[s]; v.r[s] = L.res[s]; v.e[s] = L.err[s]; }
+    for (int s = 0; s < 3; s++) { v.s[s] = L.sol[s]; v.r[s] = L.res[s]; v.e[s] = L.err[s]; v.e2[s] = L.err2[s]; }
     return v;
 }
 
@@ -61,7 +61,7 @@ MgLvlF mg_lvl_f(const bcg_ctx* c, int l)
     MgLvlF v;
     const MgLevel& L = c->mg[l];
     v.nx = L.nx; v.nz = L.nz; v.pitch = L.pitch;
-    for (int s = 0; s < 3; s++) { v.s[s] = L.sol[s]; v.r[s] = L.resf[s]; v.e[s] = L.errf[s]; }
+    for (int s = 0; s < 3; s++) { v.s[s] = L.sol[s]; v.r[s] = L.resf[s]; v.e[s] = L.errf[s]; v.e2[s] = L.errf2[s]; }
     return v;
 }
 
@@ -325,6 +325,151 @@ __global__ void __launch_bounds__(1024) k_mg_relax_coarse(MgConst m, MgLvlT<T> L
             }
             __syncthreads();
         }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Fused zebra smoother: S full sweeps (even columns, then odd columns, each */
+/* bottom to top) in one pass over the rows, out of place (E -> E2).        */
+/* ------------------------------------------------------------------------ */
+/* The relaxation formula of relax_point with the stencil values passed in:
+ * below = new value at (i, k-1), up = value at (i, k+1) before this sweep,
+ * xm/xp = values at (i-1, k)/(i+1, k) as the sweep order sees them, old =
+ * the point's value before this sweep (kept where the point is not relaxed).
+ * Same operations in the same order as relax_point. */
+template <class T>
+__device__ __forceinline__ T relax_val(const MgConst& m, int nx, int nz, int l, int sp, int i, int k,
+                                       T r, T below, T up, T xm, T xp, T old, const double* __restrict__ inside0)
+{
+    const T h2 = (T)(m.bl2 * (double)(1 << (2 * l)));
+    const T dt = (T)m.dt, D = (T)m.D[sp];
+    const T half = (T)0.5;
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    const bool side = (i == 0 || i == nx);
+    const T s1 = (i == 0) ? xp : xm;
+    if (k == 0) {
+        int d = 1 << l;
+        int i0 = (i - nx / 2) * d + m.box_x / 2;
+        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+        if (inside0[(size_t)i0 * m.box_z] > 0) return r;
+        if (side) {
+            if (!top_levels) return old;
+            if (oxy) return r;
+            return (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
+        }
+        if (oxy) return r;
+        return (r * h2 / dt / D + up + half * xm + half * xp) / (h2 / dt / D + 2);
+    }
+    if (k == nz) {
+        if (!top_levels) return old;
+        if (side) {
+            if (oxy) return r;
+            return (r * h2 / dt / D + (s1 + below)) / (h2 / dt / D + 2);
+        }
+        return (r * h2 / dt / D + below + half * xp + half * xm) / (h2 / dt / D + 2);
+    }
+    if (side) {
+        if (!top_levels) return old;
+        if (oxy) return r;
+        return (r * h2 / dt / D + half * below + half * up + s1) / (h2 / dt / D + 2);
+    }
+    return (r * h2 / dt / D + half * below + half * up + half * xm + half * xp) / (h2 / dt / D + 2);
+}
+
+template <class T> struct Pair2;
+template <> struct Pair2<double> { typedef double2 type; };
+template <> struct Pair2<float> { typedef float2 type; };
+
+/* Each warp owns a strip of column pairs (lane t: columns c0+2t, c0+2t+1)
+ * and one segment of rows.  Sweep s runs one row behind sweep s-1, so at
+ * row step r sweep s relaxes row r-(s-1) with:
+ *   the even column from the odd neighbours of sweep s-1 (shuffle from
+ *   lane t-1, own odd column), the odd column from the new even
+ *   neighbours of sweep s (own even column, shuffle from lane t+1), the
+ *   value above from sweep s-1 (one row ahead) and the value below from
+ *   sweep s itself.
+ * A sweep's result is exact where all of its inputs were, which loses one
+ * column pair at each strip edge per sweep: lanes S .. 31-S are written.
+ * Segments other than the first start RELAX_WARM_F rows early from the
+ * pre-smoothing values; the row recurrence contracts by at least 1/4 per
+ * row, so the start error is below rounding when the segment's own rows
+ * begin.  Rows above the segment are relaxed by the early sweeps as far
+ * as the later sweeps need them, and only the segment's rows are stored. */
+#define RELAX_WARM_F 40
+template <class T, int S>
+__global__ void __launch_bounds__(128) k_mg_smooth(MgConst m, MgLvlT<T> L, int l, int seg_len,
+                                                   const double* __restrict__ inside0)
+{
+    typedef typename Pair2<T>::type T2;
+    const int lane = threadIdx.x;
+    const int warp = blockIdx.x * blockDim.y + threadIdx.y;
+    const int sp = blockIdx.z;
+    const int nx = L.nx, nz = L.nz, pitch = L.pitch;
+    const int OUTP = 32 - 2 * S;
+    const int c0 = warp * 2 * OUTP - 2 * S;
+    const int ce = c0 + 2 * lane, co = ce + 1;
+    if (warp * 2 * OUTP > nx) return;            /* whole warp: strip starts past the last column */
+    const bool ld_ok = ce >= 0 && co < pitch;
+    const bool st_e = lane >= S && lane <= 31 - S && ce >= 0 && ce <= nx;
+    const bool st_o = lane >= S && lane <= 31 - S && co >= 0 && co <= nx;
+    const int ks = blockIdx.y * seg_len;
+    if (ks > nz) return;
+    const int ke = min(ks + seg_len, nz + 1);
+    const int kw = max(0, ks - RELAX_WARM_F);
+    const T* __restrict__ E = L.e[sp];
+    const T* __restrict__ R = L.r[sp];
+    T* __restrict__ EO = L.e2[sp];
+    auto ld = [&](const T* a, int k) -> T2 {
+        T2 v; v.x = T(0); v.y = T(0);
+        if (ld_ok && k >= 0 && k <= nz) v = *reinterpret_cast<const T2*>(a + (size_t)k * pitch + ce);
+        return v;
+    };
+    /* prv[s]/cur[s]: sweep s's values at its previous/current row; s = 0 is
+     * the input (prv[0] = row r, cur[0] = row r+1) */
+    T2 prv[S + 1], cur[S + 1], rr[S];
+    {
+        T2 e0 = ld(E, kw - 1);
+#pragma unroll
+        for (int s = 1; s <= S; s++) { prv[s] = e0; cur[s] = e0; }
+        prv[0] = ld(E, kw);
+        cur[0] = ld(E, kw + 1);
+#pragma unroll
+        for (int s = 0; s < S; s++) { rr[s].x = T(0); rr[s].y = T(0); }
+    }
+    T2 nr = ld(R, kw), ne = ld(E, kw + 2);
+    const int r_end = ke - 1 + (S - 1);
+    for (int r = kw; r <= r_end; r++) {
+        /* R of row r enters the ring (rr[s-1] = R at sweep s's row) */
+#pragma unroll
+        for (int s = S - 1; s > 0; s--) rr[s] = rr[s - 1];
+        rr[0] = nr;
+        T2 pr = ld(R, r + 1), pe = ld(E, r + 3);   /* prefetch for the next step */
+#pragma unroll
+        for (int s = 1; s <= S; s++) {
+            const int k = r - (s - 1);
+            const int top = min(nz, ke - 1 + (S - s));
+            if (k < kw || k > top) { cur[s] = prv[s]; continue; }
+            /* even column */
+            T xm = __shfl_up_sync(0xffffffffu, prv[s - 1].y, 1);
+            T ve = relax_val<T>(m, nx, nz, l, sp, ce, k, rr[s - 1].x, prv[s].x, cur[s - 1].x, xm, prv[s - 1].y,
+                                prv[s - 1].x, inside0);
+            T xp = __shfl_down_sync(0xffffffffu, ve, 1);
+            T vo = relax_val<T>(m, nx, nz, l, sp, co, k, rr[s - 1].y, prv[s].y, cur[s - 1].y, ve, xp,
+                                prv[s - 1].y, inside0);
+            cur[s].x = ve; cur[s].y = vo;
+        }
+        const int kS = r - (S - 1);
+        if (kS >= ks && kS < ke) {
+            T* dst = EO + (size_t)kS * pitch;
+            if (st_e && st_o) *reinterpret_cast<T2*>(dst + ce) = cur[S];
+            else if (st_e) dst[ce] = cur[S].x;
+        }
+#pragma unroll
+        for (int s = 1; s <= S; s++) prv[s] = cur[s];
+        prv[0] = cur[0];
+        cur[0] = ne;
+        nr = pr; ne = pe;
+    }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -612,8 +757,16 @@ __global__ void k_mg_copy_from(MgLvl L, int X, double* cC, double* cO, double* c
 /* ------------------------------------------------------------------------ */
 static inline dim3 grid2(int n, int threads) { return dim3((unsigned)((n + threads - 1) / threads), 3); }
 
-static int g_relax_mode = 1;   /* 0 = one thread per column, 1 = segmented */
-extern "C" int bcg_set_relax_mode(int mode) { if (mode < 0 || mode > 1) return BCG_E_ARG; g_relax_mode = mode; return BCG_OK; }
+/* 0 = one thread per column and half-sweep, 1 = segmented half-sweeps,
+ * 2 = fused sweeps (k_mg_smooth) on levels taller than 96 rows */
+static int g_relax_mode = 2;
+extern "C" int bcg_set_relax_mode(int mode)
+{
+    if (mode < 0 || mode > 2) return BCG_E_ARG;
+    if (mode != g_relax_mode) bcg_kernel_config_changed();
+    g_relax_mode = mode;
+    return BCG_OK;
+}
 
 template <class T> static MgLvlT<T> lvl(const bcg_ctx* c, int l);
 template <> MgLvlT<double> lvl<double>(const bcg_ctx* c, int l) { return mg_lvl(c, l); }
@@ -642,12 +795,55 @@ static void relax_level(bcg_ctx* c, const MgConst& m, int l)
     c->launches += 2;
 }
 
+template <class T> static void swap_err(bcg_ctx* c, int l);
+template <> void swap_err<double>(bcg_ctx* c, int l)
+{
+    for (int sp = 0; sp < 3; sp++) { double* t = c->mg[l].err[sp]; c->mg[l].err[sp] = c->mg[l].err2[sp]; c->mg[l].err2[sp] = t; }
+}
+template <> void swap_err<float>(bcg_ctx* c, int l)
+{
+    for (int sp = 0; sp < 3; sp++) { float* t = c->mg[l].errf[sp]; c->mg[l].errf[sp] = c->mg[l].errf2[sp]; c->mg[l].errf2[sp] = t; }
+}
+
+/* `sweeps` zebra sweeps of level l.  In mode 2 tall levels take the fused
+ * kernel, up to 3 sweeps per launch; each launch swaps the level's two
+ * correction buffers.  Pre- and post-smoothing use the same number of
+ * launches, so a V-cycle always swaps an even number of times and leaves
+ * the buffers where it found them (captured graphs rely on this). */
+template <class T>
+static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
+{
+    const int rows = c->mg[l].nz + 1;
+    if (g_relax_mode != 2 || rows <= 96) {
+        for (int j = 0; j < sweeps; j++) relax_level<T>(c, m, l);
+        return;
+    }
+    while (sweeps > 0) {
+        const int S = sweeps >= 3 ? 3 : sweeps;
+        MgLvlT<T> L = lvl<T>(c, l);
+        const int outp = 32 - 2 * S;
+        const int nwx = (L.nx + 1 + 2 * outp - 1) / (2 * outp);
+        int nseg = (1400 + 3 * nwx - 1) / (3 * nwx);
+        const int max_seg = rows / 64 > 1 ? rows / 64 : 1;
+        if (nseg > max_seg) nseg = max_seg;
+        if (nseg < 1) nseg = 1;
+        const int seg_len = (rows + nseg - 1) / nseg;
+        dim3 block(32, 4), grid((unsigned)((nwx + 3) / 4), (unsigned)nseg, 3);
+        if (S == 3) k_mg_smooth<T, 3><<<grid, block, 0, c->stream>>>(m, L, l, seg_len, c->inside);
+        else if (S == 2) k_mg_smooth<T, 2><<<grid, block, 0, c->stream>>>(m, L, l, seg_len, c->inside);
+        else k_mg_smooth<T, 1><<<grid, block, 0, c->stream>>>(m, L, l, seg_len, c->inside);
+        c->launches++;
+        swap_err<T>(c, l);
+        sweeps -= S;
+    }
+}
+
 /* mu2 sweeps on the coarsest level: fused when it fits one block */
 template <class T>
 static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
     MgLvlT<T> L = lvl<T>(c, l);
-    if (g_relax_mode == 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
+    if (g_relax_mode >= 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
         k_mg_relax_coarse<T><<<1, 1024, 0, c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
     } else {
@@ -661,7 +857,7 @@ void mg_vcycle_t(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
 {
     const int Lv = c->mg_levels;
     for (int l = 0; l < Lv - 1; l++) {
-        for (int j = 0; j < mu1; j++) relax_level<T>(c, m, l);
+        smooth_level<T>(c, m, l, mu1);
         MgLvlT<T> Lc = lvl<T>(c, l + 1), Lf = lvl<T>(c, l);
         k_mg_restrict<T><<<grid2((Lc.nx + 1) * (Lc.nz + 1), 256), 256, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
         c->launches++;
@@ -671,7 +867,7 @@ void mg_vcycle_t(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
         MgLvlT<T> Lf = lvl<T>(c, l), Lc = lvl<T>(c, l + 1);
         k_mg_interp<T><<<grid2((Lf.nx + 1) * (Lf.nz + 1), 256), 256, 0, c->stream>>>(m, Lf, Lc, l);
         c->launches++;
-        for (int j = 0; j < mu1; j++) relax_level<T>(c, m, l);
+        smooth_level<T>(c, m, l, mu1);
     }
 }
 template void mg_vcycle_t<double>(bcg_ctx*, const MgConst&, int, int);

@@ -20,6 +20,7 @@ struct MgLvlT {
     double* s[3];
     T* r[3];
     T* e[3];
+    T* e2[3];         /* the other correction buffer (fused smoother output) */
 };
 typedef MgLvlT<double> MgLvl;
 typedef MgLvlT<float> MgLvlF;

@@ -146,13 +146,14 @@ def test_colony_sweeps_odd_count(gpu):
 
 
 def test_segmented_smoother_matches_sequential(gpu):
-    """The segmented zebra sweep (default) reproduces the one-thread-per-
-    column sweep to rounding on a grid tall enough to be segmented."""
+    """The segmented half-sweeps (mode 1) and the fused sweeps (mode 2, the
+    default) reproduce the one-thread-per-column sweep (mode 0) to rounding
+    on a grid tall enough to be segmented."""
     lib = _abi.load()
     p = params.workload_params("scale_262k")
     cells = workload_colony("scale_262k", n=20000)
     out = []
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         assert lib.bcg_set_relax_mode(mode) == 0
         col = Colony(p, cells)
         col.update_density()
@@ -160,10 +161,11 @@ def test_segmented_smoother_matches_sequential(gpu):
         col.mg_solve(2)
         out.append([col.field("MG_SOL_" + sp, l) for l in range(3) for sp in ("CARBON", "OXYGEN", "ACETATE")])
         col.close()
-    lib.bcg_set_relax_mode(1)
+    lib.bcg_set_relax_mode(2)
     assert np.ptp(out[0][0]) > 0          # carbon level 0 is no longer uniform
-    for a, b in zip(*out):
-        assert close(a, b) <= 1e-14
+    for other in (1, 2):
+        for a, b in zip(out[0], out[other]):
+            assert close(a, b) <= 1e-14, other
 
 
 def _solve_state(col, p):
@@ -183,16 +185,34 @@ def test_tolerance_solve_fixed_cycles_equals_solve(gpu):
         assert np.array_equal(x, y)
 
 
-@pytest.mark.parametrize("workload,n", [("small_4k", 4096), ("scale_262k", 40000)])
-def test_mixed_precision_reaches_fp64_tolerance(gpu, workload, n):
-    p = params.workload_params(workload)
-    cells = workload_colony(workload, n=n)
-    ref = Colony(p, cells); ref.update_density(); ref.deplete_wall()
-    it64, rel64 = ref.mg_solve_tol(1e-8, 64, 60)
-    mix = Colony(p, cells); mix.update_density(); mix.deplete_wall()
-    it32, rel32 = mix.mg_solve_tol(1e-8, 32, 60)
-    assert it64 > 1 and it32 > 1, (it64, it32)
-    assert rel64 < 1e-8 and rel32 < 1e-8, (it64, rel64, it32, rel32)
-    # both solve the same system to the same tolerance
-    for x, y in zip(_solve_state(ref, p), _solve_state(mix, p)):
-        assert close(x, y) <= 1e-9
+def test_mixed_precision_reaches_fp64_tolerance(gpu):
+    """FP64 V-cycles and FP32 V-cycles + FP64 refinement both reach a 1e-8
+    relative defect, and both solutions lie within 5e-8 (relative to the
+    field's maximum) of a 1e-12 FP64 solve of the same system."""
+    p = params.workload_params("scale_262k")
+    cells = workload_colony("scale_262k", n=40000)
+    sols = {}
+    for key, tol, prec in (("tight", 1e-12, 64), ("fp64", 1e-8, 64), ("mixed", 1e-8, 32)):
+        col = Colony(p, cells); col.update_density(); col.deplete_wall()
+        it, rel = col.mg_solve_tol(tol, prec, 80)
+        assert it > 1 and rel < tol, (key, it, rel)
+        sols[key] = _solve_state(col, p)
+        col.close()
+    for key in ("fp64", "mixed"):
+        for x, y in zip(sols["tight"], sols[key]):
+            assert close(x, y) <= 5e-8, key
+
+
+def test_tolerance_solve_reports_stagnation(gpu):
+    """On the small input's grid (coarsest levels of 0 and 1 interior rows)
+    the reference's composite V-cycle stalls near a 1e-2 relative defect and
+    then drifts (the C restatement shows the same).  The tolerance solve
+    runs to max_iters and returns the defect it reached instead of claiming
+    convergence."""
+    p = params.workload_params("small_4k")
+    cells = workload_colony("small_4k", n=4096)
+    for prec in (64, 32):
+        col = Colony(p, cells); col.update_density(); col.deplete_wall()
+        it, rel = col.mg_solve_tol(1e-8, prec, 20)
+        assert it == 20 and rel > 1e-8, (prec, it, rel)
+        col.close()

@@ -18,9 +18,11 @@ REL_TOL = 1e-10
 pytestmark = pytest.mark.gpu
 
 
-def setup_pair(n=4096, seed=12345, spread=1.0, growth=0.9, workload="small_4k"):
+def setup_pair(n=4096, seed=12345, spread=1.0, growth=0.9, workload="small_4k", mutate=None):
     p = params.workload_params(workload)
     cells = workload_colony(workload, n=n, div_phase_spread=spread)
+    if mutate is not None:
+        mutate(cells)
     orc = ck.Oracle(p, seed=seed)
     orc.load(cells)
     orc.update_height()
@@ -92,6 +94,29 @@ def test_multi_step_divisions(gpu):
     assert nbr_sets(orc.neighbours()) == nbr_sets(col.neighbours())
 
 
+def test_crowded_divisions(gpu):
+    """Half of the cells divide in the same step, so most divisions have
+    neighbouring divisions whose footprints overlap: the device runs them
+    in groups, and the result must equal the reference's one-by-one loop
+    (lineage, cells, neighbour sets), also over the following steps."""
+    def mutate(cells):
+        r = np.random.default_rng(5)
+        pick = r.random(len(cells)) < 0.5
+        cells["ldiv"][pick] = cells["length"][pick]     # divide after this step's growth
+    p, orc, col, rng = setup_pair(mutate=mutate)
+    col.rebuild_neighbours()
+    t = 0.0
+    for s in range(3):
+        _, calls_o, lin_o = orc.step(p.dt, t)
+        lin = col.step(p.dt, t, rng)
+        assert np.array_equal(lin, lin_o), s
+        if s == 0:
+            assert len(lin) > 1000
+        t += p.dt
+    assert_cells_close(orc.cells(), col.cells())
+    assert nbr_sets(orc.neighbours()) == nbr_sets(col.neighbours())
+
+
 def test_neighbour_refresh_after_steps(gpu):
     p, orc, col, rng = setup_pair()
     col.rebuild_neighbours()
@@ -126,8 +151,10 @@ def test_out_of_grid_is_reported(gpu):
     cells["p"][5, 0] = 1e6   # far outside the box grid
     cells["q"][5, 0] = 1e6 + 2
     col = Colony(p, cells)
+    # entries are asynchronous: the error surfaces at the next synchronising call
     with pytest.raises(_abi.BcgError) as e:
         col.rebuild_neighbours()
+        col.synchronize()
     assert e.value.code == _abi.E_OUT_OF_GRID
     # the context stays usable after the error
     cells["p"][5, 0] = 0.0
