@@ -195,6 +195,7 @@ PROTOTYPES = {
     "bcg_mg_solve": (_I, [_VP, _I]),
     "bcg_colony_sweeps": (_I, [_VP, _I, _I]),
     "bcg_mg_solve_tol": (_I, [_VP, _D, _I, _I, _PI, _PD]),
+    "bcg_autotune": (_I, [_VP, _I, _PI]),
     "bcg_enable_timers": (_I, [_VP, _I]),
     "bcg_get_timer": (_I, [_VP, _I, _PD, _PI64]),
     "bcg_rng_seed": (None, [ctypes.POINTER(Rng), ctypes.c_uint32]),
@@ -220,6 +221,8 @@ EXTRA_PROTOTYPES = {
     "bcg_set_bbox": (_I, [_VP, _I, _I, _I]),
     "bcg_set_relax_mode": (_I, [_I]),
 }
+
+TUNE = dict(FORCE_GROUP=1, SMOOTHER=2)
 
 _lib = None
 

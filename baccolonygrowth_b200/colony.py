@@ -232,6 +232,12 @@ class Colony:
         _abi.check(self.lib.bcg_get_timer(self.h, _abi.TIMERS[name], ctypes.byref(ms), ctypes.byref(n)), "bcg_get_timer")
         return ms.value, n.value
 
+    def autotune(self, what):
+        """bcg_autotune: 'FORCE_GROUP' or 'SMOOTHER'; returns the choice."""
+        ch = ctypes.c_int()
+        _abi.check(self.lib.bcg_autotune(self.h, _abi.TUNE[what], ctypes.byref(ch)), "bcg_autotune")
+        return ch.value
+
     def synchronize(self):
         _abi.check(self.lib.bcg_synchronize(self.h), "bcg_synchronize")
 

@@ -99,6 +99,9 @@ struct bcg_ctx {
     double timer_ms[BCG_T_COUNT];
     long long timer_launches[BCG_T_COUNT];
     long long launches;    /* kernels queued by this context (all kinds) */
+    /* kernel shapes chosen by bcg_autotune for this context (0 = default) */
+    int force_group;
+    int smooth_warps;
 };
 
 MechParams mech_params(const bcg_ctx* c);
@@ -110,3 +113,7 @@ int ensure_pinned(bcg_ctx* c, size_t bytes);
 /* bumped whenever a kernel variant is switched (captured graphs go stale) */
 int bcg_kernel_config_generation();
 void bcg_kernel_config_changed();
+void nutrient_graphs_drop(bcg_ctx* c);
+int launch_move_grow(bcg_ctx* c, double dt, int group);
+int mg_tune_smoother(bcg_ctx* c, int* choice);
+int mg_kernel_attributes();

@@ -394,10 +394,8 @@ extern "C" int bcg_set_force_group(int g)
 /* Cells are walked in the order of the last binning (spatially coherent,
  * so neighbouring groups share record lines in L1/L2); cells created after
  * that binning follow in id order. */
-extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_calls)
+int launch_move_grow(bcg_ctx* c, double dt, int group)
 {
-    if (!c) return BCG_E_ARG;
-    timer_begin(c, BCG_T_MOVE_GROW);
     int n = c->n;
     BCG_CUDA_TRY(cudaMemsetAsync(c->div_count, 0, sizeof(int), c->stream));
     BCG_CUDA_TRY(cudaMemsetAsync(c->fcw_count, 0, sizeof(unsigned long long), c->stream));
@@ -406,11 +404,11 @@ extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_cal
         FieldPtrs fp = field_ptrs(c);
         int nb = c->n_binned < n ? c->n_binned : n;
         const int threads = 256;
-        long tot = (long)n * g_group;
+        long tot = (long)n * group;
         unsigned blocks = (unsigned)((tot + threads - 1) / threads);
         const CellRec* old = c->rec[c->cur];
         CellRec* nw = c->rec[c->cur ^ 1];
-        switch (g_group) {
+        switch (group) {
         case 1: k_move_grow<1><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
         case 2: k_move_grow<2><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
         case 4: k_move_grow<4><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
@@ -420,16 +418,80 @@ extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_cal
         c->launches++;
         BCG_CUDA_TRY(cudaGetLastError());
     }
-    timer_end(c, BCG_T_MOVE_GROW, n > 0 ? 1 : 0);
+    return BCG_OK;
+}
+
+extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_calls)
+{
+    if (!c) return BCG_E_ARG;
+    timer_begin(c, BCG_T_MOVE_GROW);
+    int rc = launch_move_grow(c, dt, c->force_group ? c->force_group : g_group);
+    if (rc) return rc;
+    timer_end(c, BCG_T_MOVE_GROW, c->n > 0 ? 1 : 0);
     /* the two counters are the only values the host needs this step */
     int* hp = (int*)c->pinned;
     BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->div_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     BCG_CUDA_TRY(cudaMemcpyAsync(hp + 2, c->fcw_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
-    int rc = ctx_check_status(c);
+    rc = ctx_check_status(c);
     if (rc) return rc;
     c->last_ndiv = hp[0];
     if (n_div) *n_div = hp[0];
     if (fcw_calls) *fcw_calls = (int64_t)(*(unsigned long long*)(hp + 2));
+    return BCG_OK;
+}
+
+/* time `reps` launches of MoveCell+GrowCell with `group` lanes per cell;
+ * the records of the current buffer are read only, so the state is kept */
+static int time_move_grow(bcg_ctx* c, int group, int reps, float* ms)
+{
+    cudaEvent_t a, b;
+    BCG_CUDA_TRY(cudaEventCreate(&a));
+    BCG_CUDA_TRY(cudaEventCreate(&b));
+    int rc = launch_move_grow(c, c->P.dt, group);           /* warm-up */
+    if (!rc) rc = (cudaEventRecord(a, c->stream) == cudaSuccess) ? BCG_OK : BCG_E_CUDA;
+    for (int r = 0; r < reps && !rc; r++) rc = launch_move_grow(c, c->P.dt, group);
+    if (!rc) rc = (cudaEventRecord(b, c->stream) == cudaSuccess) ? BCG_OK : BCG_E_CUDA;
+    if (!rc) rc = (cudaEventSynchronize(b) == cudaSuccess) ? BCG_OK : BCG_E_CUDA;
+    if (!rc) cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+}
+
+extern "C" int bcg_autotune(bcg_ctx* c, int what, int* choice)
+{
+    if (!c) return BCG_E_ARG;
+    if (what == BCG_TUNE_SMOOTHER) return mg_tune_smoother(c, choice);
+    if (what != BCG_TUNE_FORCE_GROUP) return BCG_E_ARG;
+    if (c->n == 0) { if (choice) *choice = c->force_group ? c->force_group : g_group; return BCG_OK; }
+    const int saved_ndiv = c->last_ndiv;
+    /* the trial launches rewrite the per-cell outputs of a step (growth
+     * rate, friction accumulators): keep a copy and put it back */
+    double* keep[7] = {c->soa.gr, c->soa.dfx, c->soa.dfy, c->soa.dfz, c->soa.sfx, c->soa.sfy, c->soa.sfz};
+    const size_t nb = (size_t)c->n * sizeof(double);
+    double* save = nullptr;
+    BCG_CUDA_TRY(cudaMallocAsync((void**)&save, 7 * nb, c->stream));
+    for (int a = 0; a < 7; a++)
+        BCG_CUDA_TRY(cudaMemcpyAsync(save + a * (size_t)c->n, keep[a], nb, cudaMemcpyDeviceToDevice, c->stream));
+    const int groups[5] = {1, 2, 4, 8, 16};
+    float best = 3.4e38f;
+    int best_g = g_group;
+    int rc = BCG_OK;
+    for (int gi = 0; gi < 5 && !rc; gi++) {
+        float ms = 0;
+        rc = time_move_grow(c, groups[gi], 3, &ms);
+        if (!rc && ms < best) { best = ms; best_g = groups[gi]; }
+    }
+    for (int a = 0; a < 7; a++)
+        cudaMemcpyAsync(keep[a], save + a * (size_t)c->n, nb, cudaMemcpyDeviceToDevice, c->stream);
+    cudaFreeAsync(save, c->stream);
+    int rc2 = ctx_check_status(c);
+    c->last_ndiv = saved_ndiv;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (best_g != c->force_group) { c->force_group = best_g; nutrient_graphs_drop(c); }
+    if (best_g != g_group) { g_group = best_g; bcg_kernel_config_changed(); }   /* default for new contexts */
+    if (choice) *choice = best_g;
     return BCG_OK;
 }
 

@@ -34,6 +34,34 @@ __device__ __forceinline__ P at_ref(const P* a, const LV& L, int i, int k)
     return AT(a, L, i2, k2);
 }
 
+/* The relaxation update of relaxationAgarElementwise (Multigrid.cpp:160-249)
+ *   E = (R h^2/(dt D) + sum of weighted neighbours) / (h^2/(dt D) + 2)
+ * with cf = h^2/(dt D) and 1/(cf + 2) computed once per level and species
+ * (the reference divides per point; the results differ by rounding). */
+template <class T> struct RelaxK { T cf, inv; };
+template <class T>
+__device__ __forceinline__ RelaxK<T> relax_k(const MgConst& m, int l, int sp)
+{
+    const double cf = m.bl2 * (double)(1 << (2 * l)) / m.dt / m.D[sp];
+    RelaxK<T> k; k.cf = (T)cf; k.inv = (T)(1.0 / (cf + 2.0));
+    return k;
+}
+/* interior: neighbours below, above, left, right with weight 1/2 */
+template <class T> __device__ __forceinline__ T rx_in(T r, T b, T u, T xm, T xp, const RelaxK<T>& K)
+{ return fma(r, K.cf, T(0.5) * ((b + u) + (xm + xp))) * K.inv; }
+/* bottom row (k = 0): above weight 1, sides 1/2 */
+template <class T> __device__ __forceinline__ T rx_k0(T r, T u, T xm, T xp, const RelaxK<T>& K)
+{ return fma(r, K.cf, u + T(0.5) * (xm + xp)) * K.inv; }
+/* top row (k = nz): below weight 1, sides 1/2 */
+template <class T> __device__ __forceinline__ T rx_top(T r, T b, T xm, T xp, const RelaxK<T>& K)
+{ return fma(r, K.cf, b + T(0.5) * (xm + xp)) * K.inv; }
+/* side column (i = 0 or nx), interior row: inner neighbour weight 1 */
+template <class T> __device__ __forceinline__ T rx_side(T r, T b, T u, T s1, const RelaxK<T>& K)
+{ return fma(r, K.cf, T(0.5) * (b + u) + s1) * K.inv; }
+/* corners: inner neighbour and the one vertical neighbour, weight 1 each */
+template <class T> __device__ __forceinline__ T rx_corner(T r, T s1, T v, const RelaxK<T>& K)
+{ return fma(r, K.cf, s1 + v) * K.inv; }
+
 MgConst mg_const(const bcg_ctx* c, double dt)
 {
     MgConst m;
@@ -73,9 +101,7 @@ __device__ __forceinline__ void relax_point(const MgConst& m, const MgLvlT<T>& L
                                             const double* __restrict__ inside0, T& e_below, bool have_below)
 {
     const int nx = L.nx, nz = L.nz;
-    const T h2 = (T)(m.bl2 * (double)(1 << (2 * l)));
-    const T dt = (T)m.dt, D = (T)m.D[sp];
-    const T half = (T)0.5;
+    const RelaxK<T> K = relax_k<T>(m, l, sp);
     T* E = L.e[sp];
     const T* R = L.r[sp];
     const bool oxy = (sp == 1);
@@ -92,44 +118,26 @@ __device__ __forceinline__ void relax_point(const MgConst& m, const MgLvlT<T>& L
         else if (i == 0 || i == nx) {
             if (top_levels) {
                 if (oxy) out = r;
-                else {
-                    T s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
-                    T up = at_ref(E, L, i, 1);
-                    out = (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
-                }
+                else out = rx_corner(r, (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0), at_ref(E, L, i, 1), K);
             } else write = false;
         } else {
             if (oxy) out = r;
-            else {
-                T up = at_ref(E, L, i, 1), xm = AT(E, L, i - 1, 0), xp = AT(E, L, i + 1, 0);
-                out = (r * h2 / dt / D + up + half * xm + half * xp) / (h2 / dt / D + 2);
-            }
+            else out = rx_k0(r, at_ref(E, L, i, 1), AT(E, L, i - 1, 0), AT(E, L, i + 1, 0), K);
         }
     } else if (k == nz) {
         if (top_levels) {
             if (i == 0 || i == nx) {
                 if (oxy) out = r;
-                else {
-                    T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
-                    out = (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
-                }
-            } else {
-                T xp = AT(E, L, i + 1, k), xm = AT(E, L, i - 1, k);
-                out = (r * h2 / dt / D + e_dn + half * xp + half * xm) / (h2 / dt / D + 2);
-            }
+                else out = rx_corner(r, (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k), e_dn, K);
+            } else out = rx_top(r, e_dn, AT(E, L, i - 1, k), AT(E, L, i + 1, k), K);
         } else write = false;
     } else if (i == 0 || i == nx) {
         if (top_levels) {
             if (oxy) out = r;
-            else {
-                T up = AT(E, L, i, k + 1);
-                T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
-                out = (r * h2 / dt / D + half * e_dn + half * up + s1) / (h2 / dt / D + 2);
-            }
+            else out = rx_side(r, e_dn, AT(E, L, i, k + 1), (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k), K);
         } else write = false;
     } else {
-        T up = AT(E, L, i, k + 1), xm = AT(E, L, i - 1, k), xp = AT(E, L, i + 1, k);
-        out = (r * h2 / dt / D + half * e_dn + half * up + half * xm + half * xp) / (h2 / dt / D + 2);
+        out = rx_in(r, e_dn, AT(E, L, i, k + 1), AT(E, L, i - 1, k), AT(E, L, i + 1, k), K);
     }
     if (write) AT(E, L, i, k) = out;
     e_below = write ? out : AT(E, L, i, k);
@@ -144,13 +152,12 @@ __device__ __forceinline__ double relax_eval(const MgConst& m, const MgLvlT<T>& 
                                              const double* __restrict__ inside0, int& kind, double& cfac)
 {
     const int nx = L.nx, nz = L.nz;
-    const double h2 = m.bl2 * (double)(1 << (2 * l));
-    const double dt = m.dt, D = m.D[sp];
+    const RelaxK<double> K = relax_k<double>(m, l, sp);
     const T* E = L.e[sp];
     const double r = AT(R64, L, i, k);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
-    cfac = h2 / dt / D;
+    cfac = K.cf;
     kind = 2;
     if (k == 0) {
         int d = 1 << l;
@@ -161,10 +168,10 @@ __device__ __forceinline__ double relax_eval(const MgConst& m, const MgLvlT<T>& 
             if (!top_levels) { kind = 0; return 0.0; }
             if (oxy) { kind = 1; return r; }
             double s1 = (i == 0) ? (double)AT(E, L, i + 1, 0) : (double)AT(E, L, i - 1, 0);
-            return (r * h2 / dt / D + (s1 + (double)at_ref(E, L, i, 1))) / (h2 / dt / D + 2);
+            return rx_corner(r, s1, (double)at_ref(E, L, i, 1), K);
         }
         if (oxy) { kind = 1; return r; }
-        return (r * h2 / dt / D + (double)at_ref(E, L, i, 1) + 0.5 * (double)AT(E, L, i - 1, 0) + 0.5 * (double)AT(E, L, i + 1, 0)) / (h2 / dt / D + 2);
+        return rx_k0(r, (double)at_ref(E, L, i, 1), (double)AT(E, L, i - 1, 0), (double)AT(E, L, i + 1, 0), K);
     }
     const double e_dn = (double)AT(E, L, i, k - 1);
     if (k == nz) {
@@ -172,17 +179,17 @@ __device__ __forceinline__ double relax_eval(const MgConst& m, const MgLvlT<T>& 
         if (i == 0 || i == nx) {
             if (oxy) { kind = 1; return r; }
             double s1 = (i == 0) ? (double)AT(E, L, i + 1, k) : (double)AT(E, L, i - 1, k);
-            return (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
+            return rx_corner(r, s1, e_dn, K);
         }
-        return (r * h2 / dt / D + e_dn + 0.5 * (double)AT(E, L, i + 1, k) + 0.5 * (double)AT(E, L, i - 1, k)) / (h2 / dt / D + 2);
+        return rx_top(r, e_dn, (double)AT(E, L, i - 1, k), (double)AT(E, L, i + 1, k), K);
     }
     if (i == 0 || i == nx) {
         if (!top_levels) { kind = 0; return 0.0; }
         if (oxy) { kind = 1; return r; }
         double s1 = (i == 0) ? (double)AT(E, L, i + 1, k) : (double)AT(E, L, i - 1, k);
-        return (r * h2 / dt / D + 0.5 * e_dn + 0.5 * (double)AT(E, L, i, k + 1) + s1) / (h2 / dt / D + 2);
+        return rx_side(r, e_dn, (double)AT(E, L, i, k + 1), s1, K);
     }
-    return (r * h2 / dt / D + 0.5 * e_dn + 0.5 * (double)AT(E, L, i, k + 1) + 0.5 * (double)AT(E, L, i - 1, k) + 0.5 * (double)AT(E, L, i + 1, k)) / (h2 / dt / D + 2);
+    return rx_in(r, e_dn, (double)AT(E, L, i, k + 1), (double)AT(E, L, i - 1, k), (double)AT(E, L, i + 1, k), K);
 }
 
 /* one thread per (column of the given parity, species), bottom to top */
@@ -236,15 +243,12 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvlT<T> L, in
     }
     __syncthreads();
     if (!active || k_begin > nz) return;
-    const T h2 = (T)(m.bl2 * (double)(1 << (2 * l)));
-    const T dt = (T)m.dt, D = (T)m.D[sp];
-    const T half = (T)0.5;
     const T* R = L.r[sp];
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
     const int nx = L.nx;
     const bool side = (i == 0 || i == nx);
-    T xm_, xp_;
+    const RelaxK<T> K = relax_k<T>(m, l, sp);
     for (int k = k_start; k < k_end; k++) {
         const bool warm = k < k_begin;
         T r = AT(R, L, i, k);
@@ -260,42 +264,26 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvlT<T> L, in
             else if (side) {
                 if (top_levels) {
                     if (oxy) out = r;
-                    else {
-                        T s1 = (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0);
-                        out = (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
-                    }
+                    else out = rx_corner(r, (i == 0) ? AT(E, L, i + 1, 0) : AT(E, L, i - 1, 0), up, K);
                 } else write = false;
             } else {
                 if (oxy) out = r;
-                else {
-                    xm_ = AT(E, L, i - 1, 0); xp_ = AT(E, L, i + 1, 0);
-                    out = (r * h2 / dt / D + up + half * xm_ + half * xp_) / (h2 / dt / D + 2);
-                }
+                else out = rx_k0(r, up, AT(E, L, i - 1, 0), AT(E, L, i + 1, 0), K);
             }
         } else if (k == nz) {
             if (top_levels) {
                 if (side) {
                     if (oxy) out = r;
-                    else {
-                        T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
-                        out = (r * h2 / dt / D + (s1 + e_dn)) / (h2 / dt / D + 2);
-                    }
-                } else {
-                    xp_ = AT(E, L, i + 1, k); xm_ = AT(E, L, i - 1, k);
-                    out = (r * h2 / dt / D + e_dn + half * xp_ + half * xm_) / (h2 / dt / D + 2);
-                }
+                    else out = rx_corner(r, (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k), e_dn, K);
+                } else out = rx_top(r, e_dn, AT(E, L, i - 1, k), AT(E, L, i + 1, k), K);
             } else write = false;
         } else if (side) {
             if (top_levels) {
                 if (oxy) out = r;
-                else {
-                    T s1 = (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k);
-                    out = (r * h2 / dt / D + half * e_dn + half * up + s1) / (h2 / dt / D + 2);
-                }
+                else out = rx_side(r, e_dn, up, (i == 0) ? AT(E, L, i + 1, k) : AT(E, L, i - 1, k), K);
             } else write = false;
         } else {
-            xm_ = AT(E, L, i - 1, k); xp_ = AT(E, L, i + 1, k);
-            out = (r * h2 / dt / D + half * e_dn + half * up + half * xm_ + half * xp_) / (h2 / dt / D + 2);
+            out = rx_in(r, e_dn, up, AT(E, L, i - 1, k), AT(E, L, i + 1, k), K);
         }
         /* points that are not relaxed keep their value; those columns and
          * rows (composite edges) are written by no thread in this sweep */
@@ -327,22 +315,95 @@ __global__ void __launch_bounds__(1024) k_mg_relax_coarse(MgConst m, MgLvlT<T> L
         }
 }
 
+/* All mu2 relaxations of the coarsest level with the level held in shared
+ * memory: one block per species, E and R of that species copied in (row k
+ * at offset k*(nx+1)), even then odd columns per sweep with a block barrier
+ * between half-sweeps, E copied back.  Reads outside 0..nz follow the
+ * reference's flat index i*(nz+1)+k like at_ref. */
+template <class T>
+__device__ __forceinline__ T at_s(const T* a, int nx, int nz, int i, int k)
+{
+    if (k >= 0 && k <= nz) return a[k * (nx + 1) + i];
+    long f = (long)i * (nz + 1) + k;
+    long n = (long)(nx + 1) * (nz + 1);
+    if (f < 0 || f >= n) return T(0);
+    return a[(int)(f % (nz + 1)) * (nx + 1) + (int)(f / (nz + 1))];
+}
+template <class T>
+__global__ void __launch_bounds__(1024) k_mg_coarse_smem(MgConst m, MgLvlT<T> L, int l, int sweeps,
+                                                         const double* __restrict__ inside0)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int sp = blockIdx.x;
+    const int nx = L.nx, nz = L.nz, W = nx + 1;
+    const int np = W * (nz + 1);
+    T* Es = reinterpret_cast<T*>(smem_raw);
+    T* Rs = Es + np;
+    T* E = L.e[sp];
+    const T* R = L.r[sp];
+    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        int i = q % W, k = q / W;
+        Es[q] = AT(E, L, i, k);
+        Rs[q] = AT(R, L, i, k);
+    }
+    __syncthreads();
+    const RelaxK<T> K = relax_k<T>(m, l, sp);
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    for (int s = 0; s < sweeps; s++)
+        for (int parity = 0; parity < 2; parity++) {
+            const int ncol = (W - parity + 1) / 2;
+            for (int t = threadIdx.x; t < ncol; t += blockDim.x) {
+                const int i = 2 * t + parity;
+                const bool side = (i == 0 || i == nx);
+                T below = T(0);
+                for (int k = 0; k <= nz; k++) {
+                    const T r = Rs[k * W + i];
+                    const T old = Es[k * W + i];
+                    T out = old;
+                    if (k == 0) {
+                        int d = 1 << l;
+                        int i0 = (i - nx / 2) * d + m.box_x / 2;
+                        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+                        if (inside0[(size_t)i0 * m.box_z] > 0) out = r;
+                        else if (side) {
+                            if (top_levels) out = oxy ? r : rx_corner(r, (i == 0) ? Es[i + 1] : Es[i - 1], at_s(Es, nx, nz, i, 1), K);
+                        } else out = oxy ? r : rx_k0(r, at_s(Es, nx, nz, i, 1), Es[i - 1], Es[i + 1], K);
+                    } else if (k == nz) {
+                        if (top_levels) {
+                            if (side) out = oxy ? r : rx_corner(r, (i == 0) ? Es[k * W + i + 1] : Es[k * W + i - 1], below, K);
+                            else out = rx_top(r, below, Es[k * W + i - 1], Es[k * W + i + 1], K);
+                        }
+                    } else if (side) {
+                        if (top_levels) out = oxy ? r : rx_side(r, below, Es[(k + 1) * W + i], (i == 0) ? Es[k * W + i + 1] : Es[k * W + i - 1], K);
+                    } else {
+                        out = rx_in(r, below, Es[(k + 1) * W + i], Es[k * W + i - 1], Es[k * W + i + 1], K);
+                    }
+                    Es[k * W + i] = out;
+                    below = out;
+                }
+            }
+            __syncthreads();
+        }
+    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        int i = q % W, k = q / W;
+        AT(E, L, i, k) = Es[q];
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Fused zebra smoother: S full sweeps (even columns, then odd columns, each */
 /* bottom to top) in one pass over the rows, out of place (E -> E2).        */
 /* ------------------------------------------------------------------------ */
-/* The relaxation formula of relax_point with the stencil values passed in:
+/* The relaxation of relax_point with the stencil values passed in:
  * below = new value at (i, k-1), up = value at (i, k+1) before this sweep,
  * xm/xp = values at (i-1, k)/(i+1, k) as the sweep order sees them, old =
  * the point's value before this sweep (kept where the point is not relaxed).
- * Same operations in the same order as relax_point. */
+ * Same operations as relax_point. */
 template <class T>
-__device__ __forceinline__ T relax_val(const MgConst& m, int nx, int nz, int l, int sp, int i, int k,
+__device__ __forceinline__ T relax_val(const MgConst& m, const RelaxK<T>& K, int nx, int nz, int l, int sp, int i, int k,
                                        T r, T below, T up, T xm, T xp, T old, const double* __restrict__ inside0)
 {
-    const T h2 = (T)(m.bl2 * (double)(1 << (2 * l)));
-    const T dt = (T)m.dt, D = (T)m.D[sp];
-    const T half = (T)0.5;
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
     const bool side = (i == 0 || i == nx);
@@ -355,25 +416,25 @@ __device__ __forceinline__ T relax_val(const MgConst& m, int nx, int nz, int l, 
         if (side) {
             if (!top_levels) return old;
             if (oxy) return r;
-            return (r * h2 / dt / D + (s1 + up)) / (h2 / dt / D + 2);
+            return rx_corner(r, s1, up, K);
         }
         if (oxy) return r;
-        return (r * h2 / dt / D + up + half * xm + half * xp) / (h2 / dt / D + 2);
+        return rx_k0(r, up, xm, xp, K);
     }
     if (k == nz) {
         if (!top_levels) return old;
         if (side) {
             if (oxy) return r;
-            return (r * h2 / dt / D + (s1 + below)) / (h2 / dt / D + 2);
+            return rx_corner(r, s1, below, K);
         }
-        return (r * h2 / dt / D + below + half * xp + half * xm) / (h2 / dt / D + 2);
+        return rx_top(r, below, xm, xp, K);
     }
     if (side) {
         if (!top_levels) return old;
         if (oxy) return r;
-        return (r * h2 / dt / D + half * below + half * up + s1) / (h2 / dt / D + 2);
+        return rx_side(r, below, up, s1, K);
     }
-    return (r * h2 / dt / D + half * below + half * up + half * xm + half * xp) / (h2 / dt / D + 2);
+    return rx_in(r, below, up, xm, xp, K);
 }
 
 template <class T> struct Pair2;
@@ -381,13 +442,14 @@ template <> struct Pair2<double> { typedef double2 type; };
 template <> struct Pair2<float> { typedef float2 type; };
 
 /* Each warp owns a strip of column pairs (lane t: columns c0+2t, c0+2t+1)
- * and one segment of rows.  Sweep s runs one row behind sweep s-1, so at
- * row step r sweep s relaxes row r-(s-1) with:
- *   the even column from the odd neighbours of sweep s-1 (shuffle from
- *   lane t-1, own odd column), the odd column from the new even
- *   neighbours of sweep s (own even column, shuffle from lane t+1), the
- *   value above from sweep s-1 (one row ahead) and the value below from
- *   sweep s itself.
+ * and one segment of rows.  Sweep s runs two rows behind sweep s-1: at row
+ * step r it relaxes row k = r - 2(s-1), using
+ *   from sweep s-1 the value above (its result of step r-1) and the point
+ *   itself and its odd neighbours (its result of step r-2: shuffle from
+ *   lane t-1, own odd column);
+ *   from sweep s itself the value below (step r-1) and, for the odd
+ *   column, the new even neighbours (own even column, shuffle from t+1).
+ * The S sweeps of one row step are therefore independent of each other.
  * A sweep's result is exact where all of its inputs were, which loses one
  * column pair at each strip edge per sweep: lanes S .. 31-S are written.
  * Segments other than the first start RELAX_WARM_F rows early from the
@@ -419,55 +481,54 @@ __global__ void __launch_bounds__(128) k_mg_smooth(MgConst m, MgLvlT<T> L, int l
     const T* __restrict__ E = L.e[sp];
     const T* __restrict__ R = L.r[sp];
     T* __restrict__ EO = L.e2[sp];
+    const RelaxK<T> K = relax_k<T>(m, l, sp);
     auto ld = [&](const T* a, int k) -> T2 {
         T2 v; v.x = T(0); v.y = T(0);
         if (ld_ok && k >= 0 && k <= nz) v = *reinterpret_cast<const T2*>(a + (size_t)k * pitch + ce);
         return v;
     };
-    /* prv[s]/cur[s]: sweep s's values at its previous/current row; s = 0 is
-     * the input (prv[0] = row r, cur[0] = row r+1) */
-    T2 prv[S + 1], cur[S + 1], rr[S];
+    /* h1[s]/h2[s]: sweep s's results of the last two row steps (s >= 1);
+     * in0/in1: input rows r and r+1; rr[j]: R of row r-j */
+    T2 h1[S + 1], h2[S + 1], cur[S + 1], rr[2 * S - 1];
     {
         T2 e0 = ld(E, kw - 1);
 #pragma unroll
-        for (int s = 1; s <= S; s++) { prv[s] = e0; cur[s] = e0; }
-        prv[0] = ld(E, kw);
-        cur[0] = ld(E, kw + 1);
+        for (int s = 1; s <= S; s++) { h1[s] = e0; h2[s] = e0; }
 #pragma unroll
-        for (int s = 0; s < S; s++) { rr[s].x = T(0); rr[s].y = T(0); }
+        for (int j = 0; j < 2 * S - 1; j++) { rr[j].x = T(0); rr[j].y = T(0); }
     }
+    T2 in0 = ld(E, kw), in1 = ld(E, kw + 1);
     T2 nr = ld(R, kw), ne = ld(E, kw + 2);
-    const int r_end = ke - 1 + (S - 1);
+    const int r_end = ke - 1 + 2 * (S - 1);
     for (int r = kw; r <= r_end; r++) {
-        /* R of row r enters the ring (rr[s-1] = R at sweep s's row) */
 #pragma unroll
-        for (int s = S - 1; s > 0; s--) rr[s] = rr[s - 1];
+        for (int j = 2 * S - 2; j > 0; j--) rr[j] = rr[j - 1];
         rr[0] = nr;
         T2 pr = ld(R, r + 1), pe = ld(E, r + 3);   /* prefetch for the next step */
 #pragma unroll
         for (int s = 1; s <= S; s++) {
-            const int k = r - (s - 1);
+            const int k = r - 2 * (s - 1);
             const int top = min(nz, ke - 1 + (S - s));
-            if (k < kw || k > top) { cur[s] = prv[s]; continue; }
-            /* even column */
-            T xm = __shfl_up_sync(0xffffffffu, prv[s - 1].y, 1);
-            T ve = relax_val<T>(m, nx, nz, l, sp, ce, k, rr[s - 1].x, prv[s].x, cur[s - 1].x, xm, prv[s - 1].y,
-                                prv[s - 1].x, inside0);
+            if (k < kw || k > top) { cur[s] = h1[s]; continue; }
+            /* inputs from sweep s-1: point and odd neighbours at row k, value above */
+            const T2 at = (s == 1) ? in0 : h2[s - 1];
+            const T2 up = (s == 1) ? in1 : h1[s - 1];
+            const T2 rk = rr[2 * (s - 1)];
+            T xm = __shfl_up_sync(0xffffffffu, at.y, 1);
+            T ve = relax_val<T>(m, K, nx, nz, l, sp, ce, k, rk.x, h1[s].x, up.x, xm, at.y, at.x, inside0);
             T xp = __shfl_down_sync(0xffffffffu, ve, 1);
-            T vo = relax_val<T>(m, nx, nz, l, sp, co, k, rr[s - 1].y, prv[s].y, cur[s - 1].y, ve, xp,
-                                prv[s - 1].y, inside0);
+            T vo = relax_val<T>(m, K, nx, nz, l, sp, co, k, rk.y, h1[s].y, up.y, ve, xp, at.y, inside0);
             cur[s].x = ve; cur[s].y = vo;
         }
-        const int kS = r - (S - 1);
+        const int kS = r - 2 * (S - 1);
         if (kS >= ks && kS < ke) {
             T* dst = EO + (size_t)kS * pitch;
             if (st_e && st_o) *reinterpret_cast<T2*>(dst + ce) = cur[S];
             else if (st_e) dst[ce] = cur[S].x;
         }
 #pragma unroll
-        for (int s = 1; s <= S; s++) prv[s] = cur[s];
-        prv[0] = cur[0];
-        cur[0] = ne;
+        for (int s = 1; s <= S; s++) { h2[s] = h1[s]; h1[s] = cur[s]; }
+        in0 = in1; in1 = ne;
         nr = pr; ne = pe;
     }
 }
@@ -795,6 +856,8 @@ static void relax_level(bcg_ctx* c, const MgConst& m, int l)
     c->launches += 2;
 }
 
+static int g_smooth_warps = 1400;   /* default resident-warp target of the fused smoother */
+
 template <class T> static void swap_err(bcg_ctx* c, int l);
 template <> void swap_err<double>(bcg_ctx* c, int l)
 {
@@ -805,8 +868,8 @@ template <> void swap_err<float>(bcg_ctx* c, int l)
     for (int sp = 0; sp < 3; sp++) { float* t = c->mg[l].errf[sp]; c->mg[l].errf[sp] = c->mg[l].errf2[sp]; c->mg[l].errf2[sp] = t; }
 }
 
-/* `sweeps` zebra sweeps of level l.  In mode 2 tall levels take the fused
- * kernel, up to 3 sweeps per launch; each launch swaps the level's two
+/* `sweeps` zebra sweeps of level l.  In mode 2 levels of 3 or more rows
+ * take the fused kernel, up to 3 sweeps per launch; each launch swaps the level's two
  * correction buffers.  Pre- and post-smoothing use the same number of
  * launches, so a V-cycle always swaps an even number of times and leaves
  * the buffers where it found them (captured graphs rely on this). */
@@ -814,7 +877,9 @@ template <class T>
 static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
     const int rows = c->mg[l].nz + 1;
-    if (g_relax_mode != 2 || rows <= 96) {
+    /* levels of 0-1 interior rows read across columns through the flat
+     * index (at_ref); they keep the in-place kernels */
+    if (g_relax_mode != 2 || rows < 3) {
         for (int j = 0; j < sweeps; j++) relax_level<T>(c, m, l);
         return;
     }
@@ -823,7 +888,8 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         MgLvlT<T> L = lvl<T>(c, l);
         const int outp = 32 - 2 * S;
         const int nwx = (L.nx + 1 + 2 * outp - 1) / (2 * outp);
-        int nseg = (1400 + 3 * nwx - 1) / (3 * nwx);
+        const int target = c->smooth_warps > 0 ? c->smooth_warps : g_smooth_warps;
+        int nseg = (target + 3 * nwx - 1) / (3 * nwx);
         const int max_seg = rows / 64 > 1 ? rows / 64 : 1;
         if (nseg > max_seg) nseg = max_seg;
         if (nseg < 1) nseg = 1;
@@ -838,12 +904,68 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
     }
 }
 
+/* kernel attributes set once per process, outside any stream capture */
+int mg_kernel_attributes()
+{
+    static bool done = false;
+    if (done) return BCG_OK;
+    if (cudaFuncSetAttribute(k_mg_coarse_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_coarse_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+        return BCG_E_CUDA;
+    done = true;
+    return BCG_OK;
+}
+
+/* bcg_autotune(BCG_TUNE_SMOOTHER): time the fused smoother on the finest
+ * level for several resident-warp targets (two launches each, so the
+ * correction buffers end where they started) and keep the fastest */
+int mg_tune_smoother(bcg_ctx* c, int* choice)
+{
+    const int rows = c->mg[0].nz + 1;
+    if (g_relax_mode != 2 || rows <= 96) { if (choice) *choice = 0; return BCG_OK; }
+    MgConst m = mg_const(c, c->P.mg_dt);
+    const int targets[5] = {350, 700, 1400, 2800, 5600};
+    const int saved = c->smooth_warps;
+    cudaEvent_t a, b;
+    BCG_CUDA_TRY(cudaEventCreate(&a));
+    BCG_CUDA_TRY(cudaEventCreate(&b));
+    float best = 3.4e38f;
+    int best_t = saved > 0 ? saved : g_smooth_warps;
+    for (int ti = 0; ti < 5; ti++) {
+        c->smooth_warps = targets[ti];
+        smooth_level<double>(c, m, 0, 3);                  /* warm-up */
+        smooth_level<double>(c, m, 0, 3);
+        cudaEventRecord(a, c->stream);
+        smooth_level<double>(c, m, 0, 3);
+        smooth_level<double>(c, m, 0, 3);
+        cudaEventRecord(b, c->stream);
+        if (cudaEventSynchronize(b) != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); c->smooth_warps = saved; return BCG_E_CUDA; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) { best = ms; best_t = targets[ti]; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    c->smooth_warps = best_t;
+    if (best_t != saved) nutrient_graphs_drop(c);
+    if (best_t != g_smooth_warps) { g_smooth_warps = best_t; bcg_kernel_config_changed(); }   /* default for new contexts */
+    if (choice) *choice = best_t;
+    return ctx_check_status(c);
+}
+
 /* mu2 sweeps on the coarsest level: fused when it fits one block */
 template <class T>
 static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
     MgLvlT<T> L = lvl<T>(c, l);
-    if (g_relax_mode >= 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
+    const size_t smem = 2 * sizeof(T) * (size_t)(L.nx + 1) * (L.nz + 1);
+    if (g_relax_mode >= 1 && smem <= 200 * 1024) {
+        int ncol = (L.nx + 2) / 2;
+        int threads = ((ncol + 31) / 32) * 32;
+        if (threads > 1024) threads = 1024;
+        k_mg_coarse_smem<T><<<3, threads, smem, c->stream>>>(m, L, l, sweeps, c->inside);
+        c->launches++;
+    } else if (g_relax_mode >= 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
         k_mg_relax_coarse<T><<<1, 1024, 0, c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
     } else {

@@ -349,6 +349,14 @@ extern "C" int bcg_colony_sweeps(bcg_ctx* c, int sweeps, int count0)
  * count the local buffer indices and the sweep-count parity are back where
  * they started after each unit, so every unit issues the same kernels with
  * the same arguments. */
+/* drop the cached graphs (a kernel shape of this context changed) */
+void nutrient_graphs_drop(bcg_ctx* c)
+{
+    for (int g = 0; g < 2; g++)
+        if (c->nutrient_graph[g]) { cudaGraphExecDestroy(c->nutrient_graph[g]); c->nutrient_graph[g] = nullptr; }
+    c->nutrient_graph_sweeps = 0;
+}
+
 static int nutrient_unit_graph(bcg_ctx* c, int sweeps, int last, cudaGraphExec_t* out)
 {
     if (c->nutrient_graph_sweeps != sweeps || c->nutrient_graph_gen != bcg_kernel_config_generation()) {

@@ -261,9 +261,16 @@ def b200_arm(args):
         _abi.check(lib.bcg_set_field(ctx, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size), "set growth")
         _abi.check(lib.bcg_update_density(ctx), "bcg_update_density")
         rows = set_depleted_wall(lib, ctx, p)
-        return sim, ctx, rows
+        # kernel shapes for this colony and grid (project autotuner)
+        _abi.check(lib.bcg_rebuild_neighbours(ctx), "rebuild")
+        tuned = {}
+        for name in ("FORCE_GROUP", "SMOOTHER"):
+            ch = ctypes.c_int()
+            _abi.check(lib.bcg_autotune(ctx, _abi.TUNE[name], ctypes.byref(ch)), "autotune " + name)
+            tuned[name.lower()] = ch.value
+        return sim, ctx, rows, tuned
 
-    sim, ctx, wall_rows = make_sim()
+    sim, ctx, wall_rows, tuned = make_sim()
     stream = torch.cuda.ExternalStream(lib.bcg_stream(ctx))
     _abi.check(lib.bcg_sim_run(sim, args.warmup), "warmup")
     torch.cuda.synchronize()
@@ -404,6 +411,7 @@ def b200_arm(args):
                    "box": [p.box_x, p.box_y, p.box_z], "box_z_agar": p.box_z_agar,
                    "agar_levels": p.max_levels_mg, "mg_levels": p.mg_levels, "mg_dof": dof,
                    "vcycles_per_step": args.vcycles, "neighbour_rebuild_every": 100,
+                   "autotuned": tuned,
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (cell records 2x%d MB + fields)" % (n0 * 128 // 2 ** 20)},
         "mg_dof_per_s": dof * args.vcycles / (mg_ms / 1e3) if mg_ms > 0 else None,

@@ -282,12 +282,33 @@ int bcg_colony_sweeps(bcg_ctx* ctx, int sweeps, int count0);
 /* an FP64 iterative-refinement loop); no reference counterpart.         */
 /* ------------------------------------------------------------------ */
 /* Solve the backward-Euler agar step (the system Multigrid::solve
- * iterates on) until the FP64 residual max-norm falls below
- * rel_tol * (max-norm of the right-hand side), with V-cycles on the inner
- * correction run in precision `precision` (32 or 64).  *iters receives the
- * outer iterations used and *rel_res the final relative residual. */
+ * iterates on) until the FP64 defect max-norm at the relaxed points of the
+ * composite levels falls below rel_tol * (its value at the start).
+ * precision 64: FP64 V-cycles.  precision 32: V-cycles on FP32 copies of
+ * the correction and right-hand side (smoothing, restriction and
+ * prolongation in FP32; solution and defect in FP64) while the defect
+ * still halves per cycle, then FP64 V-cycles from that correction.
+ * *iters receives the V-cycles run and *rel_res the final relative defect
+ * (where the V-cycle itself stalls, as on grids whose coarsest levels have
+ * 0-1 interior rows, the solve stops at max_iters above rel_tol). */
 int bcg_mg_solve_tol(bcg_ctx* ctx, double rel_tol, int precision, int max_iters,
                      int* iters, double* rel_res);
+
+/* ------------------------------------------------------------------ */
+/* kernel-shape autotuning (no reference counterpart)                    */
+/* ------------------------------------------------------------------ */
+/* Times the variants of one kernel on the context's current state and
+ * keeps the fastest for this context (*choice receives it):
+ *   BCG_TUNE_FORCE_GROUP  lanes per cell in MoveCell+GrowCell (1..16);
+ *                         needs binned cells and neighbour lists; leaves
+ *                         the colony unchanged;
+ *   BCG_TUNE_SMOOTHER     resident-warp target of the fused agar smoother
+ *                         (how many row segments a level is cut into);
+ *                         changes only the multigrid's correction scratch.
+ * The choice also becomes the default of contexts created afterwards.
+ * Synchronises the stream; not for use inside a stream capture. */
+typedef enum bcg_tune_id { BCG_TUNE_FORCE_GROUP = 1, BCG_TUNE_SMOOTHER = 2 } bcg_tune_id;
+int bcg_autotune(bcg_ctx* ctx, int what, int* choice);
 
 /* ------------------------------------------------------------------ */
 /* timing: device time of the kernels queued by the last call of each    */

@@ -187,8 +187,10 @@ def test_tolerance_solve_fixed_cycles_equals_solve(gpu):
 
 def test_mixed_precision_reaches_fp64_tolerance(gpu):
     """FP64 V-cycles and FP32 V-cycles + FP64 refinement both reach a 1e-8
-    relative defect, and both solutions lie within 5e-8 (relative to the
-    field's maximum) of a 1e-12 FP64 solve of the same system."""
+    relative defect; measured against a 1e-12 FP64 solve of the same
+    system, the mixed solution is as accurate as the FP64 one at the same
+    tolerance (within 2x, or 1e-9 of the field's maximum) and both are
+    within 1e-6."""
     p = params.workload_params("scale_262k")
     cells = workload_colony("scale_262k", n=40000)
     sols = {}
@@ -198,9 +200,8 @@ def test_mixed_precision_reaches_fp64_tolerance(gpu):
         assert it > 1 and rel < tol, (key, it, rel)
         sols[key] = _solve_state(col, p)
         col.close()
-    for key in ("fp64", "mixed"):
-        for x, y in zip(sols["tight"], sols[key]):
-            assert close(x, y) <= 5e-8, key
+    err = {key: max(close(x, y) for x, y in zip(sols["tight"], sols[key])) for key in ("fp64", "mixed")}
+    assert err["fp64"] <= 1e-6 and err["mixed"] <= max(2 * err["fp64"], 1e-9), err
 
 
 def test_tolerance_solve_reports_stagnation(gpu):
@@ -216,3 +217,22 @@ def test_tolerance_solve_reports_stagnation(gpu):
         it, rel = col.mg_solve_tol(1e-8, prec, 20)
         assert it == 20 and rel > 1e-8, (prec, it, rel)
         col.close()
+
+
+def test_smoother_autotune_same_solution(gpu):
+    """The smoother's segment count changes where rows are cut, not the
+    result (to rounding)."""
+    p = params.workload_params("scale_262k")
+    cells = workload_colony("scale_262k", n=20000)
+    out = []
+    for tune in (False, True):
+        col = Colony(p, cells); col.update_density(); col.deplete_wall()
+        if tune:
+            assert col.autotune("SMOOTHER") in (350, 700, 1400, 2800, 5600)
+            col.update_density(); col.deplete_wall()
+        col.mg_solve(3)
+        out.append(_solve_state(col, p))
+        col.close()
+    for a, b in zip(*out):
+        assert close(a, b) <= 1e-14
+

@@ -18,8 +18,8 @@ REL_TOL = 1e-10
 pytestmark = pytest.mark.gpu
 
 
-def setup_pair(n=4096, seed=12345, spread=1.0, growth=0.9, workload="small_4k", mutate=None):
-    p = params.workload_params(workload)
+def setup_pair(n=4096, seed=12345, spread=1.0, growth=0.9, workload="small_4k", mutate=None, max_cells=None):
+    p = params.workload_params(workload, max_cells=max_cells)
     cells = workload_colony(workload, n=n, div_phase_spread=spread)
     if mutate is not None:
         mutate(cells)
@@ -103,7 +103,7 @@ def test_crowded_divisions(gpu):
         r = np.random.default_rng(5)
         pick = r.random(len(cells)) < 0.5
         cells["ldiv"][pick] = cells["length"][pick]     # divide after this step's growth
-    p, orc, col, rng = setup_pair(mutate=mutate)
+    p, orc, col, rng = setup_pair(mutate=mutate, max_cells=16384)
     col.rebuild_neighbours()
     t = 0.0
     for s in range(3):
@@ -177,3 +177,20 @@ def test_mean_stress(gpu):
     assert calls.value == calls_o
     assert rel_err(st_o.reshape(-1), st) <= 1e-10
     assert rel_err(fn_o.reshape(-1), fn) <= 1e-10
+
+
+def test_autotune_keeps_state(gpu):
+    """Tuning the lane group times trial launches on the live colony: the
+    colony (records and per-cell outputs) is unchanged afterwards and the
+    next step still matches the oracle."""
+    p, orc, col, rng = setup_pair()
+    col.rebuild_neighbours()
+    before = col.cells().tobytes()
+    g = col.autotune("FORCE_GROUP")
+    assert g in (1, 2, 4, 8, 16)
+    assert col.cells().tobytes() == before
+    _, calls_o, lin_o = orc.step(p.dt, 0.0)
+    lin = col.step(p.dt, 0.0, rng)
+    assert np.array_equal(lin, lin_o)
+    assert_cells_close(orc.cells(), col.cells())
+
