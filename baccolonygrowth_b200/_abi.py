@@ -212,6 +212,7 @@ PROTOTYPES = {
     "bcg_save_restart": (_I, [ctypes.c_char_p, _D, _D, _VP, _I]),
     "bcg_load_restart": (_I, [ctypes.c_char_p, _PD, _PD, _VP, _I, _PI]),
     "bcg_mean_stress": (_I, [_VP, _PD, _PD, _PI64]),
+    "bcg_mean_stress_noalloc": (_I, [_VP, _PD, _PD, _PI64]),
 }
 
 # library entry points outside include/bcg.h, used by tests and the benchmark
@@ -223,6 +224,7 @@ EXTRA_PROTOTYPES = {
 }
 
 TUNE = dict(FORCE_GROUP=1, SMOOTHER=2)
+NOALLOC_MAX_CELLS = 32768   # BCG_NOALLOC_MAX_CELLS
 
 _lib = None
 

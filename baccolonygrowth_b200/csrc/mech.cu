@@ -8,6 +8,7 @@
 #include "ctx.cuh"
 #include "cellmath.cuh"
 #include <string.h>
+#include <mutex>
 
 /* ======================================================================= */
 /* binning: counting sort of cell ids by UniformGrid address               */
@@ -873,3 +874,61 @@ extern "C" int bcg_mean_stress(bcg_ctx* c, double* stress, double* fnet, int64_t
     if (fcw_calls) *fcw_calls = (int64_t)h;
     return rc;
 }
+
+/* ======================================================================= */
+/* bcg_mean_stress_noalloc: the same kernel with its staging in a device   */
+/* array compiled into the library (no allocation on any call)             */
+/* ======================================================================= */
+/* 5 stress + 3 force doubles per cell, then the F_cw counter */
+static __device__ __align__(256) double g_noalloc_stress[8 * BCG_NOALLOC_MAX_CELLS + 32];
+
+#define NOALLOC_MAX_DEVICES 64
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+/* the array's device address on device `dev` (current), looked up once */
+static int noalloc_staging(int dev, double** out)
+{
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return BCG_E_ARG;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_stress);
+        if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
+        g_noalloc_addr[dev] = (double*)p;
+    }
+    *out = g_noalloc_addr[dev];
+    return BCG_OK;
+}
+
+extern "C" int bcg_mean_stress_noalloc(bcg_ctx* c, double* stress, double* fnet, int64_t* fcw_calls)
+{
+    if (!c || !stress) return BCG_E_ARG;
+    const int n = c->n;
+    if (n > BCG_NOALLOC_MAX_CELLS) return BCG_E_UNSUPPORTED;
+    int dev = -1;
+    BCG_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != c->device) return BCG_E_ARG;
+    double* base = nullptr;
+    int rc = noalloc_staging(dev, &base);
+    if (rc) return rc;
+    double* ds = base;
+    double* df = base + 5 * (size_t)BCG_NOALLOC_MAX_CELLS;
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(base + 8 * (size_t)BCG_NOALLOC_MAX_CELLS);
+    /* the counter still holds the previous call's count */
+    BCG_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(*cnt), c->stream));
+    if (n > 0) {
+        k_mean_stress<<<(n + 127) / 128, 128, 0, c->stream>>>(n, c->rec[c->cur], c->nbr, c->ncount, field_ptrs(c),
+                                                              mech_params(c), ds, fnet ? df : nullptr, cnt, c->status);
+        c->launches++;
+        BCG_CUDA_TRY(cudaGetLastError());
+        BCG_CUDA_TRY(cudaMemcpyAsync(stress, ds, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+        if (fnet) BCG_CUDA_TRY(cudaMemcpyAsync(fnet, df, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    unsigned long long h = 0;
+    BCG_CUDA_TRY(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    rc = ctx_check_status(c);
+    if (fcw_calls) *fcw_calls = (int64_t)h;
+    return rc;
+}
+

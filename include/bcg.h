@@ -353,6 +353,29 @@ int bcg_load_restart(const char* path, double* t, double* dt, bcg_cell* cells, i
  * rand() draws the reference makes here (one per wall-near cell). */
 int bcg_mean_stress(bcg_ctx* ctx, double* stress, double* fnet, int64_t* fcw_calls);
 
+/* bcg_mean_stress without any allocation.  No counterpart in the reference.
+ * bcg_mean_stress stages its per-cell results in device buffers it
+ * allocates on each call; this variant is for hosts that cannot allocate
+ * device memory when they write an output step: a host whose device memory
+ * is reserved up front (another framework's caching allocator holding the
+ * GPU, so an allocation here can fail), or an output thread that must not
+ * call into the CUDA allocator (whose pool operations and frees can wait on
+ * other work on the device).  Same arguments and results as
+ * bcg_mean_stress.  The results are staged instead in one fixed device array
+ * built into the library, room for BCG_NOALLOC_MAX_CELLS cells (2 MiB),
+ * which every GPU that loads the library holds until the process exits.
+ *   - A colony of more than BCG_NOALLOC_MAX_CELLS cells returns
+ *     BCG_E_UNSUPPORTED; a call whose current device is not the context's
+ *     returns BCG_E_ARG.
+ *   - The first call on a device looks the array's device address up
+ *     (cudaGetSymbolAddress); make that first call before any stream
+ *     capture on that device.
+ *   - Every call on a device uses the same array, which keeps the previous
+ *     call's contents.  Calls that can overlap on the GPU (other contexts,
+ *     other host threads) race on it and must be serialised by the caller. */
+#define BCG_NOALLOC_MAX_CELLS 32768
+int bcg_mean_stress_noalloc(bcg_ctx* ctx, double* stress, double* fnet, int64_t* fcw_calls);
+
 /* ------------------------------------------------------------------ */
 /* C++ host loop (rewrite of SimSingleThread, Simulation.cpp:42-434)     */
 /* ------------------------------------------------------------------ */
