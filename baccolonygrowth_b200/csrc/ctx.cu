@@ -520,6 +520,7 @@ extern "C" int bcg_set_field(bcg_ctx* c, int f, int level, const double* in, siz
     if (rc) return rc;
     if (n < v.n) return BCG_E_ARG;
     if (v.mg == 2) return BCG_E_UNSUPPORTED;  /* the agar view is derived */
+    if (v.mg == 1) { c->mg_clean = 0; nutrient_graphs_drop(c); }   /* Err/Res may no longer be zero */
     if (!v.mg) {
         BCG_CUDA_TRY(cudaMemcpy(v.ptr, in, v.n * 8, cudaMemcpyHostToDevice));
         return BCG_OK;

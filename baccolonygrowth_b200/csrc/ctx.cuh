@@ -102,6 +102,9 @@ struct bcg_ctx {
     /* kernel shapes chosen by bcg_autotune for this context (0 = default) */
     int force_group;
     int smooth_warps;
+    /* multigrid Err (all levels) and Res (levels > 0) are zero, as the last
+     * reset() left them; setup() then skips its resetZero */
+    int mg_clean;
 };
 
 MechParams mech_params(const bcg_ctx* c);

@@ -391,6 +391,90 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_smem(MgConst m, MgLvlT<T> L,
     }
 }
 
+/* Relaxation of point (i, k) of a level held in shared memory (row k at
+ * offset k*(nx+1)), in place; the point code of k_mg_coarse_smem. */
+template <class T>
+__device__ __forceinline__ void relax_smem(const MgConst& m, const RelaxK<T>& K, int l, bool oxy, bool top_levels,
+                                           int nx, int nz, int i, int k, T* Es, const T* Rs,
+                                           const double* __restrict__ inside0)
+{
+    const int W = nx + 1;
+    const bool side = (i == 0 || i == nx);
+    const T r = Rs[k * W + i];
+    T out = Es[k * W + i];
+    if (k == 0) {
+        int d = 1 << l;
+        int i0 = (i - nx / 2) * d + m.box_x / 2;
+        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+        if (inside0[(size_t)i0 * m.box_z] > 0) out = r;
+        else if (side) {
+            if (top_levels) out = oxy ? r : rx_corner(r, (i == 0) ? Es[i + 1] : Es[i - 1], at_s(Es, nx, nz, i, 1), K);
+        } else out = oxy ? r : rx_k0(r, at_s(Es, nx, nz, i, 1), Es[i - 1], Es[i + 1], K);
+    } else {
+        const T below = Es[(k - 1) * W + i];
+        if (k == nz) {
+            if (top_levels) {
+                if (side) out = oxy ? r : rx_corner(r, (i == 0) ? Es[k * W + i + 1] : Es[k * W + i - 1], below, K);
+                else out = rx_top(r, below, Es[k * W + i - 1], Es[k * W + i + 1], K);
+            }
+        } else if (side) {
+            if (top_levels) out = oxy ? r : rx_side(r, below, Es[(k + 1) * W + i], (i == 0) ? Es[k * W + i + 1] : Es[k * W + i - 1], K);
+        } else {
+            out = rx_in(r, below, Es[(k + 1) * W + i], Es[k * W + i - 1], Es[k * W + i + 1], K);
+        }
+    }
+    Es[k * W + i] = out;
+}
+
+/* All mu2 relaxations of a level of nz >= 1 held in shared memory, as a
+ * wavefront over the sweeps: at step t sweep s relaxes row k = t - 2s, its
+ * even columns in one phase and its odd columns in the next.  Two rows of
+ * lag keep every read on the value the sequential order gives it: row k+1
+ * still holds sweep s-1's value, row k-1 already holds sweep s's, and no
+ * other sweep writes row k or its neighbours in the same phase.  About
+ * (nz+1)/2 sweeps progress per step instead of one. */
+template <class T>
+__global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L, int l, int sweeps,
+                                                         const double* __restrict__ inside0)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int sp = blockIdx.x;
+    const int nx = L.nx, nz = L.nz, W = nx + 1;
+    const int np = W * (nz + 1);
+    T* Es = reinterpret_cast<T*>(smem_raw);
+    T* Rs = Es + np;
+    T* E = L.e[sp];
+    const T* R = L.r[sp];
+    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        int i = q % W, k = q / W;
+        Es[q] = AT(E, L, i, k);
+        Rs[q] = AT(R, L, i, k);
+    }
+    __syncthreads();
+    const RelaxK<T> K = relax_k<T>(m, l, sp);
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    const int steps = nz + 1 + 2 * (sweeps - 1);
+    for (int t = 0; t < steps; t++) {
+        const int s_lo = t > nz ? (t - nz + 1) / 2 : 0;
+        const int s_hi = min(sweeps - 1, t / 2);
+        const int na = s_hi - s_lo + 1;
+        for (int parity = 0; parity < 2; parity++) {
+            const int ncol = (W - parity + 1) / 2;
+            for (int q = threadIdx.x; q < na * ncol; q += blockDim.x) {
+                const int sw = s_lo + q / ncol;
+                const int i = 2 * (q % ncol) + parity;
+                relax_smem<T>(m, K, l, oxy, top_levels, nx, nz, i, t - 2 * sw, Es, Rs, inside0);
+            }
+            __syncthreads();
+        }
+    }
+    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        int i = q % W, k = q / W;
+        AT(E, L, i, k) = Es[q];
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Fused zebra smoother: S full sweeps (even columns, then odd columns, each */
 /* bottom to top) in one pass over the rows, out of place (E -> E2).        */
@@ -441,28 +525,52 @@ template <class T> struct Pair2;
 template <> struct Pair2<double> { typedef double2 type; };
 template <> struct Pair2<float> { typedef float2 type; };
 
+/* Interior rows (0 < k < nz) need only the column's kind, fixed per lane:
+ * 0 interior column, 1 left side (i = 0), 2 right side (i = nx), 3 side
+ * held at R (oxygen on the top levels), 4 side not relaxed (keeps old). */
+__device__ __forceinline__ int col_kind(int i, int nx, bool oxy, bool top_levels)
+{
+    if (i != 0 && i != nx) return 0;
+    if (!top_levels) return 4;
+    if (oxy) return 3;
+    return i == 0 ? 1 : 2;
+}
+template <class T>
+__device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T old, const RelaxK<T>& K)
+{
+    if (kind == 0) return rx_in(r, below, up, xm, xp, K);
+    if (kind == 1) return rx_side(r, below, up, xp, K);
+    if (kind == 2) return rx_side(r, below, up, xm, K);
+    return kind == 3 ? r : old;
+}
+
 /* Each warp owns a strip of column pairs (lane t: columns c0+2t, c0+2t+1)
- * and one segment of rows.  Sweep s runs two rows behind sweep s-1: at row
- * step r it relaxes row k = r - 2(s-1), using
- *   from sweep s-1 the value above (its result of step r-1) and the point
- *   itself and its odd neighbours (its result of step r-2: shuffle from
- *   lane t-1, own odd column);
- *   from sweep s itself the value below (step r-1) and, for the odd
- *   column, the new even neighbours (own even column, shuffle from t+1).
- * The S sweeps of one row step are therefore independent of each other.
- * A sweep's result is exact where all of its inputs were, which loses one
- * column pair at each strip edge per sweep: lanes S .. 31-S are written.
- * Segments other than the first start RELAX_WARM_F rows early from the
- * pre-smoothing values; the row recurrence contracts by at least 1/4 per
- * row, so the start error is below rounding when the segment's own rows
- * begin.  Rows above the segment are relaxed by the early sweeps as far
- * as the later sweeps need them, and only the segment's rows are stored. */
+ * and one segment of rows.  The S sweeps are 2S half-sweeps (even columns,
+ * then odd columns, per sweep) run as a pipeline: half-sweep h relaxes row
+ * k = r - h at row step r.  Every input it needs was produced at step r-1
+ * or r-2:
+ *   even half of sweep s: value above and the point itself from sweep
+ *   s-1's even half (steps r-1, r-2), odd neighbours from sweep s-1's odd
+ *   half (step r-1; shuffle from lane t-1 and the lane's own odd column);
+ *   odd half of sweep s: likewise from sweep s-1's odd half, even
+ *   neighbours from sweep s's even half (step r-1; own even column and
+ *   shuffle from lane t+1);
+ *   value below from the half-sweep itself (step r-1);
+ * so the 2S updates of a step are independent.  A half-sweep's result is
+ * exact where all of its inputs were, which loses one lane at one strip
+ * edge per half-sweep: lanes S .. 31-S are written.  Segments other than
+ * the first start RELAX_WARM_F rows early from the pre-smoothing values;
+ * the row recurrence contracts by at least 1/4 per row, so the start
+ * error is below rounding when the segment's own rows begin.  Rows above
+ * the segment are relaxed by the early half-sweeps as far as the later
+ * ones need them, and only the segment's rows are stored. */
 #define RELAX_WARM_F 40
 template <class T, int S>
 __global__ void __launch_bounds__(128) k_mg_smooth(MgConst m, MgLvlT<T> L, int l, int seg_len,
                                                    const double* __restrict__ inside0)
 {
     typedef typename Pair2<T>::type T2;
+    constexpr int H = 2 * S;
     const int lane = threadIdx.x;
     const int warp = blockIdx.x * blockDim.y + threadIdx.y;
     const int sp = blockIdx.z;
@@ -482,54 +590,71 @@ __global__ void __launch_bounds__(128) k_mg_smooth(MgConst m, MgLvlT<T> L, int l
     const T* __restrict__ R = L.r[sp];
     T* __restrict__ EO = L.e2[sp];
     const RelaxK<T> K = relax_k<T>(m, l, sp);
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    const int kind_e = col_kind(ce, nx, oxy, top_levels), kind_o = col_kind(co, nx, oxy, top_levels);
     auto ld = [&](const T* a, int k) -> T2 {
         T2 v; v.x = T(0); v.y = T(0);
         if (ld_ok && k >= 0 && k <= nz) v = *reinterpret_cast<const T2*>(a + (size_t)k * pitch + ce);
         return v;
     };
-    /* h1[s]/h2[s]: sweep s's results of the last two row steps (s >= 1);
-     * in0/in1: input rows r and r+1; rr[j]: R of row r-j */
-    T2 h1[S + 1], h2[S + 1], cur[S + 1], rr[2 * S - 1];
-    {
-        T2 e0 = ld(E, kw - 1);
+    /* h1[h]/h2[h]: half-sweep h's results of steps r-1 and r-2 (its own
+     * column parity); inm/in0/inp: input rows r-1, r, r+1; rr[j]: R row r-j */
+    T h1[H], h2[H], cur[H];
+    T2 rr[H];
+    T2 inm = ld(E, kw - 1), in0 = ld(E, kw), inp = ld(E, kw + 1);
 #pragma unroll
-        for (int s = 1; s <= S; s++) { h1[s] = e0; h2[s] = e0; }
-#pragma unroll
-        for (int j = 0; j < 2 * S - 1; j++) { rr[j].x = T(0); rr[j].y = T(0); }
+    for (int h = 0; h < H; h++) {
+        h1[h] = (h & 1) ? inm.y : inm.x;       /* value below the first row: pre-smoothing */
+        h2[h] = h1[h];
+        rr[h].x = T(0); rr[h].y = T(0);
     }
-    T2 in0 = ld(E, kw), in1 = ld(E, kw + 1);
-    T2 nr = ld(R, kw), ne = ld(E, kw + 2);
-    const int r_end = ke - 1 + 2 * (S - 1);
+    T2 nr1 = ld(R, kw), nr2 = ld(R, kw + 1);
+    T2 ne1 = ld(E, kw + 2), ne2 = ld(E, kw + 3);
+    const int r_end = ke - 1 + (H - 1);
     for (int r = kw; r <= r_end; r++) {
 #pragma unroll
-        for (int j = 2 * S - 2; j > 0; j--) rr[j] = rr[j - 1];
-        rr[0] = nr;
-        T2 pr = ld(R, r + 1), pe = ld(E, r + 3);   /* prefetch for the next step */
+        for (int j = H - 1; j > 0; j--) rr[j] = rr[j - 1];
+        rr[0] = nr1;
+        const T2 nr3 = ld(R, r + 2), ne3 = ld(E, r + 4);     /* two rows ahead */
+        /* neighbours from other lanes, all from the previous step */
+        T nb[H];
 #pragma unroll
-        for (int s = 1; s <= S; s++) {
-            const int k = r - 2 * (s - 1);
-            const int top = min(nz, ke - 1 + (S - s));
-            if (k < kw || k > top) { cur[s] = h1[s]; continue; }
-            /* inputs from sweep s-1: point and odd neighbours at row k, value above */
-            const T2 at = (s == 1) ? in0 : h2[s - 1];
-            const T2 up = (s == 1) ? in1 : h1[s - 1];
-            const T2 rk = rr[2 * (s - 1)];
-            T xm = __shfl_up_sync(0xffffffffu, at.y, 1);
-            T ve = relax_val<T>(m, K, nx, nz, l, sp, ce, k, rk.x, h1[s].x, up.x, xm, at.y, at.x, inside0);
-            T xp = __shfl_down_sync(0xffffffffu, ve, 1);
-            T vo = relax_val<T>(m, K, nx, nz, l, sp, co, k, rk.y, h1[s].y, up.y, ve, xp, at.y, inside0);
-            cur[s].x = ve; cur[s].y = vo;
+        for (int h = 0; h < H; h++) {
+            const T src = (h == 0) ? in0.y : h1[h - 1];
+            nb[h] = (h & 1) ? __shfl_down_sync(0xffffffffu, src, 1) : __shfl_up_sync(0xffffffffu, src, 1);
         }
-        const int kS = r - 2 * (S - 1);
+#pragma unroll
+        for (int h = 0; h < H; h++) {
+            const int k = r - h;
+            const int top = min(nz, ke - 1 + (H - 1 - h) / 2);
+            if (k < kw || k > top) { cur[h] = h1[h]; continue; }
+            const bool odd = h & 1;
+            /* inputs from the half-sweep two before (same parity), the one before (other parity) */
+            const T old = (h == 0) ? in0.x : (h == 1) ? inm.y : h2[h - 2];
+            const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
+            const T own_other = (h == 0) ? in0.y : h1[h - 1];      /* odd column c+1 / even column c-1 */
+            const T xm = odd ? own_other : nb[h];
+            const T xp = odd ? nb[h] : own_other;
+            const T rv = odd ? rr[h].y : rr[h].x;
+            const int col = odd ? co : ce;
+            if (k > 0 && k < nz)
+                cur[h] = rx_row<T>(odd ? kind_o : kind_e, rv, h1[h], up, xm, xp, old, K);
+            else
+                cur[h] = relax_val<T>(m, K, nx, nz, l, sp, col, k, rv, h1[h], up, xm, xp, old, inside0);
+        }
+        const int kS = r - (H - 1);
         if (kS >= ks && kS < ke) {
             T* dst = EO + (size_t)kS * pitch;
-            if (st_e && st_o) *reinterpret_cast<T2*>(dst + ce) = cur[S];
-            else if (st_e) dst[ce] = cur[S].x;
+            T2 v; v.x = h1[H - 2]; v.y = cur[H - 1];              /* even half finished this row one step ago */
+            if (st_e && st_o) *reinterpret_cast<T2*>(dst + ce) = v;
+            else if (st_e) dst[ce] = v.x;
         }
 #pragma unroll
-        for (int s = 1; s <= S; s++) { h2[s] = h1[s]; h1[s] = cur[s]; }
-        in0 = in1; in1 = ne;
-        nr = pr; ne = pe;
+        for (int h = 0; h < H; h++) { h2[h] = h1[h]; h1[h] = cur[h]; }
+        inm = in0; in0 = inp; inp = ne1;
+        ne1 = ne2; ne2 = ne3;
+        nr1 = nr2; nr2 = nr3;
     }
 }
 
@@ -910,7 +1035,9 @@ int mg_kernel_attributes()
     static bool done = false;
     if (done) return BCG_OK;
     if (cudaFuncSetAttribute(k_mg_coarse_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(k_mg_coarse_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+        cudaFuncSetAttribute(k_mg_coarse_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_coarse_wave<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_coarse_wave<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
         return BCG_E_CUDA;
     done = true;
     return BCG_OK;
@@ -947,7 +1074,8 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     c->smooth_warps = best_t;
-    if (best_t != saved) nutrient_graphs_drop(c);
+    c->mg_clean = 0;                 /* the trial sweeps wrote Err */
+    nutrient_graphs_drop(c);
     if (best_t != g_smooth_warps) { g_smooth_warps = best_t; bcg_kernel_config_changed(); }   /* default for new contexts */
     if (choice) *choice = best_t;
     return ctx_check_status(c);
@@ -959,7 +1087,10 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
     MgLvlT<T> L = lvl<T>(c, l);
     const size_t smem = 2 * sizeof(T) * (size_t)(L.nx + 1) * (L.nz + 1);
-    if (g_relax_mode >= 1 && smem <= 200 * 1024) {
+    if (g_relax_mode >= 1 && smem <= 200 * 1024 && L.nz >= 1) {
+        k_mg_coarse_wave<T><<<3, 1024, smem, c->stream>>>(m, L, l, sweeps, c->inside);
+        c->launches++;
+    } else if (g_relax_mode >= 1 && smem <= 200 * 1024) {
         int ncol = (L.nx + 2) / 2;
         int threads = ((ncol + 31) / 32) * 32;
         if (threads > 1024) threads = 1024;
@@ -1021,7 +1152,8 @@ static void update_res(bcg_ctx* c, const MgConst& m, int l)
 /* setup(), Multigrid.cpp:818-825 */
 void mg_setup(bcg_ctx* c, const MgConst& m)
 {
-    reset_zero(c);
+    if (!c->mg_clean) reset_zero(c);
+    c->mg_clean = 0;
     for (int l = 0; l <= m.A - 1; l++) update_sol(c, m, l);
     for (int l = 0; l <= m.A - 1; l++) update_res(c, m, l);
 }
@@ -1036,13 +1168,16 @@ void mg_reset(bcg_ctx* c, const MgConst& m)
         k_mg_rewrite_bdry<<<grid2(n, 256), 256, 0, c->stream>>>(m, L, Lc, l);
         c->launches++;
     }
-    for (int l = 0; l <= m.A - 1; l++) update_res(c, m, l);
+    /* the reference recomputes Res on every composite level here, and the
+     * resetZero below clears it again on levels > 0: only level 0's stays */
+    update_res(c, m, 0);
     reset_zero(c);
     for (int l = 1; l < m.A; l++) {
         MgLvl L = mg_lvl(c, l), Lf = mg_lvl(c, l - 1);
         k_mg_nest<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lf, l);
         c->launches++;
     }
+    c->mg_clean = 1;
 }
 
 void mg_copy_to(bcg_ctx* c, const MgConst& m, int wall_buf)
