@@ -42,7 +42,7 @@ template <class T> struct RelaxK { T cf, inv; };
 template <class T>
 __device__ __forceinline__ RelaxK<T> relax_k(const MgConst& m, int l, int sp)
 {
-    const double cf = m.bl2 * (double)(1 << (2 * l)) / m.dt / m.D[sp];
+    const double cf = m.bl2 * (double)(1 << (2 * l)) / m.dt / SP(m.D);
     RelaxK<T> k; k.cf = (T)cf; k.inv = (T)(1.0 / (cf + 2.0));
     return k;
 }
@@ -102,8 +102,8 @@ __device__ __forceinline__ void relax_point(const MgConst& m, const MgLvlT<T>& L
 {
     const int nx = L.nx, nz = L.nz;
     const RelaxK<T> K = relax_k<T>(m, l, sp);
-    T* E = L.e[sp];
-    const T* R = L.r[sp];
+    T* E = SP(L.e);
+    const T* R = SP(L.r);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
     T r = AT(R, L, i, k);
@@ -153,7 +153,7 @@ __device__ __forceinline__ double relax_eval(const MgConst& m, const MgLvlT<T>& 
 {
     const int nx = L.nx, nz = L.nz;
     const RelaxK<double> K = relax_k<double>(m, l, sp);
-    const T* E = L.e[sp];
+    const T* E = SP(L.e);
     const double r = AT(R64, L, i, k);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvlT<T> L, in
     const int k_begin = seg * seg_len;
     const int k_end = min(k_begin + seg_len, nz + 1);
     const int k_start = max(0, k_begin - RELAX_WARM);
-    T* E = L.e[sp];
+    T* E = SP(L.e);
     /* pre-sweep values this thread needs from rows other threads write */
     T up_w[RELAX_WARM + 1];
     T below = T(0), above_end = T(0);
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(512) k_mg_relax_seg(MgConst m, MgLvlT<T> L, in
     }
     __syncthreads();
     if (!active || k_begin > nz) return;
-    const T* R = L.r[sp];
+    const T* R = SP(L.r);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
     const int nx = L.nx;
@@ -339,8 +339,8 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_smem(MgConst m, MgLvlT<T> L,
     const int np = W * (nz + 1);
     T* Es = reinterpret_cast<T*>(smem_raw);
     T* Rs = Es + np;
-    T* E = L.e[sp];
-    const T* R = L.r[sp];
+    T* E = SP(L.e);
+    const T* R = SP(L.r);
     for (int q = threadIdx.x; q < np; q += blockDim.x) {
         int i = q % W, k = q / W;
         Es[q] = AT(E, L, i, k);
@@ -443,8 +443,8 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
     const int np = W * (nz + 1);
     T* Es = reinterpret_cast<T*>(smem_raw);
     T* Rs = Es + np;
-    T* E = L.e[sp];
-    const T* R = L.r[sp];
+    T* E = SP(L.e);
+    const T* R = SP(L.r);
     for (int q = threadIdx.x; q < np; q += blockDim.x) {
         int i = q % W, k = q / W;
         Es[q] = AT(E, L, i, k);
@@ -563,98 +563,136 @@ __device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T 
  * the row recurrence contracts by at least 1/4 per row, so the start
  * error is below rounding when the segment's own rows begin.  Rows above
  * the segment are relaxed by the early half-sweeps as far as the later
- * ones need them, and only the segment's rows are stored. */
+ * ones need them, and only the segment's rows are stored.
+ *
+ * Register use: a half-sweep's last two results live in two arrays that
+ * swap roles every step (the loop runs two steps per trip), and R and the
+ * input rows are re-read through L1, prefetched SMOOTH_PF rows ahead. */
 #define RELAX_WARM_F 40
+#define SMOOTH_PF 8
+struct SmoothArgs {
+    int nx, nz, pitch, l, sp, ce, co, kind_e, kind_o, kw, ks, ke;
+    bool ld_ok, st_e, st_o, plain_cols;
+};
+
+template <class T>
+__device__ __forceinline__ typename Pair2<T>::type ld_pair(const T* a, const SmoothArgs& g, int k)
+{
+    typename Pair2<T>::type v; v.x = T(0); v.y = T(0);
+    if (g.ld_ok && k >= 0 && k <= g.nz) v = *reinterpret_cast<const typename Pair2<T>::type*>(a + (size_t)k * g.pitch + g.ce);
+    return v;
+}
+
+/* one row step: h1 = results of step r-1 (read only), h2 = results of step
+ * r-2 on entry and of step r on exit */
+template <class T, int S>
+__device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T (&h2)[2 * S],
+                                            const T* __restrict__ E, const T* __restrict__ R, T* __restrict__ EO,
+                                            const MgConst& m, const RelaxK<T>& K, const SmoothArgs& g,
+                                            const double* __restrict__ inside0)
+{
+    typedef typename Pair2<T>::type T2;
+    constexpr int H = 2 * S;
+    if (g.ld_ok) {
+        const int kp = r + 1 + SMOOTH_PF;
+        if (kp <= g.nz) {
+            asm volatile("prefetch.global.L1 [%0];" :: "l"(E + (size_t)kp * g.pitch + g.ce));
+            asm volatile("prefetch.global.L1 [%0];" :: "l"(R + (size_t)(kp - 1) * g.pitch + g.ce));
+        }
+    }
+    const T2 inm = ld_pair(E, g, r - 1), in0 = ld_pair(E, g, r), inp = ld_pair(E, g, r + 1);
+    T nb[H];
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+        const T src = (h == 0) ? in0.y : h1[h - 1];
+        nb[h] = (h & 1) ? __shfl_down_sync(0xffffffffu, src, 1) : __shfl_up_sync(0xffffffffu, src, 1);
+    }
+    /* all half-sweeps on interior rows of this segment, no side column in the warp */
+    const bool plain = g.plain_cols && (r - (H - 1) >= g.kw) && (r - (H - 1) >= 1) && (r <= g.nz - 1) && (r <= g.ke - 1);
+    if (plain) {
+#pragma unroll
+        for (int h = H - 1; h >= 0; h--) {
+            constexpr bool dummy = false; (void)dummy;
+            const bool odd = h & 1;
+            const T old = (h == 0) ? in0.x : (h == 1) ? inm.y : h2[h - 2];
+            const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
+            const T own_other = (h == 0) ? in0.y : h1[h - 1];
+            (void)old;
+            const T2 rk = ld_pair(R, g, r - h);
+            h2[h] = odd ? rx_in(rk.y, h1[h], up, own_other, nb[h], K) : rx_in(rk.x, h1[h], up, nb[h], own_other, K);
+        }
+    } else {
+#pragma unroll
+        for (int h = H - 1; h >= 0; h--) {
+            const int k = r - h;
+            const bool odd = h & 1;
+            const int top = min(g.nz, g.ke - 1 + (H - 1 - h) / 2);
+            if (k < g.kw || k > top) { h2[h] = h1[h]; continue; }
+            const T old = (h == 0) ? in0.x : (h == 1) ? inm.y : h2[h - 2];
+            const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
+            const T own_other = (h == 0) ? in0.y : h1[h - 1];
+            const T xm = odd ? own_other : nb[h];
+            const T xp = odd ? nb[h] : own_other;
+            const T2 rk = ld_pair(R, g, k);
+            const T rv = odd ? rk.y : rk.x;
+            if (k > 0 && k < g.nz)
+                h2[h] = rx_row<T>(odd ? g.kind_o : g.kind_e, rv, h1[h], up, xm, xp, old, K);
+            else
+                h2[h] = relax_val<T>(m, K, g.nx, g.nz, g.l, g.sp, odd ? g.co : g.ce, k, rv, h1[h], up, xm, xp, old, inside0);
+        }
+    }
+    const int kS = r - (H - 1);
+    if (kS >= g.ks && kS < g.ke) {
+        T* dst = EO + (size_t)kS * g.pitch;
+        T2 v; v.x = h1[H - 2]; v.y = h2[H - 1];       /* the even half finished this row one step ago */
+        if (g.st_e && g.st_o) *reinterpret_cast<T2*>(dst + g.ce) = v;
+        else if (g.st_e) dst[g.ce] = v.x;
+    }
+}
+
 template <class T, int S>
 __global__ void __launch_bounds__(128) k_mg_smooth(MgConst m, MgLvlT<T> L, int l, int seg_len,
                                                    const double* __restrict__ inside0)
 {
-    typedef typename Pair2<T>::type T2;
     constexpr int H = 2 * S;
     const int lane = threadIdx.x;
     const int warp = blockIdx.x * blockDim.y + threadIdx.y;
     const int sp = blockIdx.z;
-    const int nx = L.nx, nz = L.nz, pitch = L.pitch;
+    SmoothArgs g;
+    g.nx = L.nx; g.nz = L.nz; g.pitch = L.pitch; g.l = l; g.sp = sp;
     const int OUTP = 32 - 2 * S;
     const int c0 = warp * 2 * OUTP - 2 * S;
-    const int ce = c0 + 2 * lane, co = ce + 1;
-    if (warp * 2 * OUTP > nx) return;            /* whole warp: strip starts past the last column */
-    const bool ld_ok = ce >= 0 && co < pitch;
-    const bool st_e = lane >= S && lane <= 31 - S && ce >= 0 && ce <= nx;
-    const bool st_o = lane >= S && lane <= 31 - S && co >= 0 && co <= nx;
-    const int ks = blockIdx.y * seg_len;
-    if (ks > nz) return;
-    const int ke = min(ks + seg_len, nz + 1);
-    const int kw = max(0, ks - RELAX_WARM_F);
-    const T* __restrict__ E = L.e[sp];
-    const T* __restrict__ R = L.r[sp];
-    T* __restrict__ EO = L.e2[sp];
+    g.ce = c0 + 2 * lane; g.co = g.ce + 1;
+    if (warp * 2 * OUTP > g.nx) return;            /* whole warp: strip starts past the last column */
+    g.ld_ok = g.ce >= 0 && g.co < g.pitch;
+    g.st_e = lane >= S && lane <= 31 - S && g.ce >= 0 && g.ce <= g.nx;
+    g.st_o = lane >= S && lane <= 31 - S && g.co >= 0 && g.co <= g.nx;
+    g.ks = blockIdx.y * seg_len;
+    if (g.ks > g.nz) return;
+    g.ke = min(g.ks + seg_len, g.nz + 1);
+    g.kw = max(0, g.ks - RELAX_WARM_F);
+    const T* __restrict__ E = SP(L.e);
+    const T* __restrict__ R = SP(L.r);
+    T* __restrict__ EO = SP(L.e2);
     const RelaxK<T> K = relax_k<T>(m, l, sp);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
-    const int kind_e = col_kind(ce, nx, oxy, top_levels), kind_o = col_kind(co, nx, oxy, top_levels);
-    auto ld = [&](const T* a, int k) -> T2 {
-        T2 v; v.x = T(0); v.y = T(0);
-        if (ld_ok && k >= 0 && k <= nz) v = *reinterpret_cast<const T2*>(a + (size_t)k * pitch + ce);
-        return v;
-    };
-    /* h1[h]/h2[h]: half-sweep h's results of steps r-1 and r-2 (its own
-     * column parity); inm/in0/inp: input rows r-1, r, r+1; rr[j]: R row r-j */
-    T h1[H], h2[H], cur[H];
-    T2 rr[H];
-    T2 inm = ld(E, kw - 1), in0 = ld(E, kw), inp = ld(E, kw + 1);
+    g.kind_e = col_kind(g.ce, g.nx, oxy, top_levels);
+    g.kind_o = col_kind(g.co, g.nx, oxy, top_levels);
+    /* lanes whose columns are outside 0..nx compute garbage that no written
+     * lane reads; only real side columns need the per-lane path */
+    const bool side_e = (g.ce == 0 || g.ce == g.nx), side_o = (g.co == 0 || g.co == g.nx);
+    g.plain_cols = !__any_sync(0xffffffffu, side_e || side_o);
+    T a[H], b[H];
+    {
+        const typename Pair2<T>::type e0 = ld_pair(E, g, g.kw - 1);
 #pragma unroll
-    for (int h = 0; h < H; h++) {
-        h1[h] = (h & 1) ? inm.y : inm.x;       /* value below the first row: pre-smoothing */
-        h2[h] = h1[h];
-        rr[h].x = T(0); rr[h].y = T(0);
+        for (int h = 0; h < H; h++) { a[h] = (h & 1) ? e0.y : e0.x; b[h] = a[h]; }
     }
-    T2 nr1 = ld(R, kw), nr2 = ld(R, kw + 1);
-    T2 ne1 = ld(E, kw + 2), ne2 = ld(E, kw + 3);
-    const int r_end = ke - 1 + (H - 1);
-    for (int r = kw; r <= r_end; r++) {
-#pragma unroll
-        for (int j = H - 1; j > 0; j--) rr[j] = rr[j - 1];
-        rr[0] = nr1;
-        const T2 nr3 = ld(R, r + 2), ne3 = ld(E, r + 4);     /* two rows ahead */
-        /* neighbours from other lanes, all from the previous step */
-        T nb[H];
-#pragma unroll
-        for (int h = 0; h < H; h++) {
-            const T src = (h == 0) ? in0.y : h1[h - 1];
-            nb[h] = (h & 1) ? __shfl_down_sync(0xffffffffu, src, 1) : __shfl_up_sync(0xffffffffu, src, 1);
-        }
-#pragma unroll
-        for (int h = 0; h < H; h++) {
-            const int k = r - h;
-            const int top = min(nz, ke - 1 + (H - 1 - h) / 2);
-            if (k < kw || k > top) { cur[h] = h1[h]; continue; }
-            const bool odd = h & 1;
-            /* inputs from the half-sweep two before (same parity), the one before (other parity) */
-            const T old = (h == 0) ? in0.x : (h == 1) ? inm.y : h2[h - 2];
-            const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
-            const T own_other = (h == 0) ? in0.y : h1[h - 1];      /* odd column c+1 / even column c-1 */
-            const T xm = odd ? own_other : nb[h];
-            const T xp = odd ? nb[h] : own_other;
-            const T rv = odd ? rr[h].y : rr[h].x;
-            const int col = odd ? co : ce;
-            if (k > 0 && k < nz)
-                cur[h] = rx_row<T>(odd ? kind_o : kind_e, rv, h1[h], up, xm, xp, old, K);
-            else
-                cur[h] = relax_val<T>(m, K, nx, nz, l, sp, col, k, rv, h1[h], up, xm, xp, old, inside0);
-        }
-        const int kS = r - (H - 1);
-        if (kS >= ks && kS < ke) {
-            T* dst = EO + (size_t)kS * pitch;
-            T2 v; v.x = h1[H - 2]; v.y = cur[H - 1];              /* even half finished this row one step ago */
-            if (st_e && st_o) *reinterpret_cast<T2*>(dst + ce) = v;
-            else if (st_e) dst[ce] = v.x;
-        }
-#pragma unroll
-        for (int h = 0; h < H; h++) { h2[h] = h1[h]; h1[h] = cur[h]; }
-        inm = in0; in0 = inp; inp = ne1;
-        ne1 = ne2; ne2 = ne3;
-        nr1 = nr2; nr2 = nr3;
+    const int r_end = g.ke - 1 + (H - 1);
+    for (int r = g.kw; r <= r_end; r += 2) {
+        smooth_step<T, S>(r, a, b, E, R, EO, m, K, g, inside0);
+        if (r + 1 <= r_end) smooth_step<T, S>(r + 1, b, a, E, R, EO, m, K, g, inside0);
     }
 }
 
@@ -674,17 +712,17 @@ __global__ void k_mg_restrict(MgConst m, MgLvlT<T> Lc, MgLvlT<T> Lf, int l, cons
     int nxp = X * d0 / d < X ? X * d0 / d : X;
     int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
     const T h2 = (T)(m.bl2 * d * d);
-    const T dt = (T)m.dt, D = (T)m.D[sp];
+    const T dt = (T)m.dt, D = (T)SP(m.D);
     const T half = (T)0.5;
     const bool oxy = sp == 1;
     int i0 = (i - nx / 2) * d + X / 2;
     i0 = i0 < 0 ? 0 : (i0 > X ? X : i0);   /* clamped to BoxX as in the reference */
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
-    const T* EP = Lf.e[sp];
-    const T* RP = Lf.r[sp];
-    const double* AP = Lf.s[sp];
-    const double* AL = Lc.s[sp];
-    T* R = &AT(Lc.r[sp], Lc, i, k);
+    const T* EP = SP(Lf.e);
+    const T* RP = SP(Lf.r);
+    const double* AP = SP(Lf.s);
+    const double* AL = SP(Lc.s);
+    T* R = &AT(SP(Lc.r), Lc, i, k);
 #define EPv(a, b) at_ref(EP, Lf, a, b)
 #define RPv(a, b) at_ref(RP, Lf, a, b)
 #define APv(a, b) ((T)at_ref(AP, Lf, a, b))
@@ -751,8 +789,8 @@ __global__ void k_mg_interp(MgConst m, MgLvlT<T> Lf, MgLvlT<T> Lc, int l)
     const int X = m.box_x;
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
-    const T* C = Lc.e[sp];
-    T& e = AT(Lf.e[sp], Lf, i, k);
+    const T* C = SP(Lc.e);
+    T& e = AT(SP(Lf.e), Lf, i, k);
     const T half = (T)0.5, quarter = (T)0.25;
 #define CV(a, b) at_ref(C, Lc, a, b)
     if (i % 2 == 0) {
@@ -778,8 +816,8 @@ __global__ void k_mg_reset_zero(MgLvlT<T> L, int zero_res)
     int sp = blockIdx.y;
     if (idx >= (L.nx + 1) * (L.nz + 1)) return;
     int i = idx % (L.nx + 1), k = idx / (L.nx + 1);
-    AT(L.e[sp], L, i, k) = 0;
-    if (zero_res) AT(L.r[sp], L, i, k) = 0;
+    AT(SP(L.e), L, i, k) = 0;
+    if (zero_res) AT(SP(L.r), L, i, k) = 0;
 }
 
 /* updateSolAgaElementwise, Multigrid.cpp:544-568 */
@@ -794,11 +832,11 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l)
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d < X ? X * d0 / d : X;
     int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
-    AT(L.r[sp], L, i, k) = 0;
+    AT(SP(L.r), L, i, k) = 0;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
-    double& e = AT(L.e[sp], L, i, k);
+    double& e = AT(SP(L.e), L, i, k);
     if (l < m.A && (l == 0 || ip <= 0 || ip >= nxp || kp >= nzp)) {
-        double& a = AT(L.s[sp], L, i, k);
+        double& a = AT(SP(L.s), L, i, k);
         a += e;
         if (sp == 0) a = dmaxd(dmind(a, m.max_carbon), 0.0);
         else if (sp == 1) a = dmaxd(dmind(a, m.max_o2_agar), 0.0);
@@ -820,13 +858,13 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
     int nxp = X * d0 / d < X ? X * d0 / d : X;
     int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
     double h2 = m.bl2 * d * d;
-    const double dt = m.dt, D = m.D[sp];
+    const double dt = m.dt, D = SP(m.D);
     const bool oxy = sp == 1;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
-    const double* A = L.s[sp];
-    double* R = &AT(L.r[sp], L, i, k);
+    const double* A = SP(L.s);
+    double* R = &AT(SP(L.r), L, i, k);
 #define AL(a, b) AT(A, L, a, b)
-#define APv(a, b) AT(Lp.s[sp], Lp, a, b)
+#define APv(a, b) AT(SP(Lp.s), Lp, a, b)
     if (i == 0 || i == nx) {
         if (l == m.A - 1) {
             int sx = (i == 0) ? 1 : -1;
@@ -879,17 +917,17 @@ __global__ void k_mg_rewrite_bdry(MgConst m, MgLvl L, MgLvl Lc, int l)
     int d = 1 << l, d0 = 1 << m.A;
     const int nx = L.nx, nz = L.nz;
     int nx2 = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
-    const double* C = Lc.s[sp];
+    const double* C = SP(Lc.s);
     if (t < nx + 1) {
         int i = t, k2 = nz / 2;
         int i2 = nx2 / 2 + i / 2 - nx / 4, i2p1 = nx2 / 2 + (i + 1) / 2 - nx / 4;
-        AT(L.s[sp], L, i, nz) = (AT(C, Lc, i2, k2) + AT(C, Lc, i2p1, k2)) / 2;
+        AT(SP(L.s), L, i, nz) = (AT(C, Lc, i2, k2) + AT(C, Lc, i2p1, k2)) / 2;
     } else if (t < nx + 1 + 2 * nz) {
         int u = t - (nx + 1);
         int k = u >> 1, side = u & 1;
         int i = side ? nx : 0;
         int i2 = nx2 / 2 + i / 2 - nx / 4;
-        AT(L.s[sp], L, i, k) = (AT(C, Lc, i2, k / 2) + AT(C, Lc, i2, (k + 1) / 2)) / 2;
+        AT(SP(L.s), L, i, k) = (AT(C, Lc, i2, k / 2) + AT(C, Lc, i2, (k + 1) / 2)) / 2;
     }
 }
 
@@ -906,7 +944,7 @@ __global__ void k_mg_nest(MgConst m, MgLvl L, MgLvl Lf, int l)
     int nxp = X * d0 / d < X ? X * d0 / d : X;
     int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
-    if (ip > 0 && ip < nxp && kp < nzp) AT(L.s[sp], L, i, k) = AT(Lf.s[sp], Lf, ip, kp);
+    if (ip > 0 && ip < nxp && kp < nzp) AT(SP(L.s), L, i, k) = AT(SP(Lf.s), Lf, ip, kp);
 }
 
 /* copyToMG, Multigrid.cpp:891-907: wall-under-colony values into level 0,
@@ -927,7 +965,7 @@ __global__ void k_mg_copy_edge(MgLvl L)
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     int sp = blockIdx.y;
     if (k > L.nz) return;
-    AT(L.s[sp], L, L.nx, k) = AT(L.s[sp], L, 0, k);
+    AT(SP(L.s), L, L.nx, k) = AT(SP(L.s), L, 0, k);
 }
 /* copyFromMG, Multigrid.cpp:958-981: wall rows of both buffers (the agar
  * field is read straight from the solution rows 1..BoxZAgar) */
@@ -1255,12 +1293,12 @@ __global__ void k_mg_defect(MgConst m, MgLvlT<T> L, MgLvl L64, int l, const doub
         bool uncovered = (l == 0 || ip <= 0 || ip >= nxp || kp >= nzp);
         if (uncovered) {
             int kind; double cfac;
-            double v = relax_eval<T>(m, L, L64.r[sp], l, sp, i, k, inside0, kind, cfac);
+            double v = relax_eval<T>(m, L, SP(L64.r), l, sp, i, k, inside0, kind, cfac);
             if (kind != 0) {
-                double e = (double)AT(L.e[sp], L, i, k);
+                double e = (double)AT(SP(L.e), L, i, k);
                 double def = (kind == 1) ? (v - e) : (v - e) * (cfac + 2) / cfac;
                 dmax = fabs(def);
-                rmax = fabs(AT(L64.r[sp], L64, i, k));
+                rmax = fabs(AT(SP(L64.r), L64, i, k));
             }
         }
     }

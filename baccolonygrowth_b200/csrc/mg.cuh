@@ -35,3 +35,12 @@ void mg_reset(bcg_ctx* c, const MgConst& m);
 void mg_copy_to(bcg_ctx* c, const MgConst& m, int wall_buf);
 void mg_copy_from(bcg_ctx* c, const MgConst& m, int cur_wall);
 int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf);
+
+/* One of three kernel-parameter array entries by a runtime index without
+ * indexing the parameter array itself (a runtime index into a parameter
+ * array makes the compiler copy the whole parameter block to per-thread
+ * local memory). */
+template <class P>
+__device__ __forceinline__ P pick3(const P& a0, const P& a1, const P& a2, int i) { return i == 0 ? a0 : (i == 1 ? a1 : a2); }
+#define SP(arr) pick3((arr)[0], (arr)[1], (arr)[2], sp)
+
