@@ -196,6 +196,7 @@ PROTOTYPES = {
     "bcg_colony_sweeps": (_I, [_VP, _I, _I]),
     "bcg_mg_solve_tol": (_I, [_VP, _D, _I, _I, _PI, _PD]),
     "bcg_autotune": (_I, [_VP, _I, _PI]),
+    "bcg_set_pair_precision": (_I, [_VP, _I]),
     "bcg_enable_timers": (_I, [_VP, _I]),
     "bcg_get_timer": (_I, [_VP, _I, _PD, _PI64]),
     "bcg_rng_seed": (None, [ctypes.POINTER(Rng), ctypes.c_uint32]),

@@ -232,6 +232,10 @@ class Colony:
         _abi.check(self.lib.bcg_get_timer(self.h, _abi.TIMERS[name], ctypes.byref(ms), ctypes.byref(n)), "bcg_get_timer")
         return ms.value, n.value
 
+    def set_pair_precision(self, bits):
+        """bcg_set_pair_precision: 64 (reference FP64 geometry) or 32."""
+        _abi.check(self.lib.bcg_set_pair_precision(self.h, int(bits)), "bcg_set_pair_precision")
+
     def autotune(self, what):
         """bcg_autotune: 'FORCE_GROUP' or 'SMOOTHER'; returns the choice."""
         ch = ctypes.c_int()

@@ -83,12 +83,12 @@ __device__ __forceinline__ bool keep_neighbour(V3 ap, V3 aq, double aL, double a
     return false;
 }
 
-/* F_cc, Forces.cpp:13-84.  Returns false (F = 0) when the cells do not
+/* F_cc, Forces.cpp:13-84, from the closest points c1 (on a), c2 (on b)
+ * and their distance d.  Returns false (F = 0) when the cells do not
  * overlap, in which case the reference's contribution is a signed zero. */
-__device__ __forceinline__ bool pair_force(const Cst& a, V3 acm, const Cst& b, const MechParams& mp, V3& F, V3& r)
+__device__ __forceinline__ bool pair_force_at(const Cst& a, V3 acm, const Cst& b, const MechParams& mp,
+                                              V3 c1, V3 c2, double d, V3& F, V3& r)
 {
-    V3 c1, c2;
-    double d = seg_distance(a.p, a.q, b.p, b.q, c1, c2);
     double sigma = a.R + b.R;
     double delta = dmax_(sigma - d, 0.0);
     if (!(delta > 0.0)) return false;
@@ -113,6 +113,50 @@ __device__ __forceinline__ bool pair_force(const Cst& a, V3 acm, const Cst& b, c
         F = add3(add3(FE, FDt), FDn);
     } else F = FE;
     return true;
+}
+
+/* F_cc with the reference's FP64 min_distance */
+__device__ __forceinline__ bool pair_force(const Cst& a, V3 acm, const Cst& b, const MechParams& mp, V3& F, V3& r)
+{
+    V3 c1, c2;
+    double d = seg_distance(a.p, a.q, b.p, b.q, c1, c2);
+    return pair_force_at(a, acm, b, mp, c1, c2, d, F, r);
+}
+
+/* min_distance in FP32 on offsets local to a reference point (the centre
+ * of cell a): the offsets are a few um, so their FP32 rounding is ~1e-7 um
+ * where absolute positions (up to 1e4 um) would lose ~1e-3 um */
+struct F3 { float x, y, z; };
+__device__ __forceinline__ F3 f3_off(V3 a, V3 o) { F3 r; r.x = (float)(a.x - o.x); r.y = (float)(a.y - o.y); r.z = (float)(a.z - o.z); return r; }
+__device__ __forceinline__ float f3_dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float clamp01f(float n) { return n < 0.f ? 0.f : (n > 1.f ? 1.f : n); }
+__device__ __forceinline__ float seg_distance_f(F3 p1, F3 q1, F3 p2, F3 q2, F3& c1, F3& c2)
+{
+    F3 v1 = {q1.x - p1.x, q1.y - p1.y, q1.z - p1.z}, v2 = {q2.x - p2.x, q2.y - p2.y, q2.z - p2.z};
+    F3 r = {p1.x - p2.x, p1.y - p2.y, p1.z - p2.z};
+    float l1 = f3_dot(v1, v1), l2 = f3_dot(v2, v2), f = f3_dot(v2, r), c = f3_dot(v1, r), b = f3_dot(v1, v2);
+    float denom = l1 * l2 - b * b, s, t;
+    if (denom != 0.f) s = clamp01f((b * f - c * l2) / denom);
+    else s = 0.f;
+    float tnom = b * s + f;
+    if (tnom < 0.f) { t = 0.f; s = clamp01f(-c / l1); }
+    else if (tnom > l2) { t = 1.f; s = clamp01f((b - c) / l1); }
+    else t = tnom / l2;
+    c1 = {p1.x + v1.x * s, p1.y + v1.y * s, p1.z + v1.z * s};
+    c2 = {p2.x + v2.x * t, p2.y + v2.y * t, p2.z + v2.z * t};
+    F3 cv = {c1.x - c2.x, c1.y - c2.y, c1.z - c2.z};
+    return sqrtf(f3_dot(cv, cv));
+}
+
+/* F_cc with the contact geometry in FP32 local to cell a; the force terms,
+ * the contact point and the sums stay FP64 */
+__device__ __forceinline__ bool pair_force_f32geom(const Cst& a, V3 acm, const Cst& b, const MechParams& mp, V3& F, V3& r)
+{
+    F3 c1f, c2f;
+    float df = seg_distance_f(f3_off(a.p, acm), f3_off(a.q, acm), f3_off(b.p, acm), f3_off(b.q, acm), c1f, c2f);
+    V3 c1 = mk(acm.x + (double)c1f.x, acm.y + (double)c1f.y, acm.z + (double)c1f.z);
+    V3 c2 = mk(acm.x + (double)c2f.x, acm.y + (double)c2f.y, acm.z + (double)c2f.z);
+    return pair_force_at(a, acm, b, mp, c1, c2, (double)df, F, r);
 }
 
 /* one locus of F_cw, Forces.cpp:96-152 (var_pos = 0, so the locus sits at

@@ -105,6 +105,7 @@ struct bcg_ctx {
     /* multigrid Err (all levels) and Res (levels > 0) are zero, as the last
      * reset() left them; setup() then skips its resetZero */
     int mg_clean;
+    int pair_f32;          /* contact geometry in FP32 local to cell i (bcg_set_pair_precision) */
 };
 
 MechParams mech_params(const bcg_ctx* c);

@@ -256,7 +256,7 @@ extern "C" int bcg_rebuild_neighbours(bcg_ctx* c)
 /* Forces on `a` from its neighbour list (lanes of a G-wide group split the
  * list; the group reduces with a fixed butterfly), plus the wall, drag and
  * surface-tension terms (sum_forces, Forces.cpp:332-381). */
-template <int G>
+template <int G, bool GEOM32>
 __device__ __forceinline__ void sum_forces_group(const Cst& a, int me, const CellRec* __restrict__ old,
                                                  const int* __restrict__ list, int cnt, double wall_z,
                                                  const FieldPtrs& fp, const MechParams& mp,
@@ -269,7 +269,7 @@ __device__ __forceinline__ void sum_forces_group(const Cst& a, int me, const Cel
         int id = __ldg(&list[j]);
         Cst b = load_cst(&old[id]);
         V3 f, r;
-        if (pair_force(a, cm, b, mp, f, r)) {
+        if (GEOM32 ? pair_force_f32geom(a, cm, b, mp, f, r) : pair_force(a, cm, b, mp, f, r)) {
             F = add3(F, f);
             T = add3(T, cross3(sub3(r, cm), f));
         }
@@ -299,7 +299,7 @@ __device__ __forceinline__ void sum_forces_group(const Cst& a, int me, const Cel
     Fnet = F; Tnet = T;
 }
 
-template <int G>
+template <int G, bool GEOM32>
 __global__ void __launch_bounds__(256) k_move_grow(int n, int nbinned, const int* __restrict__ order,
         const CellRec* __restrict__ old, CellRec* __restrict__ nw,
         const int* __restrict__ nbr, const int* __restrict__ ncount,
@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(256) k_move_grow(int n, int nbinned, const int
         int cnt = __ldg(&ncount[me]);
         V3 F, T, sf, df;
         /* integrate, Integrate.cpp:11-32 */
-        sum_forces_group<G>(o, me, old, list, cnt, wall_z, fp, mp, F, T, sf, df, near1);
+        sum_forces_group<G, GEOM32>(o, me, old, list, cnt, wall_z, fp, mp, F, T, sf, df, near1);
         Cst tmp = o;
         half_kick(dt, F, T, o, tmp.v, tmp.w);
         V3 rcmp = sub3(o.p, ocm), rcmq = sub3(o.q, ocm);
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(256) k_move_grow(int n, int nbinned, const int
         tmp.p = add3(o.p, scl3(vp, dt));
         tmp.q = add3(o.q, scl3(vq, dt));
         tmp.p.y = 0; tmp.q.y = 0;
-        sum_forces_group<G>(tmp, me, old, list, cnt, wall_z, fp, mp, F, T, sf, df, near2);
+        sum_forces_group<G, GEOM32>(tmp, me, old, list, cnt, wall_z, fp, mp, F, T, sf, df, near2);
         Cst nc = tmp;
         half_kick(dt, F, T, tmp, nc.v, nc.w);
         nc.v.y = 0;
@@ -409,13 +409,26 @@ int launch_move_grow(bcg_ctx* c, double dt, int group)
         unsigned blocks = (unsigned)((tot + threads - 1) / threads);
         const CellRec* old = c->rec[c->cur];
         CellRec* nw = c->rec[c->cur ^ 1];
-        switch (group) {
-        case 1: k_move_grow<1><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
-        case 2: k_move_grow<2><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
-        case 4: k_move_grow<4><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
-        case 8: k_move_grow<8><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
-        default: k_move_grow<16><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status); break;
+#define MG_ARGS(G, M) k_move_grow<G, M><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, \
+            c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status)
+        if (c->pair_f32) {
+            switch (group) {
+            case 1: MG_ARGS(1, true); break;
+            case 2: MG_ARGS(2, true); break;
+            case 4: MG_ARGS(4, true); break;
+            case 8: MG_ARGS(8, true); break;
+            default: MG_ARGS(16, true); break;
+            }
+        } else {
+            switch (group) {
+            case 1: MG_ARGS(1, false); break;
+            case 2: MG_ARGS(2, false); break;
+            case 4: MG_ARGS(4, false); break;
+            case 8: MG_ARGS(8, false); break;
+            default: MG_ARGS(16, false); break;
+            }
         }
+#undef MG_ARGS
         c->launches++;
         BCG_CUDA_TRY(cudaGetLastError());
     }
@@ -457,6 +470,14 @@ static int time_move_grow(bcg_ctx* c, int group, int reps, float* ms)
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return rc;
+}
+
+extern "C" int bcg_set_pair_precision(bcg_ctx* c, int bits)
+{
+    if (!c || (bits != 32 && bits != 64)) return BCG_E_ARG;
+    int f32 = bits == 32;
+    if (f32 != c->pair_f32) { c->pair_f32 = f32; nutrient_graphs_drop(c); }
+    return BCG_OK;
 }
 
 extern "C" int bcg_autotune(bcg_ctx* c, int what, int* choice)

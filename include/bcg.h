@@ -307,6 +307,13 @@ int bcg_mg_solve_tol(bcg_ctx* ctx, double rel_tol, int precision, int max_iters,
  *                         changes only the multigrid's correction scratch.
  * The choice also becomes the default of contexts created afterwards.
  * Synchronises the stream; not for use inside a stream capture. */
+/* Precision of the per-pair contact geometry in MoveCell (no reference
+ * counterpart).  64 (default): the reference's FP64 min_distance.  32: the
+ * closest points and their distance in FP32 on offsets local to cell i
+ * (min_distance's steps unchanged), the contact forces, positions and
+ * force sums in FP64.  Neighbour lists are built in FP64 either way. */
+int bcg_set_pair_precision(bcg_ctx* ctx, int bits);
+
 typedef enum bcg_tune_id { BCG_TUNE_FORCE_GROUP = 1, BCG_TUNE_SMOOTHER = 2 } bcg_tune_id;
 int bcg_autotune(bcg_ctx* ctx, int what, int* choice);
 

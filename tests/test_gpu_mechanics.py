@@ -194,3 +194,33 @@ def test_autotune_keeps_state(gpu):
     assert np.array_equal(lin, lin_o)
     assert_cells_close(orc.cells(), col.cells())
 
+
+def test_pair_geometry_fp32(gpu):
+    """Contact geometry in FP32 on offsets local to cell i (bcg_set_pair_precision
+    32): over 20 steps without divisions the colony stays within rounding
+    of the FP64 run (positions 1e-7 relative to the colony extent,
+    velocities 1e-2 relative to the largest velocity), and the first step's
+    F_cw draw count is the same."""
+    def mutate(cells):
+        cells["ldiv"][:] = 1e9
+    p, orc, col, rng = setup_pair(mutate=mutate)
+    cells = col.cells()
+    col32 = Colony(p, cells)
+    for f in ("HEIGHT", "NORMAL_X", "NORMAL_Z", "WALL", "ENV_GROWTH1"):
+        col32.set_field(f, col.field(f))
+    col32.set_pair_precision(32)
+    for c in (col, col32):
+        c.rebuild_neighbours()
+    for s in range(20):
+        n64, f64 = col.move_grow(p.dt)
+        n32, f32 = col32.move_grow(p.dt)
+        assert n64 == n32 == 0
+        if s == 0:
+            assert f64 == f32                  # same state: same wall-near cells
+        col.divide(np.zeros(0, np.float32), 0.0)
+        col32.divide(np.zeros(0, np.float32), 0.0)
+    a, b = col.cells(), col32.cells()
+    assert rel_err(a["p"], b["p"]) <= 1e-7 and rel_err(a["q"], b["q"]) <= 1e-7
+    assert rel_err(a["velocity"], b["velocity"]) <= 1e-2
+    col32.close()
+
