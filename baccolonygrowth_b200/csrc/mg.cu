@@ -845,7 +845,13 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l)
     e = 0;
 }
 
-/* updateResAgaElementwise, Multigrid.cpp:570-701 */
+/* updateResAgaElementwise, Multigrid.cpp:570-701.  SETUP: the setup()
+ * form after a reset() (Err zero everywhere, Res zero on levels > 0):
+ * updateSolAga then only clamps the solution at the uncovered points and
+ * zeroes Res, so one pass clamps the stencil values as it reads them,
+ * stores the point's clamped value where the clamp changed it, and
+ * writes Res (0 where updateResAga leaves it). */
+template <bool SETUP>
 __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const double* __restrict__ inside0)
 {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -863,49 +869,66 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     const double* A = SP(L.s);
     double* R = &AT(SP(L.r), L, i, k);
-#define AL(a, b) AT(A, L, a, b)
+    const double hi = sp == 0 ? m.max_carbon : (sp == 1 ? m.max_o2_agar : 1e300);
+    /* the solution value updateSolAga leaves at (a, b): clamped where uncovered */
+    auto sol = [&](int a, int b) -> double {
+        double v = AT(A, L, a, b);
+        if (SETUP) {
+            int ipa = 2 * a - nx + nxp / 2, kpa = 2 * b;
+            if (l == 0 || ipa <= 0 || ipa >= nxp || kpa >= nzp) v = dmaxd(dmind(v, hi), 0.0);
+        }
+        return v;
+    };
+    double res = 0.0;
+    bool set = SETUP;
+#define AL(a, b) sol(a, b)
 #define APv(a, b) AT(SP(Lp.s), Lp, a, b)
     if (i == 0 || i == nx) {
         if (l == m.A - 1) {
             int sx = (i == 0) ? 1 : -1;
-            if (oxy) *R = 0;
-            else if (k == 0) *R = (2 * AL(i + sx, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
-            else if (k == nz) *R = (2 * AL(i + sx, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D * dt / h2;
-            else *R = (2 * AL(i + sx, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
+            if (oxy) set = true, res = 0;
+            else if (k == 0) set = true, res = (2 * AL(i + sx, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
+            else if (k == nz) set = true, res = (2 * AL(i + sx, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D * dt / h2;
+            else set = true, res = (2 * AL(i + sx, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
         }
     } else if (k == nz) {
         if (l == m.A - 1) {
             /* oxygen omits dt here, as the reference does (Multigrid.cpp:634) */
-            if (oxy) *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D / h2;
-            else *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * dt * D / h2;
+            if (oxy) set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D / h2;
+            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * dt * D / h2;
         }
     } else if (k == 0) {
         if (l == 0) {
-            if (inside0[(size_t)i * m.box_z] > 0) *R = 0;
-            else if (oxy) *R = m.max_o2_agar - AL(i, k);
-            else *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            if (inside0[(size_t)i * m.box_z] > 0) set = true, res = 0;
+            else if (oxy) set = true, res = m.max_o2_agar - AL(i, k);
+            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
         } else if ((ip > 0 && ip < nxp) != 1) {
-            if (oxy) *R = m.max_o2_agar - AL(i, k);
-            else if (ip == 0) *R = (APv(ip + 2, kp) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
-            else if (ip == nxp) *R = (APv(ip - 2, kp) + AL(i + 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
-            else *R = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            if (oxy) set = true, res = m.max_o2_agar - AL(i, k);
+            else if (ip == 0) set = true, res = (APv(ip + 2, kp) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else if (ip == nxp) set = true, res = (APv(ip - 2, kp) + AL(i + 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
         }
     } else {
         if (l > 0) {
             if (kp == nzp && ip > 0 && ip < nxp)
-                *R = (AL(i + 1, k) + AL(i - 1, k) + APv(ip, kp - 2) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (AL(i + 1, k) + AL(i - 1, k) + APv(ip, kp - 2) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
             else if (ip == 0 && kp < nzp)
-                *R = (APv(ip + 2, kp) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (APv(ip + 2, kp) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
             else if (ip == nxp && kp < nzp)
-                *R = (AL(i + 1, k) + APv(ip - 2, kp) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (AL(i + 1, k) + APv(ip - 2, kp) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
             else if (ip <= 0 || ip >= nxp || kp >= nzp)
-                *R = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
         } else {
-            *R = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            set = true, res = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
         }
     }
 #undef AL
 #undef APv
+    if (set) *R = res;
+    if (SETUP) {
+        double v = AT(A, L, i, k), w = sol(i, k);
+        if (w != v) AT(SP(L.s), L, i, k) = w;
+    }
 }
 
 /* rewriteSolBdryAga, Multigrid.cpp:469-503 (top row, then the side columns) */
@@ -1166,9 +1189,9 @@ template void mg_vcycle_t<float>(bcg_ctx*, const MgConst&, int, int);
 
 void mg_vcycle(bcg_ctx* c, const MgConst& m, int mu1, int mu2) { mg_vcycle_t<double>(c, m, mu1, mu2); }
 
-static void reset_zero(bcg_ctx* c)
+static void reset_zero(bcg_ctx* c, int from_level = 0)
 {
-    for (int l = 0; l < c->mg_levels; l++) {
+    for (int l = from_level; l < c->mg_levels; l++) {
         MgLvl L = mg_lvl(c, l);
         k_mg_reset_zero<double><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(L, l > 0);
         c->launches++;
@@ -1180,18 +1203,24 @@ static void update_sol(bcg_ctx* c, const MgConst& m, int l)
     k_mg_update_sol<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, l);
     c->launches++;
 }
-static void update_res(bcg_ctx* c, const MgConst& m, int l)
+static void update_res(bcg_ctx* c, const MgConst& m, int l, bool setup_clean = false)
 {
     MgLvl L = mg_lvl(c, l), Lp = mg_lvl(c, l > 0 ? l - 1 : 0);
-    k_mg_update_res<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    if (setup_clean) k_mg_update_res<true><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    else k_mg_update_res<false><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lp, l, c->inside);
     c->launches++;
 }
 
 /* setup(), Multigrid.cpp:818-825 */
 void mg_setup(bcg_ctx* c, const MgConst& m)
 {
-    if (!c->mg_clean) reset_zero(c);
-    c->mg_clean = 0;
+    if (c->mg_clean) {
+        /* resetZero and updateSolAga have nothing to do but the clamp */
+        c->mg_clean = 0;
+        for (int l = 0; l <= m.A - 1; l++) update_res(c, m, l, true);
+        return;
+    }
+    reset_zero(c);
     for (int l = 0; l <= m.A - 1; l++) update_sol(c, m, l);
     for (int l = 0; l <= m.A - 1; l++) update_res(c, m, l);
 }
@@ -1209,7 +1238,8 @@ void mg_reset(bcg_ctx* c, const MgConst& m)
     /* the reference recomputes Res on every composite level here, and the
      * resetZero below clears it again on levels > 0: only level 0's stays */
     update_res(c, m, 0);
-    reset_zero(c);
+    /* updateSolAga already zeroed Err and Res on the composite levels */
+    reset_zero(c, m.A);
     for (int l = 1; l < m.A; l++) {
         MgLvl L = mg_lvl(c, l), Lf = mg_lvl(c, l - 1);
         k_mg_nest<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lf, l);
