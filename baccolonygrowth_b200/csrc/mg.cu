@@ -569,11 +569,52 @@ __device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T 
  * swap roles every step (the loop runs two steps per trip), and R and the
  * input rows are re-read through L1, prefetched SMOOTH_PF rows ahead. */
 #define RELAX_WARM_F 40
-#define SMOOTH_PF 8
+#define SMOOTH_PF 8         /* rows staged ahead of the row step */
+#define SMOOTH_RING 16      /* ring slots per array; > SMOOTH_PF + 2S for every S used */
+#define SMOOTH_WARPS 4      /* warps per block */
 struct SmoothArgs {
     int nx, nz, pitch, l, sp, ce, co, kind_e, kind_o, kw, ks, ke;
     bool ld_ok, st_e, st_o, plain_cols;
 };
+
+/* Row staging: each lane copies its own column pair of E and R row k into
+ * a per-warp ring in shared memory (cp.async, zero-filled off the grid)
+ * and later reads back only what it copied itself, so the lane's own
+ * cp.async.wait_group is the only ordering needed. */
+template <class T>
+__device__ __forceinline__ void ring_issue(typename Pair2<T>::type* ring, const T* E, const T* R,
+                                           const SmoothArgs& g, int k)
+{
+    typedef typename Pair2<T>::type T2;
+    const bool ok = g.ld_ok && k >= 0 && k <= g.nz;
+    const size_t off = ok ? (size_t)k * g.pitch + g.ce : 0;
+    T2* se = ring + (k & (SMOOTH_RING - 1)) * 32 + (threadIdx.x & 31);
+    T2* sr = se + SMOOTH_RING * 32;
+    const unsigned de = (unsigned)__cvta_generic_to_shared(se), dr = (unsigned)__cvta_generic_to_shared(sr);
+    const int n = ok ? (int)sizeof(T2) : 0;
+    if (sizeof(T2) == 16) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(de), "l"(E + off), "r"(n));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dr), "l"(R + off), "r"(n));
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(de), "l"(E + off), "r"(n));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(dr), "l"(R + off), "r"(n));
+    }
+    asm volatile("cp.async.commit_group;");
+}
+template <class T>
+__device__ __forceinline__ typename Pair2<T>::type ring_e(const typename Pair2<T>::type* ring, const SmoothArgs& g, int k)
+{
+    typename Pair2<T>::type v; v.x = T(0); v.y = T(0);
+    if (k >= 0 && k <= g.nz) v = ring[(k & (SMOOTH_RING - 1)) * 32 + (threadIdx.x & 31)];
+    return v;
+}
+template <class T>
+__device__ __forceinline__ typename Pair2<T>::type ring_r(const typename Pair2<T>::type* ring, const SmoothArgs& g, int k)
+{
+    typename Pair2<T>::type v; v.x = T(0); v.y = T(0);
+    if (k >= 0 && k <= g.nz) v = ring[SMOOTH_RING * 32 + (k & (SMOOTH_RING - 1)) * 32 + (threadIdx.x & 31)];
+    return v;
+}
 
 template <class T>
 __device__ __forceinline__ typename Pair2<T>::type ld_pair(const T* a, const SmoothArgs& g, int k)
@@ -588,19 +629,17 @@ __device__ __forceinline__ typename Pair2<T>::type ld_pair(const T* a, const Smo
 template <class T, int S>
 __device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T (&h2)[2 * S],
                                             const T* __restrict__ E, const T* __restrict__ R, T* __restrict__ EO,
+                                            typename Pair2<T>::type* ring,
                                             const MgConst& m, const RelaxK<T>& K, const SmoothArgs& g,
                                             const double* __restrict__ inside0)
 {
     typedef typename Pair2<T>::type T2;
     constexpr int H = 2 * S;
-    if (g.ld_ok) {
-        const int kp = r + 1 + SMOOTH_PF;
-        if (kp <= g.nz) {
-            asm volatile("prefetch.global.L1 [%0];" :: "l"(E + (size_t)kp * g.pitch + g.ce));
-            asm volatile("prefetch.global.L1 [%0];" :: "l"(R + (size_t)(kp - 1) * g.pitch + g.ce));
-        }
-    }
-    const T2 inm = ld_pair(E, g, r - 1), in0 = ld_pair(E, g, r), inp = ld_pair(E, g, r + 1);
+    static_assert(SMOOTH_RING > SMOOTH_PF + H, "ring slot reused before its last read");
+    /* stage row r+1+PF; rows up to r+1 are then complete */
+    ring_issue<T>(ring, E, R, g, r + 1 + SMOOTH_PF);
+    asm volatile("cp.async.wait_group %0;" :: "n"(SMOOTH_PF));
+    const T2 inm = ring_e<T>(ring, g, r - 1), in0 = ring_e<T>(ring, g, r), inp = ring_e<T>(ring, g, r + 1);
     T nb[H];
 #pragma unroll
     for (int h = 0; h < H; h++) {
@@ -618,7 +657,7 @@ __device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T
             const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
             const T own_other = (h == 0) ? in0.y : h1[h - 1];
             (void)old;
-            const T2 rk = ld_pair(R, g, r - h);
+            const T2 rk = ring_r<T>(ring, g, r - h);
             h2[h] = odd ? rx_in(rk.y, h1[h], up, own_other, nb[h], K) : rx_in(rk.x, h1[h], up, nb[h], own_other, K);
         }
     } else {
@@ -633,7 +672,7 @@ __device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T
             const T own_other = (h == 0) ? in0.y : h1[h - 1];
             const T xm = odd ? own_other : nb[h];
             const T xp = odd ? nb[h] : own_other;
-            const T2 rk = ld_pair(R, g, k);
+            const T2 rk = ring_r<T>(ring, g, k);
             const T rv = odd ? rk.y : rk.x;
             if (k > 0 && k < g.nz)
                 h2[h] = rx_row<T>(odd ? g.kind_o : g.kind_e, rv, h1[h], up, xm, xp, old, K);
@@ -651,7 +690,7 @@ __device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T
 }
 
 template <class T, int S>
-__global__ void __launch_bounds__(128) k_mg_smooth(MgConst m, MgLvlT<T> L, int l, int seg_len,
+__global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLvlT<T> L, int l, int seg_len,
                                                    const double* __restrict__ inside0)
 {
     constexpr int H = 2 * S;
@@ -683,17 +722,21 @@ __global__ void __launch_bounds__(128) k_mg_smooth(MgConst m, MgLvlT<T> L, int l
      * lane reads; only real side columns need the per-lane path */
     const bool side_e = (g.ce == 0 || g.ce == g.nx), side_o = (g.co == 0 || g.co == g.nx);
     g.plain_cols = !__any_sync(0xffffffffu, side_e || side_o);
+    extern __shared__ __align__(16) unsigned char smooth_smem[];
+    typename Pair2<T>::type* ring = reinterpret_cast<typename Pair2<T>::type*>(smooth_smem) + threadIdx.y * (2 * SMOOTH_RING * 32);
     T a[H], b[H];
     {
         const typename Pair2<T>::type e0 = ld_pair(E, g, g.kw - 1);
 #pragma unroll
         for (int h = 0; h < H; h++) { a[h] = (h & 1) ? e0.y : e0.x; b[h] = a[h]; }
     }
+    for (int k = g.kw - 1; k <= g.kw + SMOOTH_PF; k++) ring_issue<T>(ring, E, R, g, k);
     const int r_end = g.ke - 1 + (H - 1);
     for (int r = g.kw; r <= r_end; r += 2) {
-        smooth_step<T, S>(r, a, b, E, R, EO, m, K, g, inside0);
-        if (r + 1 <= r_end) smooth_step<T, S>(r + 1, b, a, E, R, EO, m, K, g, inside0);
+        smooth_step<T, S>(r, a, b, E, R, EO, ring, m, K, g, inside0);
+        if (r + 1 <= r_end) smooth_step<T, S>(r + 1, b, a, E, R, EO, ring, m, K, g, inside0);
     }
+    asm volatile("cp.async.wait_group 0;");
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1080,10 +1123,11 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         if (nseg > max_seg) nseg = max_seg;
         if (nseg < 1) nseg = 1;
         const int seg_len = (rows + nseg - 1) / nseg;
-        dim3 block(32, 4), grid((unsigned)((nwx + 3) / 4), (unsigned)nseg, 3);
-        if (S == 3) k_mg_smooth<T, 3><<<grid, block, 0, c->stream>>>(m, L, l, seg_len, c->inside);
-        else if (S == 2) k_mg_smooth<T, 2><<<grid, block, 0, c->stream>>>(m, L, l, seg_len, c->inside);
-        else k_mg_smooth<T, 1><<<grid, block, 0, c->stream>>>(m, L, l, seg_len, c->inside);
+        dim3 block(32, SMOOTH_WARPS), grid((unsigned)((nwx + SMOOTH_WARPS - 1) / SMOOTH_WARPS), (unsigned)nseg, 3);
+        const size_t smem = (size_t)SMOOTH_WARPS * 2 * SMOOTH_RING * 32 * 2 * sizeof(T);
+        if (S == 3) k_mg_smooth<T, 3><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, c->inside);
+        else if (S == 2) k_mg_smooth<T, 2><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, c->inside);
+        else k_mg_smooth<T, 1><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, c->inside);
         c->launches++;
         swap_err<T>(c, l);
         sweeps -= S;
@@ -1099,6 +1143,14 @@ int mg_kernel_attributes()
         cudaFuncSetAttribute(k_mg_coarse_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_coarse_wave<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_coarse_wave<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+        return BCG_E_CUDA;
+    const int sm_d = SMOOTH_WARPS * 2 * SMOOTH_RING * 32 * 16, sm_f = sm_d / 2;
+    if (cudaFuncSetAttribute(k_mg_smooth<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_d) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_d) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_d) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_f) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_f) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_f) != cudaSuccess)
         return BCG_E_CUDA;
     done = true;
     return BCG_OK;
