@@ -197,6 +197,11 @@ PROTOTYPES = {
     "bcg_mg_solve_tol": (_I, [_VP, _D, _I, _I, _PI, _PD]),
     "bcg_autotune": (_I, [_VP, _I, _PI]),
     "bcg_set_pair_precision": (_I, [_VP, _I]),
+    "bcg_steady_create": (_I, [_VP, _VP]),
+    "bcg_steady_destroy": (_I, [_VP]),
+    "bcg_steady_set_cells": (_I, [_VP, _PD, _I]),
+    "bcg_steady_solve": (_I, [_VP, _PD, _PD, _D, _PD, _PI, _PI]),
+    "bcg_steady_vjp": (_I, [_VP, _PD, _PD, _PD, _D]),
     "bcg_enable_timers": (_I, [_VP, _I]),
     "bcg_get_timer": (_I, [_VP, _I, _PD, _PI64]),
     "bcg_rng_seed": (None, [ctypes.POINTER(Rng), ctypes.c_uint32]),

@@ -318,6 +318,39 @@ typedef enum bcg_tune_id { BCG_TUNE_FORCE_GROUP = 1, BCG_TUNE_SMOOTHER = 2 } bcg
 int bcg_autotune(bcg_ctx* ctx, int what, int* choice);
 
 /* ------------------------------------------------------------------ */
+/* steady glucose field and its adjoint (no reference counterpart)       */
+/* ------------------------------------------------------------------ */
+/* A 2-D x-z grid of nx x nz vertices (nx, nz of the form 2^a + 1) at
+ * spacing h: rows k < nz_agar are agar, the rest the colony region; row 0
+ * is held at c0.  With theta = {d_agar, d_colony, vmax, km} the steady
+ * field C solves, at every other vertex,
+ *   sum_faces Df (C_nb - C) / h^2 = q vmax C / (km + C),
+ * Df the harmonic mean of the two vertices' diffusivities, no flux through
+ * the sides and top, q the uptake density: the sum of w_c L_c R_c / h^2
+ * over the cells whose centre rounds to the vertex (the deposition of
+ * GetDensity, Compute.cpp:120-253, weighted per cell). */
+typedef struct bcg_steady_params {
+    int nx, nz, nz_agar, max_cells;
+    double h, c0;
+} bcg_steady_params;
+typedef struct bcg_steady bcg_steady;
+int bcg_steady_create(const bcg_steady_params* p, bcg_steady** out);
+int bcg_steady_destroy(bcg_steady* s);
+/* cells as 4 doubles each: centre x (from the grid's left edge), centre z
+ * (from the agar bottom), length L, radius R; at most max_cells */
+int bcg_steady_set_cells(bcg_steady* s, const double* xzlr, int ncell);
+/* Newton to max|F| <= tol * (max|F| at C = c0); C_out (nx*nz, row k at
+ * offset k*nx, optional) receives the field.  The converged state is kept
+ * for bcg_steady_vjp. */
+int bcg_steady_solve(bcg_steady* s, const double* theta, const double* w, double tol,
+                     double* C_out, int* newton_iters, int* cg_iters);
+/* Vector-Jacobian product at the last solve: given dL/dC (nx*nz), the
+ * gradients dL/dtheta (4) and dL/dw (per cell, optional).  Exact for the
+ * converged field: one adjoint solve A lambda = -dL/dC with the symmetric
+ * Newton operator, to max|residual| <= tol * max|dL/dC|. */
+int bcg_steady_vjp(bcg_steady* s, const double* dL_dC, double* grad_theta, double* grad_w, double tol);
+
+/* ------------------------------------------------------------------ */
 /* timing: device time of the kernels queued by the last call of each    */
 /* kind (CUDA events on the context stream), in milliseconds.            */
 /* ------------------------------------------------------------------ */
