@@ -227,6 +227,7 @@ EXTRA_PROTOTYPES = {
     "bcg_kernel_launches": (ctypes.c_longlong, [_VP]),
     "bcg_set_bbox": (_I, [_VP, _I, _I, _I]),
     "bcg_set_relax_mode": (_I, [_I]),
+    "bcg_set_smoother_warps": (_I, [_VP, _I]),
 }
 
 TUNE = dict(FORCE_GROUP=1, SMOOTHER=2)

@@ -445,7 +445,8 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
     T* Rs = Es + np;
     T* E = SP(L.e);
     const T* R = SP(L.r);
-    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+    const int nth = blockDim.x * blockDim.y, th = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int q = th; q < np; q += nth) {
         int i = q % W, k = q / W;
         Es[q] = AT(E, L, i, k);
         Rs[q] = AT(R, L, i, k);
@@ -454,22 +455,22 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
     const RelaxK<T> K = relax_k<T>(m, l, sp);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
+    /* threadIdx.x: column of the parity, threadIdx.y: one of the active sweeps */
     const int steps = nz + 1 + 2 * (sweeps - 1);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     for (int t = 0; t < steps; t++) {
         const int s_lo = t > nz ? (t - nz + 1) / 2 : 0;
         const int s_hi = min(sweeps - 1, t / 2);
-        const int na = s_hi - s_lo + 1;
         for (int parity = 0; parity < 2; parity++) {
             const int ncol = (W - parity + 1) / 2;
-            for (int q = threadIdx.x; q < na * ncol; q += blockDim.x) {
-                const int sw = s_lo + q / ncol;
-                const int i = 2 * (q % ncol) + parity;
-                relax_smem<T>(m, K, l, oxy, top_levels, nx, nz, i, t - 2 * sw, Es, Rs, inside0);
-            }
+            for (int c = threadIdx.x; c < ncol; c += blockDim.x)
+                for (int sw = s_lo + threadIdx.y; sw <= s_hi; sw += blockDim.y)
+                    relax_smem<T>(m, K, l, oxy, top_levels, nx, nz, 2 * c + parity, t - 2 * sw, Es, Rs, inside0);
             __syncthreads();
         }
     }
-    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+    (void)tid;
+    for (int q = th; q < np; q += nth) {
         int i = q % W, k = q / W;
         AT(E, L, i, k) = Es[q];
     }
@@ -1119,7 +1120,7 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         const int nwx = (L.nx + 1 + 2 * outp - 1) / (2 * outp);
         const int target = c->smooth_warps > 0 ? c->smooth_warps : g_smooth_warps;
         int nseg = (target + 3 * nwx - 1) / (3 * nwx);
-        const int max_seg = rows / 64 > 1 ? rows / 64 : 1;
+        const int max_seg = rows / 32 > 1 ? rows / 32 : 1;
         if (nseg > max_seg) nseg = max_seg;
         if (nseg < 1) nseg = 1;
         const int seg_len = (rows + nseg - 1) / nseg;
@@ -1135,6 +1136,16 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 }
 
 /* kernel attributes set once per process, outside any stream capture */
+/* pin the smoother's resident-warp target for a context (0 = the default
+ * or the tuned value); used to profile a fixed kernel shape */
+extern "C" int bcg_set_smoother_warps(bcg_ctx* c, int warps)
+{
+    if (!c || warps < 0) return BCG_E_ARG;
+    c->smooth_warps = warps;
+    nutrient_graphs_drop(c);
+    return BCG_OK;
+}
+
 int mg_kernel_attributes()
 {
     static bool done = false;
@@ -1164,14 +1175,14 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     const int rows = c->mg[0].nz + 1;
     if (g_relax_mode != 2 || rows <= 96) { if (choice) *choice = 0; return BCG_OK; }
     MgConst m = mg_const(c, c->P.mg_dt);
-    const int targets[5] = {350, 700, 1400, 2800, 5600};
+    const int targets[6] = {700, 1400, 2800, 5600, 8400, 11200};
     const int saved = c->smooth_warps;
     cudaEvent_t a, b;
     BCG_CUDA_TRY(cudaEventCreate(&a));
     BCG_CUDA_TRY(cudaEventCreate(&b));
     float best = 3.4e38f;
     int best_t = saved > 0 ? saved : g_smooth_warps;
-    for (int ti = 0; ti < 5; ti++) {
+    for (int ti = 0; ti < 6; ti++) {
         c->smooth_warps = targets[ti];
         smooth_level<double>(c, m, 0, 3);                  /* warm-up */
         smooth_level<double>(c, m, 0, 3);
@@ -1201,7 +1212,15 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
     MgLvlT<T> L = lvl<T>(c, l);
     const size_t smem = 2 * sizeof(T) * (size_t)(L.nx + 1) * (L.nz + 1);
     if (g_relax_mode >= 1 && smem <= 200 * 1024 && L.nz >= 1) {
-        k_mg_coarse_wave<T><<<3, 1024, smem, c->stream>>>(m, L, l, sweeps, c->inside);
+        /* columns of one parity across x, the active sweeps (at most about
+         * nz/2 + 1 at a time) across y */
+        int cx = ((L.nx + 2) / 2 + 31) / 32 * 32;
+        if (cx > 1024) cx = 1024;
+        int cy = L.nz / 2 + 1;
+        if (cy > sweeps) cy = sweeps;
+        if (cy * cx > 1024) cy = 1024 / cx;
+        if (cy < 1) cy = 1;
+        k_mg_coarse_wave<T><<<3, dim3(cx, cy), smem, c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
     } else if (g_relax_mode >= 1 && smem <= 200 * 1024) {
         int ncol = (L.nx + 2) / 2;

@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mg-tol", action="store_true")
+    ap.add_argument("--smoother-warps", type=int, default=0,
+                    help="pin the agar smoother's resident-warp target instead of autotuning it (profiling)")
     return ap.parse_args()
 
 
@@ -265,6 +267,10 @@ def b200_arm(args):
         _abi.check(lib.bcg_rebuild_neighbours(ctx), "rebuild")
         tuned = {}
         for name in ("FORCE_GROUP", "SMOOTHER"):
+            if name == "SMOOTHER" and args.smoother_warps > 0:
+                _abi.check(lib.bcg_set_smoother_warps(ctx, args.smoother_warps), "set smoother warps")
+                tuned["smoother"] = args.smoother_warps
+                continue
             ch = ctypes.c_int()
             _abi.check(lib.bcg_autotune(ctx, _abi.TUNE[name], ctypes.byref(ch)), "autotune " + name)
             tuned[name.lower()] = ch.value
@@ -316,6 +322,8 @@ def b200_arm(args):
     _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(hostbuf), 0, 12345 + rank, 0, ctypes.byref(sim2)), "sim2")
     _abi.check(lib.bcg_sim_set_step_mode(sim2, 0, args.vcycles), "mode2")
     ctx2 = lib.bcg_sim_ctx(sim2)
+    if args.smoother_warps > 0:
+        _abi.check(lib.bcg_set_smoother_warps(ctx2, args.smoother_warps), "set smoother warps")
     g = np.full(p.box_x * p.box_z, 0.9)
     lib.bcg_set_field(ctx2, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size)
     out_pinned = torch.empty((n0 + n0 // 4) * 208, dtype=torch.uint8, pin_memory=True)

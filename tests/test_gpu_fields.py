@@ -228,7 +228,7 @@ def test_smoother_autotune_same_solution(gpu):
     for tune in (False, True):
         col = Colony(p, cells); col.update_density(); col.deplete_wall()
         if tune:
-            assert col.autotune("SMOOTHER") in (350, 700, 1400, 2800, 5600)
+            assert col.autotune("SMOOTHER") in (700, 1400, 2800, 5600, 8400, 11200)
             col.update_density(); col.deplete_wall()
         col.mg_solve(3)
         out.append(_solve_state(col, p))
