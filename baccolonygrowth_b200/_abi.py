@@ -197,6 +197,9 @@ PROTOTYPES = {
     "bcg_mg_solve_tol": (_I, [_VP, _D, _I, _I, _PI, _PD]),
     "bcg_autotune": (_I, [_VP, _I, _PI]),
     "bcg_set_pair_precision": (_I, [_VP, _I]),
+    "bcg_ensemble_create": (_I, [_VP, _I, _VP]),
+    "bcg_ensemble_run": (_I, [_VP, _I]),
+    "bcg_ensemble_destroy": (_I, [_VP]),
     "bcg_steady_create": (_I, [_VP, _VP]),
     "bcg_steady_destroy": (_I, [_VP]),
     "bcg_steady_set_cells": (_I, [_VP, _PD, _I]),

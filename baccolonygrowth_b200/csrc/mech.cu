@@ -7,6 +7,7 @@
  */
 #include "ctx.cuh"
 #include "cellmath.cuh"
+#include "internal.h"
 #include <string.h>
 #include <mutex>
 
@@ -435,6 +436,29 @@ int launch_move_grow(bcg_ctx* c, double dt, int group)
     return BCG_OK;
 }
 
+/* split halves of bcg_move_grow (used by the ensemble runner to overlap
+ * colonies): the launch queues the kernel and the two counter reads, the
+ * finish waits for them */
+int move_grow_launch(bcg_ctx* c, double dt)
+{
+    int rc = launch_move_grow(c, dt, c->force_group ? c->force_group : g_group);
+    if (rc) return rc;
+    int* hp = (int*)c->pinned;
+    BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->div_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    BCG_CUDA_TRY(cudaMemcpyAsync(hp + 2, c->fcw_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    return BCG_OK;
+}
+int move_grow_finish(bcg_ctx* c, int* n_div, int64_t* fcw_calls)
+{
+    int rc = ctx_check_status(c);
+    if (rc) return rc;
+    int* hp = (int*)c->pinned;
+    c->last_ndiv = hp[0];
+    if (n_div) *n_div = hp[0];
+    if (fcw_calls) *fcw_calls = (int64_t)(*(unsigned long long*)(hp + 2));
+    return BCG_OK;
+}
+
 extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_calls)
 {
     if (!c) return BCG_E_ARG;
@@ -446,12 +470,7 @@ extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_cal
     int* hp = (int*)c->pinned;
     BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->div_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     BCG_CUDA_TRY(cudaMemcpyAsync(hp + 2, c->fcw_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
-    rc = ctx_check_status(c);
-    if (rc) return rc;
-    c->last_ndiv = hp[0];
-    if (n_div) *n_div = hp[0];
-    if (fcw_calls) *fcw_calls = (int64_t)(*(unsigned long long*)(hp + 2));
-    return BCG_OK;
+    return move_grow_finish(c, n_div, fcw_calls);
 }
 
 /* time `reps` launches of MoveCell+GrowCell with `group` lanes per cell;
@@ -758,52 +777,64 @@ extern "C" int bcg_get_dividing(bcg_ctx* c, int* ids, int capacity)
     return BCG_OK;
 }
 
-extern "C" int bcg_divide(bcg_ctx* c, const float* draws, int n_draw_sets, double t, int* n_done, int* lineage)
+/* split halves of bcg_divide: the launch queues the binning, the draw
+ * upload, the two division kernels and the read of the counts; the
+ * finish waits, copies the lineage and advances the context */
+int divide_launch(bcg_ctx* c, const float* draws, int n_draw_sets, double t)
 {
-    if (!c) return BCG_E_ARG;
     if (n_draw_sets != c->last_ndiv) return BCG_E_ARG;
-    timer_begin(c, BCG_T_DIVIDE);
-    int done = 0;
-    int ndiv = c->last_ndiv;
+    const int ndiv = c->last_ndiv;
     if (ndiv > DIV_SORT_MAX) return BCG_E_UNSUPPORTED;
+    if (ndiv == 0) return BCG_OK;
+    if (!draws) return BCG_E_ARG;
+    int nb = c->cur ^ 1;
+    int rc = bin_cells(c, nb);
+    if (rc) return rc;
+    size_t db = sizeof(float) * 9 * (size_t)ndiv;
+    rc = ensure_pinned(c, db + 64);
+    if (rc) return rc;
+    memcpy(c->pinned, draws, db);
+    BCG_CUDA_TRY(cudaMemcpyAsync(c->draws_dev, c->pinned, db, cudaMemcpyHostToDevice, c->stream));
+    MechParams mp = mech_params(c);
+    k_div_plan<<<1, 1024, 0, c->stream>>>(c->n, ndiv, c->cap, t, c->draws_dev, c->rec[nb], c->soa, mp,
+        c->div_list, c->cell_box, c->nbr, c->ncount, c->div_rec, c->div_box, c->div_rect, c->div_pairs,
+        c->div_par, c->div_order, c->div_grp, c->lineage, c->n_done_dev, c->status);
+    k_div_groups<<<(ndiv + 3) / 4, 128, 0, c->stream>>>(c->n, c->n_done_dev, c->div_grp, c->div_order,
+        c->lineage, c->div_rec, c->div_box, c->rec[nb], mp, c->nbr, c->ncount, c->box_start, c->box_ids,
+        c->moved, c->delta_ids, c->delta_box, c->status);
+    c->launches += 2;
+    BCG_CUDA_TRY(cudaGetLastError());
+    int* hp = (int*)c->pinned;
+    BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->n_done_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    return BCG_OK;
+}
+int divide_finish(bcg_ctx* c, int* n_done, int* lineage)
+{
+    const int ndiv = c->last_ndiv;
+    int done = 0, rc = BCG_OK;
     if (ndiv > 0) {
-        if (!draws) return BCG_E_ARG;
-        int nb = c->cur ^ 1;
-        int rc = bin_cells(c, nb);
-        if (rc) return rc;
-        size_t db = sizeof(float) * 9 * (size_t)ndiv;
-        rc = ensure_pinned(c, db + 64);
-        if (rc) return rc;
-        memcpy(c->pinned, draws, db);
-        BCG_CUDA_TRY(cudaMemcpyAsync(c->draws_dev, c->pinned, db, cudaMemcpyHostToDevice, c->stream));
-        MechParams mp = mech_params(c);
-        k_div_plan<<<1, 1024, 0, c->stream>>>(c->n, ndiv, c->cap, t, c->draws_dev, c->rec[nb], c->soa, mp,
-            c->div_list, c->cell_box, c->nbr, c->ncount, c->div_rec, c->div_box, c->div_rect, c->div_pairs,
-            c->div_par, c->div_order, c->div_grp, c->lineage, c->n_done_dev, c->status);
-        k_div_groups<<<(ndiv + 3) / 4, 128, 0, c->stream>>>(c->n, c->n_done_dev, c->div_grp, c->div_order,
-            c->lineage, c->div_rec, c->div_box, c->rec[nb], mp, c->nbr, c->ncount, c->box_start, c->box_ids,
-            c->moved, c->delta_ids, c->delta_box, c->status);
-        c->launches += 2;
-        BCG_CUDA_TRY(cudaGetLastError());
-        int* hp = (int*)c->pinned;
-        BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->n_done_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         rc = ctx_check_status(c);
-        done = hp[0];
-        if (lineage && done > 0) {
+        done = ((int*)c->pinned)[0];
+        if (lineage && done > 0)
             BCG_CUDA_TRY(cudaMemcpy(lineage, c->lineage, sizeof(int) * 2 * (size_t)done, cudaMemcpyDeviceToHost));
-        }
         c->n += done;
-        c->cur ^= 1;
-        c->last_ndiv = 0;
-        timer_end(c, BCG_T_DIVIDE, 7);
-        if (n_done) *n_done = done;
-        return rc;
     }
     c->cur ^= 1;
     c->last_ndiv = 0;
-    timer_end(c, BCG_T_DIVIDE, 0);
-    if (n_done) *n_done = 0;
-    return BCG_OK;
+    if (n_done) *n_done = done;
+    return rc;
+}
+
+extern "C" int bcg_divide(bcg_ctx* c, const float* draws, int n_draw_sets, double t, int* n_done, int* lineage)
+{
+    if (!c) return BCG_E_ARG;
+    timer_begin(c, BCG_T_DIVIDE);
+    const int ndiv = c->last_ndiv;
+    int rc = divide_launch(c, draws, n_draw_sets, t);
+    if (rc) return rc;
+    rc = divide_finish(c, n_done, lineage);
+    timer_end(c, BCG_T_DIVIDE, ndiv > 0 ? 7 : 0);
+    return rc;
 }
 
 /* ======================================================================= */
@@ -952,4 +983,9 @@ extern "C" int bcg_mean_stress_noalloc(bcg_ctx* c, double* stress, double* fnet,
     if (fcw_calls) *fcw_calls = (int64_t)h;
     return rc;
 }
+
+extern "C" int bcg_int_move_grow_launch(bcg_ctx* c, double dt) { return c ? move_grow_launch(c, dt) : BCG_E_ARG; }
+extern "C" int bcg_int_move_grow_finish(bcg_ctx* c, int* n_div, int64_t* fcw) { return c ? move_grow_finish(c, n_div, fcw) : BCG_E_ARG; }
+extern "C" int bcg_int_divide_launch(bcg_ctx* c, const float* draws, int n, double t) { return c ? divide_launch(c, draws, n, t) : BCG_E_ARG; }
+extern "C" int bcg_int_divide_finish(bcg_ctx* c, int* done, int* lineage) { return c ? divide_finish(c, done, lineage) : BCG_E_ARG; }
 

@@ -12,6 +12,7 @@
  */
 #include "ctx.cuh"
 #include "mg.cuh"
+#include "internal.h"
 #include <string.h>
 
 __device__ __forceinline__ double dmaxd(double a, double b) { return a > b ? a : b; }
@@ -1512,3 +1513,11 @@ extern "C" int bcg_mg_solve_tol(bcg_ctx* c, double rel_tol, int precision, int m
     if (rel_res) *rel_res = rel;
     return ctx_check_status(c);
 }
+
+extern "C" int bcg_int_mg_solve_launch(bcg_ctx* c, int vcycles)
+{
+    if (!c) return BCG_E_ARG;
+    if (vcycles <= 0) vcycles = c->P.mg_vcycles;
+    return mg_solve_impl(c, vcycles, 0);
+}
+

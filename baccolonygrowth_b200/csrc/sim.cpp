@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/bcg.h"
+#include "internal.h"
 
 struct bcg_sim {
     bcg_params P;
@@ -89,6 +90,31 @@ extern "C" int bcg_sim_set_step_mode(bcg_sim* s, int field_cadence_reference, in
     return BCG_OK;
 }
 
+/* end of a step: lineage, time and the three flags (Simulation.cpp:418-426) */
+static int sim_advance(bcg_sim* s, size_t base, int done, int rc)
+{
+    s->lineage.resize(base + 2 * (size_t)done);
+    s->divisions += done;
+    if (rc) return rc;
+    s->t += s->dt;
+    bool out = (s->next_out <= 0);
+    s->next_out = (out ? s->P.output_time : s->next_out) - s->dt;
+    s->update_flag = (s->next_update <= 0);
+    s->next_update = (s->update_flag ? s->P.update_time : s->next_update) - s->dt;
+    s->hd_update_flag = (s->hd_next_update <= 0);
+    s->hd_next_update = (s->hd_update_flag ? s->hd_update_time : s->hd_next_update) - s->dt;
+    return BCG_OK;
+}
+
+/* the host's share of a step between MoveCell and the division loop:
+ * skip the F_cw draws, draw the division floats */
+static void sim_draws(bcg_sim* s, int nd, int64_t calls)
+{
+    bcg_rng_skip(&s->rng, calls);
+    s->draws.resize((size_t)9 * (nd > 0 ? nd : 1));
+    for (int i = 0; i < 9 * nd; i++) s->draws[i] = frand(&s->rng);
+}
+
 /* One iteration of while (t <= t_max), Simulation.cpp:254-431, without the
  * output block. */
 static int sim_step(bcg_sim* s)
@@ -118,24 +144,12 @@ static int sim_step(bcg_sim* s)
     int nd = 0;
     int64_t calls = 0;
     if ((rc = bcg_move_grow(s->ctx, s->dt, &nd, &calls))) return rc;
-    bcg_rng_skip(&s->rng, calls);
-    s->draws.resize((size_t)9 * (nd > 0 ? nd : 1));
-    for (int i = 0; i < 9 * nd; i++) s->draws[i] = frand(&s->rng);
+    sim_draws(s, nd, calls);
     size_t base = s->lineage.size();
     s->lineage.resize(base + 2 * (size_t)(nd > 0 ? nd : 0));
     int done = 0;
     rc = bcg_divide(s->ctx, s->draws.data(), nd, s->t, &done, nd > 0 ? s->lineage.data() + base : nullptr);
-    s->lineage.resize(base + 2 * (size_t)done);
-    s->divisions += done;
-    if (rc) return rc;
-    s->t += s->dt;
-    bool out = (s->next_out <= 0);
-    s->next_out = (out ? s->P.output_time : s->next_out) - s->dt;
-    s->update_flag = (s->next_update <= 0);
-    s->next_update = (s->update_flag ? s->P.update_time : s->next_update) - s->dt;
-    s->hd_update_flag = (s->hd_next_update <= 0);
-    s->hd_next_update = (s->hd_update_flag ? s->hd_update_time : s->hd_next_update) - s->dt;
-    return BCG_OK;
+    return sim_advance(s, base, done, rc);
 }
 
 extern "C" int bcg_sim_run(bcg_sim* s, int steps)
@@ -166,3 +180,86 @@ extern "C" int bcg_sim_lineage(bcg_sim* s, int* pairs, int capacity, int* n)
     if (m > 0 && pairs) memcpy(pairs, s->lineage.data(), sizeof(int) * 2 * (size_t)m);
     return BCG_OK;
 }
+
+/* ------------------------------------------------------------------------
+ * Ensembles: independent colonies (bcg_sim members in the benchmark
+ * cadence) stepped together.  Each phase of the step is queued for every
+ * member, on the member's own stream, before any member is waited for:
+ *   neighbour rebuild (when due) + agar solve + MoveCell/GrowCell,
+ *   wait for the counters; host draws,
+ *   division loop, wait.
+ * Colonies of uneven size so overlap on the GPU instead of queueing behind
+ * each other's host round trips.  Every member follows exactly the steps
+ * bcg_sim_run would take for it alone.
+ * ------------------------------------------------------------------------ */
+struct bcg_ensemble {
+    std::vector<bcg_sim*> m;
+    std::vector<int> nd;
+    std::vector<int64_t> calls;
+    std::vector<size_t> base;
+};
+
+extern "C" int bcg_ensemble_create(bcg_sim* const* members, int n, bcg_ensemble** out)
+{
+    if (!out || n < 1 || !members) return BCG_E_ARG;
+    *out = nullptr;
+    for (int i = 0; i < n; i++) {
+        if (!members[i]) return BCG_E_ARG;
+        if (members[i]->reference_cadence) return BCG_E_UNSUPPORTED;
+    }
+    bcg_ensemble* e = new bcg_ensemble();
+    e->m.assign(members, members + n);
+    e->nd.resize(n); e->calls.resize(n); e->base.resize(n);
+    *out = e;
+    return BCG_OK;
+}
+
+extern "C" int bcg_ensemble_destroy(bcg_ensemble* e)
+{
+    delete e;
+    return BCG_OK;
+}
+
+static int ens_step(bcg_ensemble* e)
+{
+    const int n = (int)e->m.size();
+    int rc;
+    for (int i = 0; i < n; i++) {
+        bcg_sim* s = e->m[i];
+        if (s->update_flag || s->first_step) {
+            s->update_flag = false;
+            if ((rc = bcg_rebuild_neighbours(s->ctx))) return rc;
+        }
+        if (s->vcycles_per_step > 0 && (rc = bcg_int_mg_solve_launch(s->ctx, s->vcycles_per_step))) return rc;
+        s->first_step = false;
+        if ((rc = bcg_int_move_grow_launch(s->ctx, s->dt))) return rc;
+    }
+    for (int i = 0; i < n; i++) {
+        bcg_sim* s = e->m[i];
+        if ((rc = bcg_int_move_grow_finish(s->ctx, &e->nd[i], &e->calls[i]))) return rc;
+        sim_draws(s, e->nd[i], e->calls[i]);
+        e->base[i] = s->lineage.size();
+        s->lineage.resize(e->base[i] + 2 * (size_t)(e->nd[i] > 0 ? e->nd[i] : 0));
+        if ((rc = bcg_int_divide_launch(s->ctx, s->draws.data(), e->nd[i], s->t))) return rc;
+    }
+    int first_rc = BCG_OK;
+    for (int i = 0; i < n; i++) {
+        bcg_sim* s = e->m[i];
+        int done = 0;
+        rc = bcg_int_divide_finish(s->ctx, &done, e->nd[i] > 0 ? s->lineage.data() + e->base[i] : nullptr);
+        rc = sim_advance(s, e->base[i], done, rc);
+        if (rc && !first_rc) first_rc = rc;
+    }
+    return first_rc;
+}
+
+extern "C" int bcg_ensemble_run(bcg_ensemble* e, int steps)
+{
+    if (!e || steps < 0) return BCG_E_ARG;
+    for (int k = 0; k < steps; k++) {
+        int rc = ens_step(e);
+        if (rc) return rc;
+    }
+    return BCG_OK;
+}
+

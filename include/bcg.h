@@ -439,6 +439,18 @@ int bcg_sim_lineage(bcg_sim* sim, int* pairs, int capacity, int* n);
  * cadence (0 = mechanics only). */
 int bcg_sim_set_step_mode(bcg_sim* sim, int field_cadence_reference, int vcycles_per_step);
 
+/* Ensembles of independent colonies (no reference counterpart; the
+ * reference runs one colony per process).  `members` are simulations in
+ * the benchmark cadence (bcg_sim_set_step_mode(.., 0, v)), of any sizes
+ * and grids; the ensemble does not own them.  bcg_ensemble_run advances
+ * every member by `steps` steps, each exactly as bcg_sim_run would, with
+ * every phase queued for all members (one stream each) before any member
+ * is waited for.  BCG_E_UNSUPPORTED for a member in the reference cadence. */
+typedef struct bcg_ensemble bcg_ensemble;
+int bcg_ensemble_create(bcg_sim* const* members, int n, bcg_ensemble** out);
+int bcg_ensemble_run(bcg_ensemble* e, int steps);
+int bcg_ensemble_destroy(bcg_ensemble* e);
+
 #ifdef __cplusplus
 }
 #endif
