@@ -155,3 +155,19 @@ def dome_size(n_cells, aspect, phi=0.45, radius=0.5, mean_len=3.0):
     area = n_cells * (2 * radius) * (mean_len + 2 * radius) / phi
     w = math.sqrt(area / (math.pi / 4.0 * aspect))
     return w, w * aspect
+
+
+def ensemble_member(n_cells, aspect=1.0 / 20.0, phi=0.45, max_cells=None):
+    """Params for one colony of an ensemble: the small-simulation physics on
+    a grid sized to the colony's dome (room for the dome, the filter margins
+    and growth; 2 composite agar levels of 64 rows)."""
+    w, h = dome_size(n_cells, aspect, phi)
+    p = finalize(parse_parameters(shipped_input_text("small")))
+    bl = p.box_length
+    p.box_x = max(128, int(math.ceil((w / bl + 24) / 32.0)) * 32)
+    p.box_y = 1
+    p.box_z = max(16, int(math.ceil(h / bl)) + 12)
+    p.box_z_agar, p.max_levels_mg = 64, 2
+    p.max_cells = max_cells if max_cells else int(n_cells * 1.25) + 1024
+    return finalize(p)
+

@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mg-tol", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--smoother-warps", type=int, default=0,
                     help="pin the agar smoother's resident-warp target instead of autotuning it (profiling)")
     return ap.parse_args()
@@ -119,6 +121,79 @@ def set_depleted_wall(lib, ctx, p, rows=None):
     for name, v in zip(("WALLF_CARBON", "WALLF_OXYGEN", "WALLF_ACETATE"), rows):
         _abi.check(lib.bcg_set_field(ctx, _abi.FIELDS[name], 0, _abi.ptr(v, ctypes.c_double), v.size), name)
     return rows
+
+
+def ensemble_bench(lib, args, steps=5, warmup=2):
+    """bcg_ensemble_run over `args.ensemble_members` colonies vs bcg_sim_run
+    on the same members in turn.  Host wall time with the device
+    synchronised on both sides (the members run on their own streams)."""
+    import numpy as np
+    import torch
+    from baccolonygrowth_b200 import _abi, params as _params
+    from baccolonygrowth_b200.colony import synth_colony
+    rng = np.random.default_rng(20261209)
+    sizes = np.exp(rng.uniform(np.log(1000), np.log(100000), args.ensemble_members)).astype(int)
+
+    def build():
+        sims, total = [], 0
+        for j, n in enumerate(sizes):
+            p = _params.ensemble_member(int(n))
+            w, h = _params.dome_size(int(n), 1.0 / 20.0)
+            cells = np.ascontiguousarray(synth_colony(int(n), w, h, seed=7000 + j, div_phase_spread=1.0))
+            sim = ctypes.c_void_p()
+            _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(cells), len(cells), 100 + j, 0, ctypes.byref(sim)), "member")
+            _abi.check(lib.bcg_sim_set_step_mode(sim, 0, args.vcycles), "member mode")
+            ctx = lib.bcg_sim_ctx(sim)
+            g = np.full(p.box_x * p.box_z, 0.9)
+            _abi.check(lib.bcg_set_field(ctx, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size), "g")
+            _abi.check(lib.bcg_update_density(ctx), "density")
+            set_depleted_wall(lib, ctx, p)
+            sims.append(sim)
+            total += len(cells)
+        return sims, total
+
+    def cells_of(sims):
+        tot = 0
+        for s in sims:
+            n = ctypes.c_int()
+            lib.bcg_num_cells(lib.bcg_sim_ctx(s), ctypes.byref(n))
+            tot += n.value
+        return tot
+
+    # together
+    sims, total = build()
+    arr = (ctypes.c_void_p * len(sims))(*[s.value for s in sims])
+    e = ctypes.c_void_p()
+    _abi.check(lib.bcg_ensemble_create(arr, len(sims), ctypes.byref(e)), "ensemble")
+    _abi.check(lib.bcg_ensemble_run(e, warmup), "ensemble warmup")
+    torch.cuda.synchronize()
+    c0 = cells_of(sims)
+    t0 = time.perf_counter()
+    _abi.check(lib.bcg_ensemble_run(e, steps), "ensemble run")
+    torch.cuda.synchronize()
+    t_ens = time.perf_counter() - t0
+    work_ens = 0.5 * (c0 + cells_of(sims)) * steps
+    lib.bcg_ensemble_destroy(e)
+    for s in sims:
+        lib.bcg_sim_destroy(s)
+    # one after another
+    sims, _ = build()
+    for s in sims:
+        _abi.check(lib.bcg_sim_run(s, warmup), "warmup")
+    torch.cuda.synchronize()
+    c0 = cells_of(sims)
+    t0 = time.perf_counter()
+    for s in sims:
+        _abi.check(lib.bcg_sim_run(s, steps), "sequential run")
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    work_seq = 0.5 * (c0 + cells_of(sims)) * steps
+    for s in sims:
+        lib.bcg_sim_destroy(s)
+    return {"members": len(sizes), "cells_total": int(total), "cells_min": int(sizes.min()), "cells_max": int(sizes.max()),
+            "steps": steps, "vcycles_per_step": args.vcycles,
+            "ensemble_cell_steps_per_s": work_ens / t_ens, "sequential_cell_steps_per_s": work_seq / t_seq,
+            "speedup": (work_ens / t_ens) / (work_seq / t_seq), "timing": "host wall clock, device synchronised"}
 
 
 def measured_peaks():
@@ -372,6 +447,12 @@ def b200_arm(args):
                   "speedup": res["fp64"]["ms"] / res["mixed"]["ms"] if res["mixed"]["ms"] > 0 else None,
                   "max_rel_diff_level0": diff, "dof": mg_dof(p)}
 
+    # ensemble of independent colonies (log-uniform 1k-100k cells, each on a
+    # grid sized to it), stepped together vs one after another
+    ens = None
+    if not args.no_ensemble and world == 1:
+        ens = ensemble_bench(lib, args)
+
     # max over ranks (time) and sum over ranks (work); no other collective
     from baccolonygrowth_b200 import replicas
     (ms_max, e2e_max), (work, work_e2e) = replicas.aggregate(
@@ -424,6 +505,7 @@ def b200_arm(args):
                    "l2": "inputs larger than L2 (cell records 2x%d MB + fields)" % (n0 * 128 // 2 ** 20)},
         "mg_dof_per_s": dof * args.vcycles / (mg_ms / 1e3) if mg_ms > 0 else None,
         "mg_tolerance_solve": mg_tol,
+        "ensemble": ens,
         "kernel_ms_per_step": timers,
         "divisions": d_.value,
         "roofline": roof,
