@@ -395,19 +395,16 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_smem(MgConst m, MgLvlT<T> L,
 /* Relaxation of point (i, k) of a level held in shared memory (row k at
  * offset k*(nx+1)), in place; the point code of k_mg_coarse_smem. */
 template <class T>
-__device__ __forceinline__ void relax_smem(const MgConst& m, const RelaxK<T>& K, int l, bool oxy, bool top_levels,
+__device__ __forceinline__ void relax_smem(const RelaxK<T>& K, bool oxy, bool top_levels,
                                            int nx, int nz, int i, int k, T* Es, const T* Rs,
-                                           const double* __restrict__ inside0)
+                                           const unsigned char* ins_row0)
 {
     const int W = nx + 1;
     const bool side = (i == 0 || i == nx);
     const T r = Rs[k * W + i];
     T out = Es[k * W + i];
     if (k == 0) {
-        int d = 1 << l;
-        int i0 = (i - nx / 2) * d + m.box_x / 2;
-        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
-        if (inside0[(size_t)i0 * m.box_z] > 0) out = r;
+        if (ins_row0[i]) out = r;
         else if (side) {
             if (top_levels) out = oxy ? r : rx_corner(r, (i == 0) ? Es[i + 1] : Es[i - 1], at_s(Es, nx, nz, i, 1), K);
         } else out = oxy ? r : rx_k0(r, at_s(Es, nx, nz, i, 1), Es[i - 1], Es[i + 1], K);
@@ -444,33 +441,52 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
     const int np = W * (nz + 1);
     T* Es = reinterpret_cast<T*>(smem_raw);
     T* Rs = Es + np;
+    unsigned char* ins = reinterpret_cast<unsigned char*>(Rs + np);   /* row-0 colony flags per column */
     T* E = SP(L.e);
     const T* R = SP(L.r);
-    const int nth = blockDim.x * blockDim.y, th = threadIdx.y * blockDim.x + threadIdx.x;
+    const int nth = blockDim.x, th = threadIdx.x;
     for (int q = th; q < np; q += nth) {
         int i = q % W, k = q / W;
         Es[q] = AT(E, L, i, k);
         Rs[q] = AT(R, L, i, k);
     }
+    for (int i = th; i < W; i += nth) {
+        int d = 1 << l;
+        int i0 = (i - nx / 2) * d + m.box_x / 2;
+        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+        ins[i] = inside0[(size_t)i0 * m.box_z] > 0;
+    }
     __syncthreads();
     const RelaxK<T> K = relax_k<T>(m, l, sp);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
-    /* threadIdx.x: column of the parity, threadIdx.y: one of the active sweeps */
+    /* work item q of a phase = (active sweep q / ncol, column q % ncol); a
+     * thread's items q = th and th + nth, split once per parity */
+    int a_[2][2], c_[2][2];
+    for (int par = 0; par < 2; par++) {
+        const int ncol = (W - par + 1) / 2;
+        for (int j = 0; j < 2; j++) { int q = th + j * nth; a_[par][j] = q / ncol; c_[par][j] = q % ncol; }
+    }
     const int steps = nz + 1 + 2 * (sweeps - 1);
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     for (int t = 0; t < steps; t++) {
         const int s_lo = t > nz ? (t - nz + 1) / 2 : 0;
         const int s_hi = min(sweeps - 1, t / 2);
-        for (int parity = 0; parity < 2; parity++) {
-            const int ncol = (W - parity + 1) / 2;
-            for (int c = threadIdx.x; c < ncol; c += blockDim.x)
-                for (int sw = s_lo + threadIdx.y; sw <= s_hi; sw += blockDim.y)
-                    relax_smem<T>(m, K, l, oxy, top_levels, nx, nz, 2 * c + parity, t - 2 * sw, Es, Rs, inside0);
+        const int na = s_hi - s_lo + 1;
+#pragma unroll
+        for (int par = 0; par < 2; par++) {
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+                if (a_[par][j] < na)
+                    relax_smem<T>(K, oxy, top_levels, nx, nz, 2 * c_[par][j] + par, t - 2 * (s_lo + a_[par][j]), Es, Rs, ins);
+            /* more active sweeps than two items per thread cover (large levels) */
+            const int ncol = (W - par + 1) / 2;
+            for (int q = th + 2 * nth; q < na * ncol; q += nth) {
+                const int sw = s_lo + q / ncol;
+                relax_smem<T>(K, oxy, top_levels, nx, nz, 2 * (q % ncol) + par, t - 2 * sw, Es, Rs, ins);
+            }
             __syncthreads();
         }
     }
-    (void)tid;
     for (int q = th; q < np; q += nth) {
         int i = q % W, k = q / W;
         AT(E, L, i, k) = Es[q];
@@ -641,28 +657,36 @@ __device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T
     /* stage row r+1+PF; rows up to r+1 are then complete */
     ring_issue<T>(ring, E, R, g, r + 1 + SMOOTH_PF);
     asm volatile("cp.async.wait_group %0;" :: "n"(SMOOTH_PF));
-    const T2 inm = ring_e<T>(ring, g, r - 1), in0 = ring_e<T>(ring, g, r), inp = ring_e<T>(ring, g, r + 1);
-    T nb[H];
-#pragma unroll
-    for (int h = 0; h < H; h++) {
-        const T src = (h == 0) ? in0.y : h1[h - 1];
-        nb[h] = (h & 1) ? __shfl_down_sync(0xffffffffu, src, 1) : __shfl_up_sync(0xffffffffu, src, 1);
-    }
     /* all half-sweeps on interior rows of this segment, no side column in the warp */
     const bool plain = g.plain_cols && (r - (H - 1) >= g.kw) && (r - (H - 1) >= 1) && (r <= g.nz - 1) && (r <= g.ke - 1);
     if (plain) {
+        /* every row read here lies inside the grid: no range checks */
+        const T2* rl = ring + (threadIdx.x & 31);
+        const T2 inm = rl[((r - 1) & (SMOOTH_RING - 1)) * 32], in0 = rl[(r & (SMOOTH_RING - 1)) * 32];
+        const T2 inp = rl[((r + 1) & (SMOOTH_RING - 1)) * 32];
+        T nb[H];
+#pragma unroll
+        for (int h = 0; h < H; h++) {
+            const T src = (h == 0) ? in0.y : h1[h - 1];
+            nb[h] = (h & 1) ? __shfl_down_sync(0xffffffffu, src, 1) : __shfl_up_sync(0xffffffffu, src, 1);
+        }
 #pragma unroll
         for (int h = H - 1; h >= 0; h--) {
-            constexpr bool dummy = false; (void)dummy;
             const bool odd = h & 1;
-            const T old = (h == 0) ? in0.x : (h == 1) ? inm.y : h2[h - 2];
             const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
             const T own_other = (h == 0) ? in0.y : h1[h - 1];
-            (void)old;
-            const T2 rk = ring_r<T>(ring, g, r - h);
+            const T2 rk = rl[(SMOOTH_RING + ((r - h) & (SMOOTH_RING - 1))) * 32];
             h2[h] = odd ? rx_in(rk.y, h1[h], up, own_other, nb[h], K) : rx_in(rk.x, h1[h], up, nb[h], own_other, K);
         }
+        (void)inm;
     } else {
+        const T2 inm = ring_e<T>(ring, g, r - 1), in0 = ring_e<T>(ring, g, r), inp = ring_e<T>(ring, g, r + 1);
+        T nb[H];
+#pragma unroll
+        for (int h = 0; h < H; h++) {
+            const T src = (h == 0) ? in0.y : h1[h - 1];
+            nb[h] = (h & 1) ? __shfl_down_sync(0xffffffffu, src, 1) : __shfl_up_sync(0xffffffffu, src, 1);
+        }
 #pragma unroll
         for (int h = H - 1; h >= 0; h--) {
             const int k = r - h;
@@ -1212,16 +1236,8 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
     MgLvlT<T> L = lvl<T>(c, l);
     const size_t smem = 2 * sizeof(T) * (size_t)(L.nx + 1) * (L.nz + 1);
-    if (g_relax_mode >= 1 && smem <= 200 * 1024 && L.nz >= 1) {
-        /* columns of one parity across x, the active sweeps (at most about
-         * nz/2 + 1 at a time) across y */
-        int cx = ((L.nx + 2) / 2 + 31) / 32 * 32;
-        if (cx > 1024) cx = 1024;
-        int cy = L.nz / 2 + 1;
-        if (cy > sweeps) cy = sweeps;
-        if (cy * cx > 1024) cy = 1024 / cx;
-        if (cy < 1) cy = 1;
-        k_mg_coarse_wave<T><<<3, dim3(cx, cy), smem, c->stream>>>(m, L, l, sweeps, c->inside);
+    if (g_relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1) {
+        k_mg_coarse_wave<T><<<3, 1024, smem + (L.nx + 1), c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
     } else if (g_relax_mode >= 1 && smem <= 200 * 1024) {
         int ncol = (L.nx + 2) / 2;
