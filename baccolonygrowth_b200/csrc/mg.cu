@@ -587,8 +587,10 @@ __device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T 
  * swap roles every step (the loop runs two steps per trip), and R and the
  * input rows are re-read through L1, prefetched SMOOTH_PF rows ahead. */
 #define RELAX_WARM_F 40
-#define SMOOTH_PF 8         /* rows staged ahead of the row step */
-#define SMOOTH_RING 16      /* ring slots per array; > SMOOTH_PF + 2S for every S used */
+#define SMOOTH_PF 4         /* rows staged ahead of the row step */
+#define SMOOTH_RING 11      /* ring slots per array; > SMOOTH_PF + 2S for every S used */
+/* slot of a row: (k - kw + 1) mod SMOOTH_RING, all rows read are >= kw - 1 */
+__device__ __forceinline__ int ring_wrap(int x) { return x < 0 ? x + SMOOTH_RING : (x >= SMOOTH_RING ? x - SMOOTH_RING : x); }
 #define SMOOTH_WARPS 4      /* warps per block */
 struct SmoothArgs {
     int nx, nz, pitch, l, sp, ce, co, kind_e, kind_o, kw, ks, ke;
@@ -601,12 +603,12 @@ struct SmoothArgs {
  * cp.async.wait_group is the only ordering needed. */
 template <class T>
 __device__ __forceinline__ void ring_issue(typename Pair2<T>::type* ring, const T* E, const T* R,
-                                           const SmoothArgs& g, int k)
+                                           const SmoothArgs& g, int k, int slot)
 {
     typedef typename Pair2<T>::type T2;
     const bool ok = g.ld_ok && k >= 0 && k <= g.nz;
     const size_t off = ok ? (size_t)k * g.pitch + g.ce : 0;
-    T2* se = ring + (k & (SMOOTH_RING - 1)) * 32 + (threadIdx.x & 31);
+    T2* se = ring + slot * 32 + (threadIdx.x & 31);
     T2* sr = se + SMOOTH_RING * 32;
     const unsigned de = (unsigned)__cvta_generic_to_shared(se), dr = (unsigned)__cvta_generic_to_shared(sr);
     const int n = ok ? (int)sizeof(T2) : 0;
@@ -623,14 +625,14 @@ template <class T>
 __device__ __forceinline__ typename Pair2<T>::type ring_e(const typename Pair2<T>::type* ring, const SmoothArgs& g, int k)
 {
     typename Pair2<T>::type v; v.x = T(0); v.y = T(0);
-    if (k >= 0 && k <= g.nz) v = ring[(k & (SMOOTH_RING - 1)) * 32 + (threadIdx.x & 31)];
+    if (k >= 0 && k <= g.nz) v = ring[((k - g.kw + 1) % SMOOTH_RING) * 32 + (threadIdx.x & 31)];
     return v;
 }
 template <class T>
 __device__ __forceinline__ typename Pair2<T>::type ring_r(const typename Pair2<T>::type* ring, const SmoothArgs& g, int k)
 {
     typename Pair2<T>::type v; v.x = T(0); v.y = T(0);
-    if (k >= 0 && k <= g.nz) v = ring[SMOOTH_RING * 32 + (k & (SMOOTH_RING - 1)) * 32 + (threadIdx.x & 31)];
+    if (k >= 0 && k <= g.nz) v = ring[SMOOTH_RING * 32 + ((k - g.kw + 1) % SMOOTH_RING) * 32 + (threadIdx.x & 31)];
     return v;
 }
 
@@ -645,7 +647,7 @@ __device__ __forceinline__ typename Pair2<T>::type ld_pair(const T* a, const Smo
 /* one row step: h1 = results of step r-1 (read only), h2 = results of step
  * r-2 on entry and of step r on exit */
 template <class T, int S>
-__device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T (&h2)[2 * S],
+__device__ __forceinline__ void smooth_step(const int r, const int sr, const T (&h1)[2 * S], T (&h2)[2 * S],
                                             const T* __restrict__ E, const T* __restrict__ R, T* __restrict__ EO,
                                             typename Pair2<T>::type* ring,
                                             const MgConst& m, const RelaxK<T>& K, const SmoothArgs& g,
@@ -655,15 +657,15 @@ __device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T
     constexpr int H = 2 * S;
     static_assert(SMOOTH_RING > SMOOTH_PF + H, "ring slot reused before its last read");
     /* stage row r+1+PF; rows up to r+1 are then complete */
-    ring_issue<T>(ring, E, R, g, r + 1 + SMOOTH_PF);
+    ring_issue<T>(ring, E, R, g, r + 1 + SMOOTH_PF, ring_wrap(sr + 1 + SMOOTH_PF));
     asm volatile("cp.async.wait_group %0;" :: "n"(SMOOTH_PF));
     /* all half-sweeps on interior rows of this segment, no side column in the warp */
     const bool plain = g.plain_cols && (r - (H - 1) >= g.kw) && (r - (H - 1) >= 1) && (r <= g.nz - 1) && (r <= g.ke - 1);
     if (plain) {
         /* every row read here lies inside the grid: no range checks */
         const T2* rl = ring + (threadIdx.x & 31);
-        const T2 inm = rl[((r - 1) & (SMOOTH_RING - 1)) * 32], in0 = rl[(r & (SMOOTH_RING - 1)) * 32];
-        const T2 inp = rl[((r + 1) & (SMOOTH_RING - 1)) * 32];
+        const T2 inm = rl[ring_wrap(sr - 1) * 32], in0 = rl[sr * 32];
+        const T2 inp = rl[ring_wrap(sr + 1) * 32];
         T nb[H];
 #pragma unroll
         for (int h = 0; h < H; h++) {
@@ -675,7 +677,7 @@ __device__ __forceinline__ void smooth_step(const int r, const T (&h1)[2 * S], T
             const bool odd = h & 1;
             const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
             const T own_other = (h == 0) ? in0.y : h1[h - 1];
-            const T2 rk = rl[(SMOOTH_RING + ((r - h) & (SMOOTH_RING - 1))) * 32];
+            const T2 rk = rl[(SMOOTH_RING + ring_wrap(sr - h)) * 32];
             h2[h] = odd ? rx_in(rk.y, h1[h], up, own_other, nb[h], K) : rx_in(rk.x, h1[h], up, nb[h], own_other, K);
         }
         (void)inm;
@@ -756,11 +758,14 @@ __global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLv
 #pragma unroll
         for (int h = 0; h < H; h++) { a[h] = (h & 1) ? e0.y : e0.x; b[h] = a[h]; }
     }
-    for (int k = g.kw - 1; k <= g.kw + SMOOTH_PF; k++) ring_issue<T>(ring, E, R, g, k);
+    for (int k = g.kw - 1; k <= g.kw + SMOOTH_PF; k++) ring_issue<T>(ring, E, R, g, k, k - g.kw + 1);
     const int r_end = g.ke - 1 + (H - 1);
+    int sr = 1;                                 /* slot of row r = kw */
     for (int r = g.kw; r <= r_end; r += 2) {
-        smooth_step<T, S>(r, a, b, E, R, EO, ring, m, K, g, inside0);
-        if (r + 1 <= r_end) smooth_step<T, S>(r + 1, b, a, E, R, EO, ring, m, K, g, inside0);
+        smooth_step<T, S>(r, sr, a, b, E, R, EO, ring, m, K, g, inside0);
+        sr = ring_wrap(sr + 1);
+        if (r + 1 <= r_end) smooth_step<T, S>(r + 1, sr, b, a, E, R, EO, ring, m, K, g, inside0);
+        sr = ring_wrap(sr + 1);
     }
     asm volatile("cp.async.wait_group 0;");
 }
