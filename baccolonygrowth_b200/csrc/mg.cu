@@ -928,17 +928,19 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l)
 template <bool SETUP>
 __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const double* __restrict__ inside0)
 {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    int sp = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    const int sp = blockIdx.z;
     const int nx = L.nx, nz = L.nz;
-    if (idx >= (nx + 1) * (nz + 1) || l >= m.A) return;
-    int i = idx % (nx + 1), k = idx / (nx + 1);
+    if (i > nx || l >= m.A) return;
     const int X = m.box_x, ZA = m.box_z_agar;
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d < X ? X * d0 / d : X;
     int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
-    double h2 = m.bl2 * d * d;
-    const double dt = m.dt, D = SP(m.D);
+    const double h2 = m.bl2 * d * d;
+    const double D = SP(m.D);
+    /* the reference scales each residual by dt*D/h^2 (D/h^2 for oxygen's
+     * top row) per point; here once per level */
+    const double cD = D / h2, cdt = m.dt * D / h2;
     const bool oxy = sp == 1;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     const double* A = SP(L.s);
@@ -961,39 +963,39 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
         if (l == m.A - 1) {
             int sx = (i == 0) ? 1 : -1;
             if (oxy) set = true, res = 0;
-            else if (k == 0) set = true, res = (2 * AL(i + sx, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
-            else if (k == nz) set = true, res = (2 * AL(i + sx, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D * dt / h2;
-            else set = true, res = (2 * AL(i + sx, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * D * dt / h2;
+            else if (k == 0) set = true, res = (2 * AL(i + sx, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * cdt;
+            else if (k == nz) set = true, res = (2 * AL(i + sx, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * cdt;
+            else set = true, res = (2 * AL(i + sx, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * cdt;
         }
     } else if (k == nz) {
         if (l == m.A - 1) {
             /* oxygen omits dt here, as the reference does (Multigrid.cpp:634) */
-            if (oxy) set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * D / h2;
-            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * dt * D / h2;
+            if (oxy) set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * cD;
+            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * cdt;
         }
     } else if (k == 0) {
         if (l == 0) {
             if (inside0[(size_t)i * m.box_z] > 0) set = true, res = 0;
             else if (oxy) set = true, res = m.max_o2_agar - AL(i, k);
-            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * cdt;
         } else if ((ip > 0 && ip < nxp) != 1) {
             if (oxy) set = true, res = m.max_o2_agar - AL(i, k);
-            else if (ip == 0) set = true, res = (APv(ip + 2, kp) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
-            else if (ip == nxp) set = true, res = (APv(ip - 2, kp) + AL(i + 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
-            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            else if (ip == 0) set = true, res = (APv(ip + 2, kp) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * cdt;
+            else if (ip == nxp) set = true, res = (APv(ip - 2, kp) + AL(i + 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * cdt;
+            else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * cdt;
         }
     } else {
         if (l > 0) {
             if (kp == nzp && ip > 0 && ip < nxp)
-                set = true, res = (AL(i + 1, k) + AL(i - 1, k) + APv(ip, kp - 2) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (AL(i + 1, k) + AL(i - 1, k) + APv(ip, kp - 2) + AL(i, k + 1) - 4 * AL(i, k)) * cdt;
             else if (ip == 0 && kp < nzp)
-                set = true, res = (APv(ip + 2, kp) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (APv(ip + 2, kp) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * cdt;
             else if (ip == nxp && kp < nzp)
-                set = true, res = (AL(i + 1, k) + APv(ip - 2, kp) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (AL(i + 1, k) + APv(ip - 2, kp) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * cdt;
             else if (ip <= 0 || ip >= nxp || kp >= nzp)
-                set = true, res = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+                set = true, res = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * cdt;
         } else {
-            set = true, res = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * dt * D / h2;
+            set = true, res = (AL(i + 1, k) + AL(i - 1, k) + AL(i, k - 1) + AL(i, k + 1) - 4 * AL(i, k)) * cdt;
         }
     }
 #undef AL
@@ -1299,8 +1301,9 @@ static void update_sol(bcg_ctx* c, const MgConst& m, int l)
 static void update_res(bcg_ctx* c, const MgConst& m, int l, bool setup_clean = false)
 {
     MgLvl L = mg_lvl(c, l), Lp = mg_lvl(c, l > 0 ? l - 1 : 0);
-    if (setup_clean) k_mg_update_res<true><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lp, l, c->inside);
-    else k_mg_update_res<false><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    dim3 grid((unsigned)((L.nx + 1 + 127) / 128), (unsigned)(L.nz + 1), 3);
+    if (setup_clean) k_mg_update_res<true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    else k_mg_update_res<false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
     c->launches++;
 }
 
