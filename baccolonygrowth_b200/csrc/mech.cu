@@ -301,7 +301,7 @@ __device__ __forceinline__ void sum_forces_group(const Cst& a, int me, const Cel
 }
 
 template <int G, bool GEOM32>
-__global__ void __launch_bounds__(256) k_move_grow(int n, int nbinned, const int* __restrict__ order,
+__global__ void __launch_bounds__(128, 4) k_move_grow(int n, int nbinned, const int* __restrict__ order,
         const CellRec* __restrict__ old, CellRec* __restrict__ nw,
         const int* __restrict__ nbr, const int* __restrict__ ncount,
         CellSoA soa, FieldPtrs fp, MechParams mp, double dt,
@@ -405,7 +405,7 @@ int launch_move_grow(bcg_ctx* c, double dt, int group)
         MechParams mp = mech_params(c);
         FieldPtrs fp = field_ptrs(c);
         int nb = c->n_binned < n ? c->n_binned : n;
-        const int threads = 256;
+        const int threads = 128;
         long tot = (long)n * group;
         unsigned blocks = (unsigned)((tot + threads - 1) / threads);
         const CellRec* old = c->rec[c->cur];
