@@ -393,32 +393,34 @@ def b200_arm(args):
     # end to end through the C ABI with host buffers: upload of the colony
     # from pinned host memory, the steps (each reads two counters back and
     # uploads the division draws), download of the final colony
-    sim2 = ctypes.c_void_p()
-    _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(hostbuf), 0, 12345 + rank, 0, ctypes.byref(sim2)), "sim2")
-    _abi.check(lib.bcg_sim_set_step_mode(sim2, 0, args.vcycles), "mode2")
-    ctx2 = lib.bcg_sim_ctx(sim2)
-    if args.smoother_warps > 0:
-        _abi.check(lib.bcg_set_smoother_warps(ctx2, args.smoother_warps), "set smoother warps")
-    g = np.full(p.box_x * p.box_z, 0.9)
-    lib.bcg_set_field(ctx2, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size)
-    out_pinned = torch.empty((n0 + n0 // 4) * 208, dtype=torch.uint8, pin_memory=True)
-    outbuf = out_pinned.numpy().view(_abi.CELL_DTYPE)
-    torch.cuda.synchronize()
-    w0 = time.perf_counter()
-    _abi.check(lib.bcg_upload_cells(ctx2, _abi.ptr(hostbuf), n0), "upload")
-    _abi.check(lib.bcg_update_density(ctx2), "density")
-    set_depleted_wall(lib, ctx2, p, wall_rows)
-    _abi.check(lib.bcg_sim_run(sim2, args.steps), "e2e steps")
-    got = ctypes.c_int()
-    _abi.check(lib.bcg_download_cells(ctx2, _abi.ptr(outbuf), len(outbuf), ctypes.byref(got)), "download")
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - w0
-    t2 = ctypes.c_double(); n2 = ctypes.c_int(); d2 = ctypes.c_int64()
-    lib.bcg_sim_time(sim2, ctypes.byref(t2), ctypes.byref(n2), ctypes.byref(d2))
-    lib.bcg_sim_destroy(sim2)
-    h2d = (n0 * 208 + 3 * 8 * p.box_x + 9 * 4 * d2.value) / args.steps
-    d2h = (got.value * 208 + 16 * args.steps + 8 * d2.value) / args.steps
-    e2e_value = 0.5 * (n0 + got.value) * args.steps / e2e_s
+    # one untimed pass (2 steps) first: first-touch costs of a new context
+    for e2e_pass, e2e_steps in ((0, 2), (1, args.steps)):
+        sim2 = ctypes.c_void_p()
+        _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(hostbuf), 0, 12345 + rank, 0, ctypes.byref(sim2)), "sim2")
+        _abi.check(lib.bcg_sim_set_step_mode(sim2, 0, args.vcycles), "mode2")
+        ctx2 = lib.bcg_sim_ctx(sim2)
+        if args.smoother_warps > 0:
+            _abi.check(lib.bcg_set_smoother_warps(ctx2, args.smoother_warps), "set smoother warps")
+        g = np.full(p.box_x * p.box_z, 0.9)
+        lib.bcg_set_field(ctx2, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size)
+        out_pinned = torch.empty((n0 + n0 // 4) * 208, dtype=torch.uint8, pin_memory=True)
+        outbuf = out_pinned.numpy().view(_abi.CELL_DTYPE)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        _abi.check(lib.bcg_upload_cells(ctx2, _abi.ptr(hostbuf), n0), "upload")
+        _abi.check(lib.bcg_update_density(ctx2), "density")
+        set_depleted_wall(lib, ctx2, p, wall_rows)
+        _abi.check(lib.bcg_sim_run(sim2, e2e_steps), "e2e steps")
+        got = ctypes.c_int()
+        _abi.check(lib.bcg_download_cells(ctx2, _abi.ptr(outbuf), len(outbuf), ctypes.byref(got)), "download")
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - w0
+        t2 = ctypes.c_double(); n2 = ctypes.c_int(); d2 = ctypes.c_int64()
+        lib.bcg_sim_time(sim2, ctypes.byref(t2), ctypes.byref(n2), ctypes.byref(d2))
+        lib.bcg_sim_destroy(sim2)
+        h2d = (n0 * 208 + 3 * 8 * p.box_x + 9 * 4 * d2.value) / e2e_steps
+        d2h = (got.value * 208 + 16 * e2e_steps + 8 * d2.value) / e2e_steps
+        e2e_value = 0.5 * (n0 + got.value) * e2e_steps / e2e_s
 
     # the agar solve to a 1e-8 relative defect: plain FP64 V-cycles vs FP32
     # V-cycles with FP64 defect checks and FP64 refinement, from the same state
