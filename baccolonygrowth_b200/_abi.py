@@ -231,6 +231,7 @@ EXTRA_PROTOTYPES = {
     "bcg_set_bbox": (_I, [_VP, _I, _I, _I]),
     "bcg_set_relax_mode": (_I, [_I]),
     "bcg_set_smoother_warps": (_I, [_VP, _I]),
+    "bcg_smoother_launch_ms": (_I, [_VP, _PD]),
 }
 
 TUNE = dict(FORCE_GROUP=1, SMOOTHER=2)

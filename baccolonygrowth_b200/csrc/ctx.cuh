@@ -106,6 +106,7 @@ struct bcg_ctx {
      * reset() left them; setup() then skips its resetZero */
     int mg_clean;
     int pair_f32;          /* contact geometry in FP32 local to cell i (bcg_set_pair_precision) */
+    double smooth_tune_ms; /* device time of one level-0 fused smoother launch at the tuned shape */
 };
 
 MechParams mech_params(const bcg_ctx* c);

@@ -1268,6 +1268,15 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 }
 
 /* kernel attributes set once per process, outside any stream capture */
+/* device time (ms) of one level-0 launch of the fused 3-sweep smoother at
+ * the shape bcg_autotune chose (0 before tuning) */
+extern "C" int bcg_smoother_launch_ms(bcg_ctx* c, double* ms)
+{
+    if (!c || !ms) return BCG_E_ARG;
+    *ms = c->smooth_tune_ms;
+    return BCG_OK;
+}
+
 /* pin the smoother's resident-warp target for a context (0 = the default
  * or the tuned value); used to profile a fixed kernel shape */
 extern "C" int bcg_set_smoother_warps(bcg_ctx* c, int warps)
@@ -1325,7 +1334,7 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
         if (cudaEventSynchronize(b) != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); c->smooth_warps = saved; return BCG_E_CUDA; }
         float ms = 0;
         cudaEventElapsedTime(&ms, a, b);
-        if (ms < best) { best = ms; best_t = targets[ti]; }
+        if (ms < best) { best = ms; best_t = targets[ti]; c->smooth_tune_ms = ms / 2.0; }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
