@@ -587,11 +587,12 @@ __device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T 
  * swap roles every step (the loop runs two steps per trip), and R and the
  * input rows are re-read through L1, prefetched SMOOTH_PF rows ahead. */
 #define RELAX_WARM_F 40
-#define SMOOTH_PF 5         /* rows staged ahead of the row step */
-#define SMOOTH_RING 12      /* ring slots per array; > SMOOTH_PF + 2S for every S used; even (steps alternate roles) */
+#define SMOOTH_PF 8         /* rows staged ahead of the row step */
+#define SMOOTH_RING 16      /* ring slots per array; > SMOOTH_PF + 2S for every S used; a power of 2 */
+#define SMOOTH_BLOCK 4      /* steady-state row steps per unrolled block; divides SMOOTH_RING, even */
 /* slot of a row: (k - kw + 1) mod SMOOTH_RING, all rows read are >= kw - 1 */
 __device__ __forceinline__ int ring_wrap(int x) { return x < 0 ? x + SMOOTH_RING : (x >= SMOOTH_RING ? x - SMOOTH_RING : x); }
-#define SMOOTH_WARPS 4      /* warps per block */
+#define SMOOTH_WARPS 2      /* warps per block */
 struct SmoothArgs {
     int nx, nz, pitch, l, sp, ce, co, kind_e, kind_o, kw, ks, ke;
     bool ld_ok, st_e, st_o, plain_cols;
@@ -717,8 +718,8 @@ __device__ __forceinline__ void smooth_step(const int r, const int sr, const T (
     }
 }
 
-/* slot of a row offset known at compile time */
-__host__ __device__ constexpr int cslot(int x) { return ((x % SMOOTH_RING) + SMOOTH_RING) % SMOOTH_RING; }
+/* slot of row r + x given the slot of row r (a multiple of SMOOTH_BLOCK) */
+__device__ __forceinline__ int bslot(int base, int x) { return (base + x) & (SMOOTH_RING - 1); }
 
 /* Pointers the steady-state steps advance by one row per step: the lane's
  * column pair in E and R of the row being staged, and in E2 of the row
@@ -726,12 +727,13 @@ __host__ __device__ constexpr int cslot(int x) { return ((x % SMOOTH_RING) + SMO
 template <class T>
 struct SmoothPtrs { const T* pe; const T* pr; T* po; };
 
-/* One steady-state row step, position J of a block of SMOOTH_RING steps
- * that starts at a row in slot 0: every ring slot is a constant.  Valid
- * when all half-sweeps relax interior rows of the segment and the warp
- * holds no side column (the conditions of the plain path of smooth_step). */
+/* One steady-state row step, position J of a block of SMOOTH_BLOCK steps
+ * whose first row sits in ring slot `base`: ring slots are base plus a
+ * constant, masked.  Valid when all half-sweeps relax interior rows of the
+ * segment and the warp holds no side column (the conditions of the plain
+ * path of smooth_step). */
 template <class T, int S, int J>
-__device__ __forceinline__ void plain_step(const int r, const T (&h1)[2 * S], T (&h2)[2 * S],
+__device__ __forceinline__ void plain_step(const int r, const int base, const T (&h1)[2 * S], T (&h2)[2 * S],
                                            typename Pair2<T>::type* ringl, SmoothPtrs<T>& q, const T* dummy,
                                            const RelaxK<T>& K, const SmoothArgs& g)
 {
@@ -742,7 +744,7 @@ __device__ __forceinline__ void plain_step(const int r, const T (&h1)[2 * S], T 
         const int kk = r + 1 + SMOOTH_PF;
         const bool ok = g.ld_ok && kk <= g.nz;
         const int n = ok ? (int)sizeof(T2) : 0;
-        T2* se = ringl + cslot(J + 1 + SMOOTH_PF) * 32;
+        T2* se = ringl + bslot(base, J + 1 + SMOOTH_PF) * 32;
         const unsigned de = (unsigned)__cvta_generic_to_shared(se), dr = (unsigned)__cvta_generic_to_shared(se + RG * 32);
         const T* ge = ok ? q.pe : dummy;
         const T* gr = ok ? q.pr : dummy;
@@ -757,7 +759,7 @@ __device__ __forceinline__ void plain_step(const int r, const T (&h1)[2 * S], T 
         q.pe += g.pitch; q.pr += g.pitch;
     }
     asm volatile("cp.async.wait_group %0;" :: "n"(SMOOTH_PF));
-    const T2 in0 = ringl[cslot(J) * 32], inp = ringl[cslot(J + 1) * 32];
+    const T2 in0 = ringl[bslot(base, J) * 32], inp = ringl[bslot(base, J + 1) * 32];
     T nb[H];
 #pragma unroll
     for (int h = 0; h < H; h++) {
@@ -769,7 +771,7 @@ __device__ __forceinline__ void plain_step(const int r, const T (&h1)[2 * S], T 
         const bool odd = h & 1;
         const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
         const T own_other = (h == 0) ? in0.y : h1[h - 1];
-        const T2 rk = ringl[(RG + cslot(J - h)) * 32];
+        const T2 rk = ringl[(RG + bslot(base, J - h)) * 32];
         h2[h] = odd ? rx_in(rk.y, h1[h], up, own_other, nb[h], K) : rx_in(rk.x, h1[h], up, nb[h], own_other, K);
     }
     if (r - (H - 1) >= g.ks) {
@@ -780,20 +782,20 @@ __device__ __forceinline__ void plain_step(const int r, const T (&h1)[2 * S], T 
     q.po += g.pitch;
 }
 
-/* SMOOTH_RING steady-state steps; the roles of the history arrays
+/* SMOOTH_BLOCK steady-state steps; the roles of the history arrays
  * alternate, starting with (h1, h2) = (x, y) */
 template <class T, int S, int J>
 struct PlainBlock {
-    static __device__ __forceinline__ void run(int r, T (&x)[2 * S], T (&y)[2 * S], typename Pair2<T>::type* ringl,
+    static __device__ __forceinline__ void run(int r, int base, T (&x)[2 * S], T (&y)[2 * S], typename Pair2<T>::type* ringl,
                                                SmoothPtrs<T>& q, const T* dummy, const RelaxK<T>& K, const SmoothArgs& g)
     {
-        plain_step<T, S, J>(r + J, x, y, ringl, q, dummy, K, g);
-        PlainBlock<T, S, J + 1>::run(r, y, x, ringl, q, dummy, K, g);
+        plain_step<T, S, J>(r + J, base, x, y, ringl, q, dummy, K, g);
+        PlainBlock<T, S, J + 1>::run(r, base, y, x, ringl, q, dummy, K, g);
     }
 };
 template <class T, int S>
-struct PlainBlock<T, S, SMOOTH_RING> {
-    static __device__ __forceinline__ void run(int, T (&)[2 * S], T (&)[2 * S], typename Pair2<T>::type*,
+struct PlainBlock<T, S, SMOOTH_BLOCK> {
+    static __device__ __forceinline__ void run(int, int, T (&)[2 * S], T (&)[2 * S], typename Pair2<T>::type*,
                                                SmoothPtrs<T>&, const T*, const RelaxK<T>&, const SmoothArgs&) {}
 };
 
@@ -842,24 +844,26 @@ __global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLv
     const int r_end = g.ke - 1 + (H - 1);
     /* steady-state rows: every half-sweep on an interior row of the segment */
     const int r_lo = max(g.kw + H - 1, H), r_hi = min(g.nz - 1, g.ke - 1);
-    /* first steady row in ring slot 0: slot(k) = (k - kw + 1) mod RING */
-    int r_al = g.kw - 1 + SMOOTH_RING;
-    if (r_al < r_lo) r_al += (r_lo - r_al + SMOOTH_RING - 1) / SMOOTH_RING * SMOOTH_RING;
+    /* first steady row whose slot is a multiple of SMOOTH_BLOCK:
+     * slot(k) = (k - kw + 1) mod RING */
+    int r_al = g.kw - 1 + SMOOTH_BLOCK;
+    if (r_al < r_lo) r_al += (r_lo - r_al + SMOOTH_BLOCK - 1) / SMOOTH_BLOCK * SMOOTH_BLOCK;
     typename Pair2<T>::type* ringl = ring + lane;
     int r = g.kw, sr = 1;                       /* sr: slot of row r */
     while (r <= r_end) {
-        if (g.plain_cols && r == r_al && r + SMOOTH_RING - 1 <= r_hi) {
-            /* (r - kw) is odd here (slot 0), so the first step reads b as h1 */
+        if (g.plain_cols && r == r_al && r + SMOOTH_BLOCK - 1 <= r_hi) {
+            /* (r - kw) is odd here (slot a multiple of the even block), so
+             * the first step reads b as h1 */
             SmoothPtrs<T> q;
             const size_t col = g.ld_ok ? (size_t)g.ce : 0;
             q.pe = E + (size_t)(r + 1 + SMOOTH_PF) * g.pitch + col;
             q.pr = R + (size_t)(r + 1 + SMOOTH_PF) * g.pitch + col;
             q.po = EO + (size_t)(r - (H - 1)) * g.pitch + (g.ce >= 0 ? g.ce : 0);
             do {
-                PlainBlock<T, S, 0>::run(r, b, a, ringl, q, E, K, g);
-                r += SMOOTH_RING;
-            } while (r + SMOOTH_RING - 1 <= r_hi);
-            sr = 0;
+                PlainBlock<T, S, 0>::run(r, sr, b, a, ringl, q, E, K, g);
+                r += SMOOTH_BLOCK;
+                sr = (sr + SMOOTH_BLOCK) & (SMOOTH_RING - 1);
+            } while (r + SMOOTH_BLOCK - 1 <= r_hi);
             continue;
         }
         if (((r - g.kw) & 1) == 0) smooth_step<T, S>(r, sr, a, b, E, R, EO, ring, m, K, g, inside0);
