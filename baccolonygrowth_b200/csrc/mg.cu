@@ -587,12 +587,11 @@ __device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T 
  * swap roles every step (the loop runs two steps per trip), and R and the
  * input rows are re-read through L1, prefetched SMOOTH_PF rows ahead. */
 #define RELAX_WARM_F 40
-#define SMOOTH_PF 8         /* rows staged ahead of the row step */
-#define SMOOTH_RING 16      /* ring slots per array; > SMOOTH_PF + 2S for every S used; a power of 2 */
-#define SMOOTH_BLOCK 4      /* steady-state row steps per unrolled block; divides SMOOTH_RING, even */
+#define SMOOTH_PF 4         /* rows staged ahead of the row step */
+#define SMOOTH_RING 11      /* ring slots per array; > SMOOTH_PF + 2S for every S used */
 /* slot of a row: (k - kw + 1) mod SMOOTH_RING, all rows read are >= kw - 1 */
 __device__ __forceinline__ int ring_wrap(int x) { return x < 0 ? x + SMOOTH_RING : (x >= SMOOTH_RING ? x - SMOOTH_RING : x); }
-#define SMOOTH_WARPS 2      /* warps per block */
+#define SMOOTH_WARPS 4      /* warps per block */
 struct SmoothArgs {
     int nx, nz, pitch, l, sp, ce, co, kind_e, kind_o, kw, ks, ke;
     bool ld_ok, st_e, st_o, plain_cols;
@@ -718,87 +717,6 @@ __device__ __forceinline__ void smooth_step(const int r, const int sr, const T (
     }
 }
 
-/* slot of row r + x given the slot of row r (a multiple of SMOOTH_BLOCK) */
-__device__ __forceinline__ int bslot(int base, int x) { return (base + x) & (SMOOTH_RING - 1); }
-
-/* Pointers the steady-state steps advance by one row per step: the lane's
- * column pair in E and R of the row being staged, and in E2 of the row
- * being stored. */
-template <class T>
-struct SmoothPtrs { const T* pe; const T* pr; T* po; };
-
-/* One steady-state row step, position J of a block of SMOOTH_BLOCK steps
- * whose first row sits in ring slot `base`: ring slots are base plus a
- * constant, masked.  Valid when all half-sweeps relax interior rows of the
- * segment and the warp holds no side column (the conditions of the plain
- * path of smooth_step). */
-template <class T, int S, int J>
-__device__ __forceinline__ void plain_step(const int r, const int base, const T (&h1)[2 * S], T (&h2)[2 * S],
-                                           typename Pair2<T>::type* ringl, SmoothPtrs<T>& q, const T* dummy,
-                                           const RelaxK<T>& K, const SmoothArgs& g)
-{
-    typedef typename Pair2<T>::type T2;
-    constexpr int H = 2 * S;
-    constexpr int RG = SMOOTH_RING;
-    {
-        const int kk = r + 1 + SMOOTH_PF;
-        const bool ok = g.ld_ok && kk <= g.nz;
-        const int n = ok ? (int)sizeof(T2) : 0;
-        T2* se = ringl + bslot(base, J + 1 + SMOOTH_PF) * 32;
-        const unsigned de = (unsigned)__cvta_generic_to_shared(se), dr = (unsigned)__cvta_generic_to_shared(se + RG * 32);
-        const T* ge = ok ? q.pe : dummy;
-        const T* gr = ok ? q.pr : dummy;
-        if (sizeof(T2) == 16) {
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(de), "l"(ge), "r"(n));
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dr), "l"(gr), "r"(n));
-        } else {
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(de), "l"(ge), "r"(n));
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(dr), "l"(gr), "r"(n));
-        }
-        asm volatile("cp.async.commit_group;");
-        q.pe += g.pitch; q.pr += g.pitch;
-    }
-    asm volatile("cp.async.wait_group %0;" :: "n"(SMOOTH_PF));
-    const T2 in0 = ringl[bslot(base, J) * 32], inp = ringl[bslot(base, J + 1) * 32];
-    T nb[H];
-#pragma unroll
-    for (int h = 0; h < H; h++) {
-        const T src = (h == 0) ? in0.y : h1[h - 1];
-        nb[h] = (h & 1) ? __shfl_down_sync(0xffffffffu, src, 1) : __shfl_up_sync(0xffffffffu, src, 1);
-    }
-#pragma unroll
-    for (int h = H - 1; h >= 0; h--) {
-        const bool odd = h & 1;
-        const T up = (h == 0) ? inp.x : (h == 1) ? in0.y : h1[h - 2];
-        const T own_other = (h == 0) ? in0.y : h1[h - 1];
-        const T2 rk = ringl[(RG + bslot(base, J - h)) * 32];
-        h2[h] = odd ? rx_in(rk.y, h1[h], up, own_other, nb[h], K) : rx_in(rk.x, h1[h], up, nb[h], own_other, K);
-    }
-    if (r - (H - 1) >= g.ks) {
-        T2 v; v.x = h1[H - 2]; v.y = h2[H - 1];
-        if (g.st_e && g.st_o) *reinterpret_cast<T2*>(q.po) = v;
-        else if (g.st_e) *q.po = v.x;
-    }
-    q.po += g.pitch;
-}
-
-/* SMOOTH_BLOCK steady-state steps; the roles of the history arrays
- * alternate, starting with (h1, h2) = (x, y) */
-template <class T, int S, int J>
-struct PlainBlock {
-    static __device__ __forceinline__ void run(int r, int base, T (&x)[2 * S], T (&y)[2 * S], typename Pair2<T>::type* ringl,
-                                               SmoothPtrs<T>& q, const T* dummy, const RelaxK<T>& K, const SmoothArgs& g)
-    {
-        plain_step<T, S, J>(r + J, base, x, y, ringl, q, dummy, K, g);
-        PlainBlock<T, S, J + 1>::run(r, base, y, x, ringl, q, dummy, K, g);
-    }
-};
-template <class T, int S>
-struct PlainBlock<T, S, SMOOTH_BLOCK> {
-    static __device__ __forceinline__ void run(int, int, T (&)[2 * S], T (&)[2 * S], typename Pair2<T>::type*,
-                                               SmoothPtrs<T>&, const T*, const RelaxK<T>&, const SmoothArgs&) {}
-};
-
 template <class T, int S>
 __global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLvlT<T> L, int l, int seg_len,
                                                    const double* __restrict__ inside0)
@@ -842,33 +760,11 @@ __global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLv
     }
     for (int k = g.kw - 1; k <= g.kw + SMOOTH_PF; k++) ring_issue<T>(ring, E, R, g, k, k - g.kw + 1);
     const int r_end = g.ke - 1 + (H - 1);
-    /* steady-state rows: every half-sweep on an interior row of the segment */
-    const int r_lo = max(g.kw + H - 1, H), r_hi = min(g.nz - 1, g.ke - 1);
-    /* first steady row whose slot is a multiple of SMOOTH_BLOCK:
-     * slot(k) = (k - kw + 1) mod RING */
-    int r_al = g.kw - 1 + SMOOTH_BLOCK;
-    if (r_al < r_lo) r_al += (r_lo - r_al + SMOOTH_BLOCK - 1) / SMOOTH_BLOCK * SMOOTH_BLOCK;
-    typename Pair2<T>::type* ringl = ring + lane;
-    int r = g.kw, sr = 1;                       /* sr: slot of row r */
-    while (r <= r_end) {
-        if (g.plain_cols && r == r_al && r + SMOOTH_BLOCK - 1 <= r_hi) {
-            /* (r - kw) is odd here (slot a multiple of the even block), so
-             * the first step reads b as h1 */
-            SmoothPtrs<T> q;
-            const size_t col = g.ld_ok ? (size_t)g.ce : 0;
-            q.pe = E + (size_t)(r + 1 + SMOOTH_PF) * g.pitch + col;
-            q.pr = R + (size_t)(r + 1 + SMOOTH_PF) * g.pitch + col;
-            q.po = EO + (size_t)(r - (H - 1)) * g.pitch + (g.ce >= 0 ? g.ce : 0);
-            do {
-                PlainBlock<T, S, 0>::run(r, sr, b, a, ringl, q, E, K, g);
-                r += SMOOTH_BLOCK;
-                sr = (sr + SMOOTH_BLOCK) & (SMOOTH_RING - 1);
-            } while (r + SMOOTH_BLOCK - 1 <= r_hi);
-            continue;
-        }
-        if (((r - g.kw) & 1) == 0) smooth_step<T, S>(r, sr, a, b, E, R, EO, ring, m, K, g, inside0);
-        else smooth_step<T, S>(r, sr, b, a, E, R, EO, ring, m, K, g, inside0);
-        r++;
+    int sr = 1;                                 /* slot of row r = kw */
+    for (int r = g.kw; r <= r_end; r += 2) {
+        smooth_step<T, S>(r, sr, a, b, E, R, EO, ring, m, K, g, inside0);
+        sr = ring_wrap(sr + 1);
+        if (r + 1 <= r_end) smooth_step<T, S>(r + 1, sr, b, a, E, R, EO, ring, m, K, g, inside0);
         sr = ring_wrap(sr + 1);
     }
     asm volatile("cp.async.wait_group 0;");
