@@ -577,7 +577,7 @@ __device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T 
  * so the 2S updates of a step are independent.  A half-sweep's result is
  * exact where all of its inputs were, which loses one lane at one strip
  * edge per half-sweep: lanes S .. 31-S are written.  Segments other than
- * the first start RELAX_WARM_F rows early from the pre-smoothing values;
+ * the first start `warm` rows early from the pre-smoothing values;
  * the row recurrence contracts by at least 1/4 per row, so the start
  * error is below rounding when the segment's own rows begin.  Rows above
  * the segment are relaxed by the early half-sweeps as far as the later
@@ -586,7 +586,6 @@ __device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T 
  * Register use: a half-sweep's last two results live in two arrays that
  * swap roles every step (the loop runs two steps per trip), and R and the
  * input rows are re-read through L1, prefetched SMOOTH_PF rows ahead. */
-#define RELAX_WARM_F 40
 #define SMOOTH_PF 4         /* rows staged ahead of the row step */
 #define SMOOTH_RING 11      /* ring slots per array; > SMOOTH_PF + 2S for every S used */
 /* slot of a row: (k - kw + 1) mod SMOOTH_RING, all rows read are >= kw - 1 */
@@ -719,7 +718,7 @@ __device__ __forceinline__ void smooth_step(const int r, const int sr, const T (
 
 template <class T, int S>
 __global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLvlT<T> L, int l, int seg_len,
-                                                   const double* __restrict__ inside0)
+                                                   int warm, const double* __restrict__ inside0)
 {
     constexpr int H = 2 * S;
     const int lane = threadIdx.x;
@@ -737,7 +736,7 @@ __global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLv
     g.ks = blockIdx.y * seg_len;
     if (g.ks > g.nz) return;
     g.ke = min(g.ks + seg_len, g.nz + 1);
-    g.kw = max(0, g.ks - RELAX_WARM_F);
+    g.kw = max(0, g.ks - warm);
     const T* __restrict__ E = SP(L.e);
     const T* __restrict__ R = SP(L.r);
     T* __restrict__ EO = SP(L.e2);
@@ -1135,6 +1134,28 @@ template <> void swap_err<float>(bcg_ctx* c, int l)
  * correction buffers.  Pre- and post-smoothing use the same number of
  * launches, so a V-cycle always swaps an even number of times and leaves
  * the buffers where it found them (captured graphs rely on this). */
+/* Rows a segment of level l starts early: the row recurrence of a sweep
+ * contracts by a = max over species of (1/2)/(cf + 2), cf = h^2/(dt D),
+ * and the start error of a segment shrinks by a^w (times a polynomial
+ * factor w^2 from the three pipelined sweeps) over w rows; w is taken so
+ * that this is below 1e-18.  About 38 rows on the finest level of the
+ * shipped input, a handful on the coarse levels, where h is larger. */
+static int warm_rows(const MgConst& m, int l)
+{
+    double a = 0.0;
+    for (int sp = 0; sp < 3; sp++) {
+        const double cf = m.bl2 * (double)(1 << (2 * l)) / m.dt / m.D[sp];
+        const double v = 0.5 / (cf + 2.0);
+        a = v > a ? v : a;
+    }
+    for (int w = 1; w < 64; w++) {
+        double e = (double)w * w;
+        for (int j = 0; j < w; j++) e *= a;
+        if (e < 1e-18) return w;
+    }
+    return 64;
+}
+
 template <class T>
 static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
@@ -1151,16 +1172,19 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         const int outp = 32 - 2 * S;
         const int nwx = (L.nx + 1 + 2 * outp - 1) / (2 * outp);
         const int target = c->smooth_warps > 0 ? c->smooth_warps : g_smooth_warps;
+        const int warm = warm_rows(m, l);
         int nseg = (target + 3 * nwx - 1) / (3 * nwx);
-        const int max_seg = rows / 32 > 1 ? rows / 32 : 1;
+        /* segments of at least 16 rows and no shorter than half the warm-up */
+        const int min_len = warm / 2 > 16 ? warm / 2 : 16;
+        const int max_seg = rows / min_len > 1 ? rows / min_len : 1;
         if (nseg > max_seg) nseg = max_seg;
         if (nseg < 1) nseg = 1;
         const int seg_len = (rows + nseg - 1) / nseg;
         dim3 block(32, SMOOTH_WARPS), grid((unsigned)((nwx + SMOOTH_WARPS - 1) / SMOOTH_WARPS), (unsigned)nseg, 3);
         const size_t smem = (size_t)SMOOTH_WARPS * 2 * SMOOTH_RING * 32 * 2 * sizeof(T);
-        if (S == 3) k_mg_smooth<T, 3><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, c->inside);
-        else if (S == 2) k_mg_smooth<T, 2><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, c->inside);
-        else k_mg_smooth<T, 1><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, c->inside);
+        if (S == 3) k_mg_smooth<T, 3><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, warm, c->inside);
+        else if (S == 2) k_mg_smooth<T, 2><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, warm, c->inside);
+        else k_mg_smooth<T, 1><<<grid, block, smem, c->stream>>>(m, L, l, seg_len, warm, c->inside);
         c->launches++;
         swap_err<T>(c, l);
         sweeps -= S;
