@@ -25,6 +25,7 @@ E_TIMEOUT = 8
 E_UNSUPPORTED = 9
 E_NEED_MORE_BOXES = 10
 E_NO_DEVICE = 11
+E_IO = 12
 
 # ---- field ids (bcg_field_id) --------------------------------------------
 FIELDS = dict(
@@ -37,7 +38,9 @@ FIELDS = dict(
     MG_SOL_CARBON=29, MG_SOL_OXYGEN=30, MG_SOL_ACETATE=31,
     MG_RES_CARBON=32, MG_RES_OXYGEN=33, MG_RES_ACETATE=34,
     MG_ERR_CARBON=35, MG_ERR_OXYGEN=36, MG_ERR_ACETATE=37,
-    DENSITY=38, ROUGH_DENSITY=39)
+    DENSITY=38, ROUGH_DENSITY=39,
+    ENV_HYDROX=40, ENV_ACETIC=41, ENV_BUFFER=42, ENV_GR_CAR_AER=43, ENV_GR_CAR_ANA=44, ENV_GR_ACE_AER=45,
+    ENV_Q_CAR_MNT=46, ENV_Q_ACE_MNT=47, ENV_P_ACE_MNT=48, ENV_Q_OXY_MNT=49)
 
 TIMERS = dict(MOVE_GROW=0, DIVIDE=1, NEIGHBOURS=2, MG_SOLVE=3, SWEEPS=4, DENSITY=5)
 
@@ -222,7 +225,34 @@ PROTOTYPES = {
     "bcg_load_restart": (_I, [ctypes.c_char_p, _PD, _PD, _VP, _I, _PI]),
     "bcg_mean_stress": (_I, [_VP, _PD, _PD, _PI64]),
     "bcg_mean_stress_noalloc": (_I, [_VP, _PD, _PD, _PI64]),
+    "bcg_write_output": (_I, [ctypes.c_char_p, _I, _I, _I, _VP, _I]),
+    "bcg_writer_create": (_I, [ctypes.c_char_p, _I, _I, _I, ctypes.POINTER(_VP)]),
+    "bcg_writer_wait": (_I, [_VP]),
+    "bcg_writer_destroy": (_I, [_VP]),
+    "bcg_output_initial": (_I, [_VP, _VP, _D]),
+    "bcg_output_cells": (_I, [_VP, _VP, _I, _D, _PI64]),
+    "bcg_output_fields": (_I, [_VP, _VP, _I, _D, _D]),
+    "bcg_writer_lineage": (_I, [_VP, _PI, _I]),
+    "bcg_sim_set_writer": (_I, [_VP, _VP, _I]),
 }
+
+OUT_CELLS = 1     # BCG_OUT_CELLS
+OUT_FIELDS = 2    # BCG_OUT_FIELDS
+
+
+class OutputData(ctypes.Structure):
+    """Mirror of struct bcg_output_data."""
+    _fields_ = [
+        ("t", ctypes.c_double), ("dt", ctypes.c_double),
+        ("n_cells", ctypes.c_int32), ("force_stride", ctypes.c_int32),
+        ("cells", _VP), ("cell_force", _VP),
+        ("n_restart", ctypes.c_int32), ("levels", ctypes.c_int32),
+        ("restart_cells", _VP),
+        ("box_x", ctypes.c_int32), ("box_z", ctypes.c_int32), ("box_z_agar", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("density", _VP), ("env", _VP * 17),
+        ("agar", _VP), ("wall", _VP),
+    ]
 
 # library entry points outside include/bcg.h, used by tests and the benchmark
 EXTRA_PROTOTYPES = {

@@ -13,8 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbcg.so")
 
-CU_SOURCES = ["ctx.cu", "mech.cu", "fields.cu", "mg.cu", "nutrients.cu", "steady.cu"]
-CPP_SOURCES = ["host.cpp", "sim.cpp"]
+CU_SOURCES = ["ctx.cu", "mech.cu", "fields.cu", "mg.cu", "nutrients.cu", "steady.cu", "output.cu"]
+CPP_SOURCES = ["host.cpp", "sim.cpp", "writer.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
@@ -57,7 +57,7 @@ def build(verbose=False, force=False):
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -25,6 +25,7 @@ extern "C" const char* bcg_status_string(int s)
     case BCG_E_UNSUPPORTED: return "unsupported parameter combination";
     case BCG_E_NEED_MORE_BOXES: return "Need more boxes";
     case BCG_E_NO_DEVICE: return "no CUDA device";
+    case BCG_E_IO: return "Can't open output file.";
     default: return "unknown status";
     }
 }
@@ -212,6 +213,10 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
             DALLOC(*arrs[k], X * Z * 8);
             if ((rc = fill(c, *arrs[k], init[k], X * Z))) { bcg_destroy(c); return rc; }
         }
+        for (int k = 0; k < 7 && b == 0; k++) {
+            DALLOC(e.extra[k], X * Z * 8);
+            if ((rc = fill(c, e.extra[k], 0.0, X * Z))) { bcg_destroy(c); return rc; }
+        }
         WallBuf& w = c->wal[b];
         for (int l = 0; l < p->max_levels_mg; l++) {
             DALLOC(w.C[l], X * 8); DALLOC(w.W[l], X * 8); DALLOC(w.O[l], X * 8); DALLOC(w.A[l], X * 8);
@@ -275,6 +280,7 @@ extern "C" int bcg_destroy(bcg_ctx* c)
         EnvBuf& e = c->env[b];
         void* ea[] = {e.C, e.W, e.A, e.O, e.gr1, e.gr2, e.ph, e.hydrox, e.acetic, e.buffer};
         for (void* q : ea) if (q) cudaFree(q);
+        for (double* q : e.extra) if (q) cudaFree(q);
         for (int l = 0; l < BCG_MAX_AGAR_LEVELS; l++) {
             void* wa[] = {c->wal[b].C[l], c->wal[b].W[l], c->wal[b].O[l], c->wal[b].A[l]};
             for (void* q : wa) if (q) cudaFree(q);
@@ -330,6 +336,13 @@ __global__ void k_pack(int n, bcg_cell* __restrict__ out, const CellRec* __restr
     c.sta_fric.x = s.sfx[i]; c.sta_fric.y = s.sfy[i]; c.sta_fric.z = s.sfz[i];
     c.type = s.type[i]; c.ancestor = s.anc[i];
     out[i] = c;
+}
+
+void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s)
+{
+    if (c->n <= 0) return;
+    k_pack<<<(c->n + 255) / 256, 256, 0, s>>>(c->n, dst, c->rec[c->cur], c->soa);
+    c->launches++;
 }
 
 /* the AoS staging buffer reuses the second record buffer's space when it is
@@ -441,6 +454,12 @@ static int field_view(bcg_ctx* c, int f, int level, FieldView* v)
     case BCG_F_ENV_GROWTH1: v->ptr = c->env[0].gr1; v->n = X * Z; return BCG_OK;
     case BCG_F_ENV_GROWTH2: v->ptr = c->env[0].gr2; v->n = X * Z; return BCG_OK;
     case BCG_F_ENV_PH: v->ptr = c->env[0].ph; v->n = X * Z; return BCG_OK;
+    case BCG_F_ENV_HYDROX: v->ptr = c->env[0].hydrox; v->n = X * Z; return BCG_OK;
+    case BCG_F_ENV_ACETIC: v->ptr = c->env[0].acetic; v->n = X * Z; return BCG_OK;
+    case BCG_F_ENV_BUFFER: v->ptr = c->env[0].buffer; v->n = X * Z; return BCG_OK;
+    case BCG_F_ENV_GR_CAR_AER: case BCG_F_ENV_GR_CAR_ANA: case BCG_F_ENV_GR_ACE_AER:
+    case BCG_F_ENV_Q_CAR_MNT: case BCG_F_ENV_Q_ACE_MNT: case BCG_F_ENV_P_ACE_MNT: case BCG_F_ENV_Q_OXY_MNT:
+        v->ptr = c->env[0].extra[f - BCG_F_ENV_GR_CAR_AER]; v->n = X * Z; return BCG_OK;
     default: break;
     }
     if (f >= BCG_F_WALLF_CARBON && f <= BCG_F_OLDWALLF_ACETATE) {

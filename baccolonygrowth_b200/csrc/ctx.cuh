@@ -25,6 +25,10 @@ struct EnvBuf {
     double *C, *W, *A, *O;     /* Carbon, Waste, Acetate, Oxygen */
     double *gr1, *gr2;         /* GrowthRate1/2 */
     double *ph, *hydrox, *acetic, *buffer;
+    /* GrCarAer, GrCarAna, GrAceAer, qCarmnt, qAcemnt, pAcemnt, qOxymnt:
+     * read by nothing but the Environment writer, so kept for buffer 0
+     * (Environment) only; null in buffer 1 */
+    double* extra[7];
 };
 
 /* one buffer of the wall rows, per composite level, 4 species */
@@ -120,5 +124,11 @@ int bcg_kernel_config_generation();
 void bcg_kernel_config_changed();
 void nutrient_graphs_drop(bcg_ctx* c);
 int launch_move_grow(bcg_ctx* c, double dt, int group);
+/* output-step kernels queued on `s`: the colony as reference records
+ * (ctx.cu), mean_stress's 5 stress components per cell with the F_cw count
+ * added to `fcw` (mech.cu), F_surf_tension's force, 3 per cell (mech.cu) */
+void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s);
+void launch_mean_stress(bcg_ctx* c, double* stress, unsigned long long* fcw, cudaStream_t s);
+void launch_surface_force(bcg_ctx* c, double* force, cudaStream_t s);
 int mg_tune_smoother(bcg_ctx* c, int* choice);
 int mg_kernel_attributes();

@@ -903,6 +903,35 @@ __global__ void k_mean_stress(int n, const CellRec* __restrict__ rec, const int*
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(fcw_count, v);
 }
 
+void launch_mean_stress(bcg_ctx* c, double* stress, unsigned long long* fcw, cudaStream_t s)
+{
+    if (c->n <= 0) return;
+    k_mean_stress<<<(c->n + 127) / 128, 128, 0, s>>>(c->n, c->rec[c->cur], c->nbr, c->ncount, field_ptrs(c),
+                                                     mech_params(c), stress, nullptr, fcw, c->status);
+    c->launches++;
+}
+
+/* F_surf_tension's force on every cell (Forces.cpp:209-317), the cell
+ * line's three force columns in the initial output block
+ * (Simulation.cpp:229-238) */
+__global__ void k_surface_force(int n, const CellRec* __restrict__ rec, FieldPtrs fp, MechParams mp,
+                                double* __restrict__ force)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Cst c = load_cst(&rec[i]);
+    V3 F, T;
+    surface_tension(c, avg_pq(c.p, c.q), fp, mp, F, T);
+    force[3 * (size_t)i] = F.x; force[3 * (size_t)i + 1] = F.y; force[3 * (size_t)i + 2] = F.z;
+}
+
+void launch_surface_force(bcg_ctx* c, double* force, cudaStream_t s)
+{
+    if (c->n <= 0) return;
+    k_surface_force<<<(c->n + 127) / 128, 128, 0, s>>>(c->n, c->rec[c->cur], field_ptrs(c), mech_params(c), force);
+    c->launches++;
+}
+
 extern "C" int bcg_mean_stress(bcg_ctx* c, double* stress, double* fnet, int64_t* fcw_calls)
 {
     if (!c || !stress) return BCG_E_ARG;

@@ -9,7 +9,10 @@
  * and reads the row this sweep wrote (the reference's 1-thread order).
  * Buffers swap after every sweep.  The acetate buffer solve, whose results
  * (pH, Hydrox, Acetic, Buffer) feed nothing else, runs only in the last two
- * sweeps of a call: those are the values that survive in each buffer.
+ * sweeps of a call: those are the values that survive in each buffer.  The
+ * same holds for the growth-rate components and maintenance rates
+ * (GrCarAer .. qOxymnt), which only the Environment writer reads; they are
+ * stored for Environment (buffer 0) in the last sweep that writes it.
  */
 #include "ctx.cuh"
 #include "mg.cuh"
@@ -98,12 +101,17 @@ static EnvP envp(bcg_ctx* c, int b)
     return p;
 }
 struct WallP { const double *C, *W, *O, *A; };
+/* Environment's GrCarAer, GrCarAna, GrAceAer, qCarmnt, qAcemnt, pAcemnt,
+ * qOxymnt (Nutrients.cpp:328-344); all null when the sweep's current
+ * buffer is not Environment or its values do not survive the call */
+struct EnvX { double *gca, *gcn, *gaa, *qcm, *qam, *pam, *qom; };
 
 /* UpdateEnvironment_OxygenAcetate (Nutrients.cpp:200-506), crossFeeding = 0,
  * for x in [minx, maxx], z in [0, maxz] where DensityShiftP > DBL_EPSILON
  * (Multigrid.cpp:1037-1047). */
 __global__ void k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur, EnvP prev, WallP pw0,
-                         const double* __restrict__ inside, const double* __restrict__ ds, int diag, DevStatus* st)
+                         const double* __restrict__ inside, const double* __restrict__ ds, int diag, EnvX ex,
+                         DevStatus* st)
 {
     const int Z = n.Z;
     int id = blockIdx.x * blockDim.x + threadIdx.x;
@@ -152,6 +160,13 @@ __global__ void k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur, Env
         double gr = GrCarAer + GrCarAna + GrAceAer;
         cur.gr1[id] = gr;
         cur.gr2[id] = gr;
+        if (ex.gca) {
+            ex.qcm[id] = n.q_car_aer_nt * mn((Cgr / n.g1s), 1.0) * fCgr_aer * fOgr + n.q_car_ana_nt * mn((Cgr / n.g2s), 1.0) * (1 - fOgr);
+            ex.qam[id] = n.q_ace_aer_nt * mn((Agr / n.g3s), 1.0) * (1 - fCgr_aer) * fOgr;
+            ex.pam[id] = n.p_ace_ana_nt * mn((Cgr / n.g2s), 1.0) * (1 - fOgr);
+            ex.qom[id] = n.q_o2_car_nt * mn((Cgr / n.g1s), 1.0) * fCgr_aer * fOgr + n.q_o2_ace_nt * mn((Agr / n.g3s), 1.0) * (1 - fCgr_aer) * fOgr;
+            ex.gca[id] = GrCarAer; ex.gcn[id] = GrCarAna; ex.gaa[id] = GrAceAer;
+        }
         if (!(x > 2)) { dev_error(st, BCG_E_NEED_MORE_BOXES, x); return; }
         const double c0C = prev.C[id], c0W = prev.W[id], c0A = prev.A[id], c0O = prev.O[id];
         const size_t up = IXZ(x, z + 1);
@@ -318,11 +333,16 @@ static void run_sweeps(bcg_ctx* c, int nsweeps, int& ce, int& cwb, int& count, i
         WallAll cw = wall_all(c, cwb), pw = wall_all(c, cwb ^ 1);
         WallP pw0 = {pw.C[0], pw.W[0], pw.O[0], pw.A[0]};
         int diag = j >= diag_from;
+        EnvX ex = {};
+        if (diag && ce == 0) {
+            double* const* x = c->env[0].extra;
+            ex = EnvX{x[0], x[1], x[2], x[3], x[4], x[5], x[6]};
+        }
         if (count % 2 == 0) {
             k_wall<<<gwal, 256, 0, c->stream>>>(n, cur, ag, cw, pw, c->inside);
-            k_colony<<<gcol, 256, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, diag, c->status);
+            k_colony<<<gcol, 256, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, diag, ex, c->status);
         } else {
-            k_colony<<<gcol, 256, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, diag, c->status);
+            k_colony<<<gcol, 256, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, diag, ex, c->status);
             k_wall<<<gwal, 256, 0, c->stream>>>(n, cur, ag, cw, pw, c->inside);
         }
         c->launches += 2;

@@ -22,6 +22,9 @@ struct bcg_sim {
     double t, dt;
     double next_out, next_update, hd_next_update, hd_update_time;
     bool update_flag, hd_update_flag;
+    bool out_flag;                 /* OutFlag, Simulation.cpp:56, 418 */
+    int koutput;                   /* output step id, Simulation.cpp:251 */
+    bcg_writer* writer;            /* writes the output steps when set */
     bool reference_cadence;
     int vcycles_per_step;
     bool first_step;
@@ -64,6 +67,9 @@ extern "C" int bcg_sim_create(const bcg_params* p, const bcg_cell* cells, int n,
     s->hd_update_time = p->update_time / 10.0;
     s->update_flag = true;
     s->hd_update_flag = true;
+    s->out_flag = false;           /* the initial block consumed the first OutFlag */
+    s->koutput = 0;
+    s->writer = nullptr;
     s->reference_cadence = true;
     s->vcycles_per_step = 0;
     s->first_step = true;
@@ -82,6 +88,14 @@ extern "C" int bcg_sim_destroy(bcg_sim* s)
 
 extern "C" bcg_ctx* bcg_sim_ctx(bcg_sim* s) { return s ? s->ctx : nullptr; }
 
+extern "C" int bcg_sim_set_writer(bcg_sim* s, bcg_writer* w, int write_initial)
+{
+    if (!s) return BCG_E_ARG;
+    s->writer = w;
+    if (w && write_initial) return bcg_output_initial(w, s->ctx, s->t);
+    return BCG_OK;
+}
+
 extern "C" int bcg_sim_set_step_mode(bcg_sim* s, int field_cadence_reference, int vcycles_per_step)
 {
     if (!s || vcycles_per_step < 0) return BCG_E_ARG;
@@ -97,8 +111,8 @@ static int sim_advance(bcg_sim* s, size_t base, int done, int rc)
     s->divisions += done;
     if (rc) return rc;
     s->t += s->dt;
-    bool out = (s->next_out <= 0);
-    s->next_out = (out ? s->P.output_time : s->next_out) - s->dt;
+    s->out_flag = (s->next_out <= 0);
+    s->next_out = (s->out_flag ? s->P.output_time : s->next_out) - s->dt;
     s->update_flag = (s->next_update <= 0);
     s->next_update = (s->update_flag ? s->P.update_time : s->next_update) - s->dt;
     s->hd_update_flag = (s->hd_next_update <= 0);
@@ -115,11 +129,16 @@ static void sim_draws(bcg_sim* s, int nd, int64_t calls)
     for (int i = 0; i < 9 * nd; i++) s->draws[i] = frand(&s->rng);
 }
 
-/* One iteration of while (t <= t_max), Simulation.cpp:254-431, without the
- * output block. */
+/* One iteration of while (t <= t_max), Simulation.cpp:254-431.  In the
+ * reference cadence an output step (OutFlag) runs mean_stress on every cell
+ * before MoveCell, whose F_cw draws the host skips, and with a writer
+ * attached writes the step's files (Simulation.cpp:316-327, 340-372) and
+ * the lineage lines (Simulation.cpp:392). */
 static int sim_step(bcg_sim* s)
 {
     int rc;
+    const bool out = s->reference_cadence && s->out_flag;
+    int64_t stress_calls = 0;
     if (s->reference_cadence) {
         if (s->update_flag) {
             s->update_flag = false;
@@ -141,14 +160,28 @@ static int sim_step(bcg_sim* s)
         if (s->vcycles_per_step > 0 && (rc = bcg_mg_solve(s->ctx, s->vcycles_per_step))) return rc;
     }
     s->first_step = false;
+    if (out) {
+        rc = s->writer ? bcg_output_cells(s->writer, s->ctx, s->koutput, s->t, &stress_calls)
+                       : bcg_int_stress_draws(s->ctx, &stress_calls);
+        if (rc) return rc;
+    }
     int nd = 0;
     int64_t calls = 0;
     if ((rc = bcg_move_grow(s->ctx, s->dt, &nd, &calls))) return rc;
-    sim_draws(s, nd, calls);
+    if (out) {
+        s->out_flag = false;
+        if (s->writer && (rc = bcg_output_fields(s->writer, s->ctx, s->koutput, s->t, s->dt))) return rc;
+        s->koutput++;
+    }
+    sim_draws(s, nd, stress_calls + calls);
     size_t base = s->lineage.size();
     s->lineage.resize(base + 2 * (size_t)(nd > 0 ? nd : 0));
     int done = 0;
     rc = bcg_divide(s->ctx, s->draws.data(), nd, s->t, &done, nd > 0 ? s->lineage.data() + base : nullptr);
+    if (s->writer && done > 0) {
+        int lrc = bcg_writer_lineage(s->writer, s->lineage.data() + base, done);
+        if (lrc && !rc) rc = lrc;
+    }
     return sim_advance(s, base, done, rc);
 }
 

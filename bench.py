@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-mg-tol", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-members", type=int, default=64)
+    ap.add_argument("--no-output", action="store_true", help="skip the output-step measurement")
     ap.add_argument("--smoother-warps", type=int, default=0,
                     help="pin the agar smoother's resident-warp target instead of autotuning it (profiling)")
     return ap.parse_args()
@@ -194,6 +195,63 @@ def ensemble_bench(lib, args, steps=5, warmup=2):
             "steps": steps, "vcycles_per_step": args.vcycles,
             "ensemble_cell_steps_per_s": work_ens / t_ens, "sequential_cell_steps_per_s": work_seq / t_seq,
             "speedup": (work_ens / t_ens) / (work_seq / t_seq), "timing": "host wall clock, device synchronised"}
+
+
+def output_step_bench(lib, sim, ctx, p, stream, steps=100):
+    """One output step of the colony through the asynchronous writer (all of
+    Cells, Restart, Density, Environment, AgarField, WallField in the
+    reference's formats, under a temporary directory) while the simulation
+    keeps stepping.  A first step, waited for, allocates the pinned staging;
+    the second is timed: the simulation thread's time to queue both halves,
+    the device time per step of the `steps` steps run while the host thread
+    writes, and the time until the files are on disk."""
+    import shutil
+    import tempfile
+    import torch
+    from baccolonygrowth_b200 import _abi
+    tmp = tempfile.mkdtemp(prefix="bcg_output_")
+    res = {"steps_while_writing": steps}
+    try:
+        if shutil.disk_usage(tmp).free < 6 * 2 ** 30:
+            return {"skipped": "less than 6 GiB free under %s" % tempfile.gettempdir()}
+        threads = max(1, (os.cpu_count() or 2) - 1)
+        w = ctypes.c_void_p()
+        _abi.check(lib.bcg_writer_create(tmp.encode(), 0, threads, 2, ctypes.byref(w)), "bcg_writer_create")
+        fcw = ctypes.c_int64()
+        try:
+            for rep in range(2):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                _abi.check(lib.bcg_output_cells(w, ctx, 0, 0.0, ctypes.byref(fcw)), "bcg_output_cells")
+                _abi.check(lib.bcg_output_fields(w, ctx, 0, 0.0, p.dt), "bcg_output_fields")
+                t1 = time.perf_counter()
+                if rep == 0:
+                    _abi.check(lib.bcg_writer_wait(w), "bcg_writer_wait")
+                    res["first_step_s"] = time.perf_counter() - t0
+                    continue
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                _abi.check(lib.bcg_sim_run(sim, steps), "steps while writing")
+                e1.record(stream)
+                torch.cuda.synchronize()
+                t2 = time.perf_counter()
+                _abi.check(lib.bcg_writer_wait(w), "bcg_writer_wait")
+                t3 = time.perf_counter()
+                res.update(queue_ms=(t1 - t0) * 1e3, ms_per_step_while_writing=e0.elapsed_time(e1) / steps,
+                           steps_done_s=t2 - t0, write_s=t3 - t0)
+        finally:
+            lib.bcg_writer_destroy(w)
+        nbytes = 0
+        for root, _, files in os.walk(tmp):
+            nbytes += sum(os.path.getsize(os.path.join(root, f)) for f in files)
+        res.update(bytes=nbytes, write_gb_s=nbytes / res["write_s"] / 1e9, format_threads=threads)
+        return res
+    except Exception as e:      # reported, not required
+        res["error"] = str(e)
+        return res
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def measured_peaks():
@@ -392,6 +450,9 @@ def b200_arm(args):
     _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
     n_now = ctypes.c_int()
     lib.bcg_num_cells(ctx, ctypes.byref(n_now))
+    out_step = None
+    if not args.no_output and world == 1:
+        out_step = output_step_bench(lib, sim, ctx, p, stream)
     lib.bcg_sim_destroy(sim)
 
     # end to end through the C ABI with host buffers: upload of the colony
@@ -525,6 +586,7 @@ def b200_arm(args):
         "mg_dof_per_s": dof * args.vcycles / (mg_ms / 1e3) if mg_ms > 0 else None,
         "mg_tolerance_solve": mg_tol,
         "ensemble": ens,
+        "output_step": out_step,
         "kernel_ms_per_step": timers,
         "divisions": d_.value,
         "roofline": roof,

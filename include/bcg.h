@@ -7,9 +7,10 @@
  * makes into Neighbours / Forces / Integrate / grow / Cells / Compute /
  * Nutrients / Multigrid.  All colony and field state lives on one GPU in
  * structure-of-arrays form inside a bcg_ctx; the host keeps the glibc rand()
- * stream, the output/restart files and the loop flags, exactly as the
- * reference does.  Every entry point returns a bcg_status (0 = OK); no entry
- * point aborts the process, and no kernel traps.
+ * stream and the loop flags, exactly as the reference does; the output
+ * files are written from device snapshots by a host thread (bcg_writer).
+ * Every entry point returns a bcg_status (0 = OK); no entry point aborts
+ * the process, and no kernel traps.
  *
  * Citations are "file:line" inside AgentBasedModel-BacColonyGrowth/.
  */
@@ -39,7 +40,9 @@ typedef enum bcg_status {
     BCG_E_TIMEOUT = 8,          /* a bounded device wait gave up                  */
     BCG_E_UNSUPPORTED = 9,      /* parameter combination the reference leaves undefined */
     BCG_E_NEED_MORE_BOXES = 10, /* colony too close to the grid edge, Nutrients.cpp:360 */
-    BCG_E_NO_DEVICE = 11        /* no CUDA device / kernels not loadable          */
+    BCG_E_NO_DEVICE = 11,       /* no CUDA device / kernels not loadable          */
+    BCG_E_IO = 12               /* an output file or directory could not be written,
+                                   "Can't open output file.", InputOutput.cpp:113-270 */
 } bcg_status;
 
 /* ------------------------------------------------------------------ */
@@ -242,7 +245,17 @@ typedef enum bcg_field_id {
     BCG_F_MG_ERR_ACETATE = 37,
     BCG_F_DENSITY = 38,       /* Density (BoxAverage of RoughDensity)      */
     BCG_F_ROUGH_DENSITY = 39, /* RoughDensity (GetDensity)                 */
-    BCG_F_COUNT = 40
+    BCG_F_ENV_HYDROX = 40,    /* Environment.Hydrox, Acetic, Buffer         */
+    BCG_F_ENV_ACETIC = 41,    /*   (acetateBufferSolve, Nutrients.cpp:806-855) */
+    BCG_F_ENV_BUFFER = 42,
+    BCG_F_ENV_GR_CAR_AER = 43, /* Environment.GrCarAer, GrCarAna, GrAceAer */
+    BCG_F_ENV_GR_CAR_ANA = 44, /*   (Nutrients.cpp:342-344)                */
+    BCG_F_ENV_GR_ACE_AER = 45,
+    BCG_F_ENV_Q_CAR_MNT = 46,  /* Environment.qCarmnt, qAcemnt, pAcemnt,   */
+    BCG_F_ENV_Q_ACE_MNT = 47,  /*   qOxymnt (Nutrients.cpp:328-331)        */
+    BCG_F_ENV_P_ACE_MNT = 48,
+    BCG_F_ENV_Q_OXY_MNT = 49,
+    BCG_F_COUNT = 50
 } bcg_field_id;
 
 /* Number of doubles of a field at a level (x-major, z fastest, matching
@@ -417,6 +430,112 @@ int bcg_mean_stress(bcg_ctx* ctx, double* stress, double* fnet, int64_t* fcw_cal
 int bcg_mean_stress_noalloc(bcg_ctx* ctx, double* stress, double* fnet, int64_t* fcw_calls);
 
 /* ------------------------------------------------------------------ */
+/* Output steps in the reference's on-disk formats.                      */
+/* Directory tree of CreateOutputFiles (InputOutput.cpp:42-271):         */
+/*   <dir>/<Name>/<id>.txt for Name in Cells, Restart, RoughDensity,     */
+/*   RoughDensity1, RoughDensity2, Density, Density1, Density2,          */
+/*   WallDensity, WallDensity1, WallDensity2, RoughHeight, Height,       */
+/*   Normal, Environment, AgarField, WallField; <dir>/lineage/0.txt      */
+/*   (CreateOutputFileLineage, InputOutput.cpp:13-33).  The reference    */
+/*   leaves all but Cells, Restart, Density, Environment, AgarField and  */
+/*   WallField empty (their writers are commented out in Simulation.cpp), */
+/*   and so does this library.                                           */
+/* Contents:                                                             */
+/*   Cells       one line per cell, Output (InputOutput.cpp:799-817)     */
+/*   Restart     {t, dt, Cell[n]} raw, SaveCells (InputOutput.cpp:434-448) */
+/*   Density     DensityShiftP, Array3D<double>::Output(f, 1)            */
+/*               (Array.h:568-584)                                       */
+/*   Environment Array3D<LocalEnv>::Output(f, 1) (Array.h:931-1122):    */
+/*               the 17 members of LocalEnv listed in bcg_output_data.env */
+/*   AgarField   Array3D<LocalAga>::Append(f, 1) of every level          */
+/*               (Array.h:1447-1494): CarbonAgar, AcetateAgar, WasteAgar, */
+/*               OxygenAgar                                              */
+/*   WallField   Array2D<LocalAga>::Append(f) of every level             */
+/*               (Array.h:417-456), the same four members                */
+/* Numbers are printed with the reference's printf formats ("%6E\t" for  */
+/* fields, the 28-field line of Output for cells), so a file holds the   */
+/* same bytes as the reference's for the same values.                    */
+/* ------------------------------------------------------------------ */
+#define BCG_OUT_CELLS  1   /* create the step's files; write Cells/<id>.txt */
+#define BCG_OUT_FIELDS 2   /* write Restart, Density, Environment, AgarField, WallField */
+
+/* One output step's data on the host.  Field arrays are x-major with z
+ * fastest, as bcg_get_field returns them (Array3D's own order with
+ * box_y = 1).  The reference's MG path never writes FieldAgar's WasteAgar,
+ * which keeps its initial 0 (Nutrients.h:66-74); a NULL agar entry prints
+ * zeros. */
+typedef struct bcg_output_data {
+    double t;                     /* time printed on every cell line            */
+    double dt;                    /* second double of the restart header        */
+    int32_t n_cells;              /* cells printed to Cells/<id>.txt            */
+    int32_t force_stride;         /* doubles per cell in cell_force (>= 3)      */
+    const bcg_cell* cells;        /* old_cells, before MoveCell                  */
+    const double* cell_force;     /* the 3 printed per cell: T.xx, T.yy, T.zz of
+                                     mean_stress (bcg_mean_stress's stride 5), or
+                                     Fnet of F_surf_tension in the initial block */
+    int32_t n_restart;            /* cells saved to Restart/<id>.txt; -1 leaves
+                                     the file empty (the initial block)          */
+    int32_t levels;               /* maxLevelsMG                                 */
+    const bcg_cell* restart_cells;/* new_cells, after MoveCell/GrowCell          */
+    int32_t box_x, box_z, box_z_agar, reserved;
+    const double* density;        /* DensityShiftP (box_x*box_z)                 */
+    const double* env[17];        /* Environment in file order: Carbon, Acetate,
+                                     Waste, Oxygen, GrowthRate1, GrowthRate2,
+                                     GrCarAer, GrCarAna, GrAceAer, pH, Hydrox,
+                                     Buffer, Acetic, qCarmnt, qAcemnt, pAcemnt,
+                                     qOxymnt (box_x*box_z each)                  */
+    const double* const* agar;    /* 4 per level, level-major: CarbonAgar,
+                                     AcetateAgar, WasteAgar, OxygenAgar of
+                                     FieldAgar[l] (box_x*box_z_agar each)        */
+    const double* const* wall;    /* 4 per level, the same members of
+                                     FieldWall[l] (box_x each)                   */
+} bcg_output_data;
+
+/* Write one output step's files from host data, synchronously, with
+ * `threads` formatting threads (0 = all hardware threads).  `what` is a
+ * mask of BCG_OUT_*: BCG_OUT_CELLS creates the step's whole tree the way
+ * CreateOutputFiles does (Cells/<id>.txt opened for append when `append`,
+ * every other file truncated); BCG_OUT_FIELDS then fills the field files
+ * and Restart.  Missing directories are created (mode 0775).  BCG_E_IO
+ * when a directory or file cannot be created or written.  Needs no GPU. */
+int bcg_write_output(const char* dir, int output_id, int what, int append,
+                     const bcg_output_data* d, int threads);
+
+/* Asynchronous output writer.  Each bcg_output_* call snapshots what the
+ * step writes on the context's stream (one gather kernel into a device
+ * staging buffer), queues one device-to-host copy of it on the writer's
+ * own copy stream, and hands the step to the writer's host thread, which
+ * waits for the copy, formats with `threads` threads and writes the files
+ * while the GPU goes on with the next steps.  At most `max_pending` steps
+ * (>= 1) are queued; a further call waits for the oldest.  All contexts
+ * given to one writer are on one device.  An error of the host thread
+ * (BCG_E_IO) is returned by the next call and by bcg_writer_wait.
+ * bcg_writer_create truncates <dir>/lineage/0.txt (CellMD3D.cpp:78). */
+typedef struct bcg_writer bcg_writer;
+int bcg_writer_create(const char* dir, int append, int threads, int max_pending, bcg_writer** out);
+/* Wait until every queued step is on disk; the first error, if any. */
+int bcg_writer_wait(bcg_writer* w);
+/* Waits, then frees the writer. */
+int bcg_writer_destroy(bcg_writer* w);
+/* The initial output block, Simulation.cpp:185-244, as output step 0: the
+ * fields, then one line per cell with F_surf_tension's force
+ * (Forces.cpp:209) in the three stress columns; Restart/0.txt stays empty. */
+int bcg_output_initial(bcg_writer* w, bcg_ctx* ctx, double t);
+/* First half of an output step, before MoveCell (Simulation.cpp:316-327):
+ * CreateOutputFiles(output_id) and one line per cell with mean_stress's
+ * T.xx, T.yy, T.zz.  mean_stress calls F_cw, so this reports in fcw_calls
+ * the rand() draws the host skips (as after bcg_mean_stress); it waits for
+ * that count, not for the copy or the files. */
+int bcg_output_cells(bcg_writer* w, bcg_ctx* ctx, int output_id, double t, int64_t* fcw_calls);
+/* Second half, after bcg_move_grow and before bcg_divide
+ * (Simulation.cpp:340-372): Restart (the moved, grown, undivided cells,
+ * t and dt) and the field files.  Does not wait for the GPU. */
+int bcg_output_fields(bcg_writer* w, bcg_ctx* ctx, int output_id, double t, double dt);
+/* Append lineage pairs (parent, daughter) to <dir>/lineage/0.txt as
+ * "%d %d\n" lines (Simulation.cpp:392), in queue order with the steps. */
+int bcg_writer_lineage(bcg_writer* w, const int* pairs, int n_pairs);
+
+/* ------------------------------------------------------------------ */
 /* C++ host loop (rewrite of SimSingleThread, Simulation.cpp:42-434)     */
 /* ------------------------------------------------------------------ */
 typedef struct bcg_sim bcg_sim;
@@ -427,9 +546,17 @@ int bcg_sim_create(const bcg_params* p, const bcg_cell* cells, int n, uint32_t s
                    int run_initial_fields, bcg_sim** out);
 int bcg_sim_destroy(bcg_sim* sim);
 /* Advance `steps` iterations of the while loop (Simulation.cpp:254-431),
- * honouring UpdateFlag / HeightDensityUpdateFlag; output steps are skipped
- * (OutFlag handling stays with the caller). */
+ * honouring UpdateFlag / HeightDensityUpdateFlag and OutFlag: an output
+ * step runs mean_stress on every cell before MoveCell and skips its
+ * rand() draws, as the reference does; with a writer attached it also
+ * writes the step's files and the lineage lines. */
 int bcg_sim_run(bcg_sim* sim, int steps);
+/* Attach (or, with NULL, detach) an output writer; the simulation does not
+ * own it.  write_initial also writes the initial block's output
+ * (Simulation.cpp:185-244) now, as output step 0; call it before the first
+ * step.  Later output steps count from 0 again (koutput, Simulation.cpp:251,
+ * 319), overwriting step 0 like the reference. */
+int bcg_sim_set_writer(bcg_sim* sim, bcg_writer* w, int write_initial);
 bcg_ctx* bcg_sim_ctx(bcg_sim* sim);
 int bcg_sim_time(bcg_sim* sim, double* t, int* n_cells, int64_t* divisions);
 /* Lineage pairs recorded so far (parent, daughter), up to capacity pairs. */

@@ -1719,6 +1719,16 @@ long orc_field(orc_state* s, int field, int level, double* buf, long n, int writ
     case BCG_F_ENV_GROWTH1: ACC(X * Z, s->env[i].GrowthRate1); return cnt;
     case BCG_F_ENV_GROWTH2: ACC(X * Z, s->env[i].GrowthRate2); return cnt;
     case BCG_F_ENV_PH: ACC(X * Z, s->env[i].pH); return cnt;
+    case BCG_F_ENV_HYDROX: ACC(X * Z, s->env[i].Hydrox); return cnt;
+    case BCG_F_ENV_ACETIC: ACC(X * Z, s->env[i].Acetic); return cnt;
+    case BCG_F_ENV_BUFFER: ACC(X * Z, s->env[i].Buffer); return cnt;
+    case BCG_F_ENV_GR_CAR_AER: ACC(X * Z, s->env[i].GrCarAer); return cnt;
+    case BCG_F_ENV_GR_CAR_ANA: ACC(X * Z, s->env[i].GrCarAna); return cnt;
+    case BCG_F_ENV_GR_ACE_AER: ACC(X * Z, s->env[i].GrAceAer); return cnt;
+    case BCG_F_ENV_Q_CAR_MNT: ACC(X * Z, s->env[i].qCarmnt); return cnt;
+    case BCG_F_ENV_Q_ACE_MNT: ACC(X * Z, s->env[i].qAcemnt); return cnt;
+    case BCG_F_ENV_P_ACE_MNT: ACC(X * Z, s->env[i].pAcemnt); return cnt;
+    case BCG_F_ENV_Q_OXY_MNT: ACC(X * Z, s->env[i].qOxymnt); return cnt;
     case BCG_F_OLDENV_CARBON: ACC(X * Z, s->oenv[i].Carbon); return cnt;
     case BCG_F_OLDENV_WASTE: ACC(X * Z, s->oenv[i].Waste); return cnt;
     case BCG_F_OLDENV_OXYGEN: ACC(X * Z, s->oenv[i].Oxygen); return cnt;

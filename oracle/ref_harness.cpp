@@ -14,6 +14,7 @@
  */
 #include <omp.h>
 #include <stdio.h>
+#include <sys/stat.h>
 #include <string.h>
 #include <stdlib.h>
 #include <math.h>
@@ -37,6 +38,7 @@
 #include "Compute.h"
 #include "Forces.h"
 #include "Multigrid.h"
+#include "InputOutput.h"
 #undef private
 
 #include "../include/bcg.h"
@@ -82,6 +84,8 @@ struct RefState {
     double t = 0, dt = 0;
     double NextOutTime, NextUpdateTime, HeightDensityNextUpdateTime, HeightDensityUpdateTime;
     bool UpdateFlag = true, HeightDensityUpdateFlag = true;
+    bool OutFlag = false;          /* false once the initial block has run, Simulation.cpp:243 */
+    int koutput = 0;
     long long lineage_n = 0;
     int* lineage = nullptr; int lineage_cap = 0;
     int last_numDivide = 0;
@@ -431,8 +435,8 @@ int ref_loop_step(int* lineage)
     ref_move_grow(S.dt, nullptr, nullptr);
     int done = ref_divide(S.t, lineage);
     S.t += S.dt;
-    bool OutFlag = (S.NextOutTime <= 0);
-    S.NextOutTime = (OutFlag ? OutputTime : S.NextOutTime) - S.dt;
+    S.OutFlag = (S.NextOutTime <= 0);
+    S.NextOutTime = (S.OutFlag ? OutputTime : S.NextOutTime) - S.dt;
     S.UpdateFlag = (S.NextUpdateTime <= 0);
     S.NextUpdateTime = (S.UpdateFlag ? UpdateTime : S.NextUpdateTime) - S.dt;
     S.HeightDensityUpdateFlag = (S.HeightDensityNextUpdateTime <= 0);
@@ -453,6 +457,165 @@ long long ref_mean_stress(double* stress, double* fnet)
         if (fnet) { fnet[3 * i] = F.x; fnet[3 * i + 1] = F.y; fnet[3 * i + 2] = F.z; }
     }
     return g_rand_calls - r0;
+}
+
+/* ---- output steps, through the reference's own writers -------------------- */
+static OutputFiles g_files;
+
+/* The files CreateOutputFiles opens (InputOutput.cpp:42-271), opened here.
+ * The reference builds each name with sprintf(name, "%s/%d", name, id),
+ * whose source and destination overlap; with this machine's glibc that
+ * yields "/<id>" and every file of the step lands on "/<id>.txt", so the
+ * harness never calls it.  The names below are the intended
+ * <dir>/<Name>/<id>.txt; the writers that fill the files are the
+ * reference's own. */
+static int open_step_files(const char* dir, int id, bool append, OutputFiles& F)
+{
+    mkdir(dir, S_IRWXU | S_IRWXG | S_IROTH | S_IXOTH);
+    const char* names[17] = {"Cells", "Restart", "RoughDensity", "RoughDensity1", "RoughDensity2", "Density",
+                             "Density1", "Density2", "WallDensity", "WallDensity1", "WallDensity2", "RoughHeight",
+                             "Height", "Normal", "Environment", "AgarField", "WallField"};
+    FILE** slots[17] = {&F.cells, &F.restart, &F.roughDensity, &F.roughDensity1, &F.roughDensity2, &F.density,
+                        &F.density1, &F.density2, &F.walldensity, &F.walldensity1, &F.walldensity2, &F.roughheight,
+                        &F.height, &F.normal, &F.env, &F.aga, &F.wal};
+    char path[1024];
+    for (int k = 0; k < 17; k++) {
+        snprintf(path, sizeof path, "%s/%s", dir, names[k]);
+        mkdir(path, S_IRWXU | S_IRWXG | S_IROTH | S_IXOTH);
+        snprintf(path, sizeof path, "%s/%s/%d.txt", dir, names[k], id);
+        *slots[k] = fopen(path, (k == 0 && append) ? "a" : "w");
+        if (!*slots[k]) {
+            for (int j = 0; j < k; j++) fclose(*slots[j]);
+            return -1;
+        }
+    }
+    return 0;
+}
+
+/* First half of an output step, Simulation.cpp:316-327: CreateOutputFiles
+ * and one Output line per cell with mean_stress's tensor, at time t.
+ * Returns the rand() draws made, or -1 when the files cannot be opened. */
+long long ref_output_cells(const char* dir, int id, double t, int append)
+{
+    if (open_step_files(dir, id, append != 0, g_files)) return -1;
+    long long r0 = g_rand_calls;
+    Tensor T;
+    DoubleCoord F;
+    for (int i = 0; i < S.N; i++) {
+        mean_stress(S.old_cells[i], S.old_cells, S.nbr[i], *S.grid, *S.Wall, *S.Height, *S.Normal, T, F);
+        Output(g_files.cells, i, t, S.old_cells[i], T);
+    }
+    return g_rand_calls - r0;
+}
+
+/* The same first half with given stress columns (T.xx, T.yy, T.zz from
+ * `stress`, `stride` doubles per cell) in place of mean_stress: the
+ * reference's Output on arbitrary values, for format checks. */
+int ref_output_cells_given(const char* dir, int id, double t, int append, const double* stress, int stride)
+{
+    if (open_step_files(dir, id, append != 0, g_files)) return -1;
+    for (int i = 0; i < S.N; i++) {
+        Tensor T(stress[(size_t)i * stride], stress[(size_t)i * stride + 1], stress[(size_t)i * stride + 2], 0.0, 0.0);
+        Output(g_files.cells, i, t, S.old_cells[i], T);
+    }
+    return 0;
+}
+
+/* overwrite new_cells (the array SaveCells writes on an output step) */
+int ref_set_new_cells(const bcg_cell* cells, int n)
+{
+    if (n > maxCells) return BCG_E_ARG;
+    memcpy(S.new_cells, cells, sizeof(Cell) * (size_t)n);
+    return 0;
+}
+
+/* Second half, Simulation.cpp:342-374 (new_cells as MoveCell/GrowCell left
+ * them), then CloseOutputFiles. */
+void ref_output_fields(double t, double dt)
+{
+    SaveCells(g_files.restart, S.new_cells, S.N, t, dt);
+    S.DensityShiftP->Output(g_files.density, 1);
+    S.Env->Output(g_files.env, 1);
+    for (int level = 0; level < maxLevelsMG; level++) {
+        S.FieldAgar[level]->Append(g_files.aga, 1);
+        S.FieldWall[level]->Append(g_files.wal);
+    }
+    CloseOutputFiles(g_files);
+}
+
+/* The initial block's output, Simulation.cpp:185-244 (step 0). */
+void ref_output_initial(const char* dir, double t, int append)
+{
+    OutputFiles F;
+    if (open_step_files(dir, 0, append != 0, F)) return;
+    S.DensityShiftP->Output(F.density, 1);
+    S.Env->Output(F.env, 1);
+    for (int level = 0; level < maxLevelsMG; level++) {
+        S.FieldAgar[level]->Append(F.aga, 1);
+        S.FieldWall[level]->Append(F.wal);
+    }
+    DoubleCoord Fnet;
+    for (int i = 0; i < S.N; i++) {
+        IntCoord XYAddress = S.grid->GetXY(S.grid->GetAddress(average(S.old_cells[i].Position)));
+        DoubleCoord T(0, 0, 0);
+        F_surf_tension(S.old_cells[i], *S.grid, XYAddress, *S.Height, *S.Normal, Fnet, T);
+        Output(F.cells, i, t, S.old_cells[i], Fnet);
+    }
+    fflush(F.cells);
+    CloseOutputFiles(F);
+}
+
+/* One iteration of the while loop with its output block
+ * (Simulation.cpp:256-431): writes the step's files under `dir` when
+ * OutFlag is set.  Returns the divisions done. */
+int ref_loop_step_out(const char* dir, int* lineage)
+{
+    if (S.UpdateFlag) {
+        S.UpdateFlag = false;
+        ref_update_density();
+        UpdateEnvArrayMG_OxygenAcetate(S.Env, S.oldEnv, S.FieldAgar, S.oldFieldAgar, S.FieldWall, S.oldFieldWall, *S.DensityShiftP, *S.Density1ShiftP, *S.Density2ShiftP, *S.WallDensityShiftP, *S.WallDensity1ShiftP, *S.WallDensity2ShiftP, S.minx, S.maxx, S.miny, S.maxy, S.maxz, *S.Height, *S.insideColonyDen, *S.mg);
+        getNeighbours(S.old_cells, S.N, *S.grid, S.nbr, S.maxNeighbours);
+    }
+    if (S.HeightDensityUpdateFlag) {
+        S.HeightDensityUpdateFlag = false;
+        ref_update_height();
+    }
+    const bool out = S.OutFlag;
+    if (out) ref_output_cells(dir, S.koutput++, S.t, 0);
+    ref_move_grow(S.dt, nullptr, nullptr);
+    if (out) {
+        S.OutFlag = false;
+        ref_output_fields(S.t, S.dt);
+    }
+    int done = ref_divide(S.t, lineage);
+    S.t += S.dt;
+    S.OutFlag = (S.NextOutTime <= 0);
+    S.NextOutTime = (S.OutFlag ? OutputTime : S.NextOutTime) - S.dt;
+    S.UpdateFlag = (S.NextUpdateTime <= 0);
+    S.NextUpdateTime = (S.UpdateFlag ? UpdateTime : S.NextUpdateTime) - S.dt;
+    S.HeightDensityUpdateFlag = (S.HeightDensityNextUpdateTime <= 0);
+    S.HeightDensityNextUpdateTime = (S.HeightDensityUpdateFlag ? S.HeightDensityUpdateTime : S.HeightDensityNextUpdateTime) - S.dt;
+    return done;
+}
+
+/* F_surf_tension's force on every cell, as the initial block computes it
+ * (Simulation.cpp:231-236) */
+void ref_surface_forces(double* out)
+{
+    for (int i = 0; i < S.N; i++) {
+        IntCoord XYAddress = S.grid->GetXY(S.grid->GetAddress(average(S.old_cells[i].Position)));
+        DoubleCoord T(0, 0, 0), F(0, 0, 0);
+        F_surf_tension(S.old_cells[i], *S.grid, XYAddress, *S.Height, *S.Normal, F, T);
+        out[3 * i] = F.x; out[3 * i + 1] = F.y; out[3 * i + 2] = F.z;
+    }
+}
+
+/* the moved, grown cells of the last ref_move_grow (new_cells) */
+int ref_get_new_cells(bcg_cell* out, int cap)
+{
+    int n = S.N < cap ? S.N : cap;
+    memcpy(out, S.new_cells, sizeof(Cell) * (size_t)n);
+    return S.N;
 }
 
 double ref_time(void) { return S.t; }
@@ -492,6 +655,16 @@ long ref_field(int field, int level, double* buf, long n, int write)
     ENVF(BCG_F_ENV_GROWTH1, Env, GrowthRate1)
     ENVF(BCG_F_ENV_GROWTH2, Env, GrowthRate2)
     ENVF(BCG_F_ENV_PH, Env, pH)
+    ENVF(BCG_F_ENV_HYDROX, Env, Hydrox)
+    ENVF(BCG_F_ENV_ACETIC, Env, Acetic)
+    ENVF(BCG_F_ENV_BUFFER, Env, Buffer)
+    ENVF(BCG_F_ENV_GR_CAR_AER, Env, GrCarAer)
+    ENVF(BCG_F_ENV_GR_CAR_ANA, Env, GrCarAna)
+    ENVF(BCG_F_ENV_GR_ACE_AER, Env, GrAceAer)
+    ENVF(BCG_F_ENV_Q_CAR_MNT, Env, qCarmnt)
+    ENVF(BCG_F_ENV_Q_ACE_MNT, Env, qAcemnt)
+    ENVF(BCG_F_ENV_P_ACE_MNT, Env, pAcemnt)
+    ENVF(BCG_F_ENV_Q_OXY_MNT, Env, qOxymnt)
     ENVF(BCG_F_OLDENV_CARBON, oldEnv, Carbon)
     ENVF(BCG_F_OLDENV_WASTE, oldEnv, Waste)
     ENVF(BCG_F_OLDENV_OXYGEN, oldEnv, Oxygen)

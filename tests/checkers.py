@@ -102,6 +102,14 @@ def ref_lib():
         _proto(lib, "ref_loop_step", ctypes.c_int, [_PI])
         _proto(lib, "ref_time", ctypes.c_double, [])
         _proto(lib, "ref_mean_stress", ctypes.c_longlong, [_PD, _PD])
+        _proto(lib, "ref_output_cells", ctypes.c_longlong, [ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int])
+        _proto(lib, "ref_output_fields", None, [ctypes.c_double, ctypes.c_double])
+        _proto(lib, "ref_output_initial", None, [ctypes.c_char_p, ctypes.c_double, ctypes.c_int])
+        _proto(lib, "ref_loop_step_out", ctypes.c_int, [ctypes.c_char_p, _PI])
+        _proto(lib, "ref_get_new_cells", ctypes.c_int, [_VP, ctypes.c_int])
+        _proto(lib, "ref_surface_forces", None, [_PD])
+        _proto(lib, "ref_output_cells_given", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _PD, ctypes.c_int])
+        _proto(lib, "ref_set_new_cells", ctypes.c_int, [_VP, ctypes.c_int])
         _ref = lib
     return _ref
 
@@ -321,3 +329,38 @@ class Reference(_Model):
         st = np.zeros(5 * self.n_cells()); fn = np.zeros(3 * self.n_cells())
         calls = self.lib.ref_mean_stress(_abi.ptr(st, ctypes.c_double), _abi.ptr(fn, ctypes.c_double))
         return st.reshape(-1, 5), fn.reshape(-1, 3), calls
+
+    # ---- output steps through the reference's own writers ----------------
+    def output_cells(self, directory, output_id, t, append=False):
+        """CreateOutputFiles + mean_stress/Output per cell; returns rand() draws."""
+        return self.lib.ref_output_cells(str(directory).encode(), output_id, t, 1 if append else 0)
+
+    def output_fields(self, t, dt):
+        self.lib.ref_output_fields(t, dt)
+
+    def output_initial(self, directory, t, append=False):
+        self.lib.ref_output_initial(str(directory).encode(), t, 1 if append else 0)
+
+    def loop_step_out(self, directory):
+        lineage = np.zeros(2 * max(1, self.n_cells()), dtype=np.int32)
+        done = self.lib.ref_loop_step_out(str(directory).encode(), _abi.ptr(lineage, ctypes.c_int))
+        return lineage[:2 * done].reshape(-1, 2).copy()
+
+    def new_cells(self):
+        out = np.zeros(self.n_cells(), dtype=_abi.CELL_DTYPE)
+        self.lib.ref_get_new_cells(_abi.ptr(out), len(out))
+        return out
+
+    def surface_forces(self):
+        f = np.zeros(3 * max(1, self.n_cells()))
+        self.lib.ref_surface_forces(_abi.ptr(f, ctypes.c_double))
+        return f[:3 * self.n_cells()].reshape(-1, 3)
+
+    def output_cells_given(self, directory, output_id, t, stress, stride=5, append=False):
+        st = np.ascontiguousarray(stress, dtype=np.float64).reshape(-1)
+        return self.lib.ref_output_cells_given(str(directory).encode(), output_id, t, 1 if append else 0,
+                                               _abi.ptr(st, ctypes.c_double), stride)
+
+    def set_new_cells(self, cells):
+        cells = np.ascontiguousarray(cells)
+        return self.lib.ref_set_new_cells(_abi.ptr(cells), len(cells))

@@ -15,6 +15,11 @@ outputs:
                    V-cycles), then one nutrient update with one solve +
                    200 sweeps.
 
+  output_format.npz one output step of seeded arbitrary values (300 cells,
+                   a 40 x 6 colony grid, 2 agar levels of 40 x 5) and the
+                   17 files the reference's own writers (Output, SaveCells,
+                   the Array2D/Array3D writers) make of it.
+
 Usage:  python tests/golden/make_golden.py
 """
 import json
@@ -102,8 +107,29 @@ def fields():
     print("fields_small.npz: bbox", tuple(out["bbox"]))
 
 
+def output_format():
+    import tempfile
+    import output_ref
+    p, d = output_ref.random_step(20261203)
+    ref = checkers.Reference(p, seed=SEED)
+    step = 5
+    with tempfile.TemporaryDirectory() as tmp:
+        output_ref.reference_tree(ref, tmp, step, d)
+        files = output_ref.read_tree(tmp, step)
+    L = p.max_levels_mg
+    out = dict(params=json.dumps(p.as_dict()), step=step, t=d.t, dt=d.dt, cells=d.cells, force=d.force,
+               restart=d.restart, density=d.density, env=np.stack(d.env),
+               agar=np.stack([a for a in d.agar if a is not None]).reshape(L, 3, -1),
+               wall=np.stack(d.wall).reshape(L, 4, -1))
+    for name, b in files.items():
+        out["file_" + name] = np.frombuffer(b, dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "output_format.npz"), **out)
+    print("output_format.npz: %d cells, %d bytes of files" % (len(d.cells), sum(len(b) for b in files.values())))
+
+
 if __name__ == "__main__":
     if not checkers.have_ref():
         sys.exit("oracle/_ref/libbcgref.so is not built (make -C oracle ref)")
-    mech()
-    fields()
+    which = sys.argv[1:] or ["mech", "fields", "output_format"]
+    for name in which:
+        globals()[name]()

@@ -121,6 +121,15 @@ def test_nutrient_update(gpu):
         assert close(orc.field(F[f]), col.field(f), mask=m) <= 1e-11, f
     inside = orc.field(F["INSIDE"]) > 0.5
     assert close(orc.field(F["ENV_PH"]), col.field("ENV_PH"), mask=inside & m) <= 1e-9
+    for f in ("ENV_HYDROX", "ENV_ACETIC", "ENV_BUFFER"):
+        assert close(orc.field(F[f]), col.field(f), mask=inside & m) <= 1e-9, f
+    # the members only the Environment writer reads (Nutrients.cpp:328-344)
+    for f in ("ENV_GR_CAR_AER", "ENV_GR_CAR_ANA", "ENV_GR_ACE_AER", "ENV_Q_CAR_MNT", "ENV_Q_ACE_MNT",
+              "ENV_P_ACE_MNT", "ENV_Q_OXY_MNT"):
+        a, b = orc.field(F[f]), col.field(f)
+        assert close(a, b, mask=m) <= 1e-11, f
+        assert np.array_equal(a == 0, b == 0), f
+    assert np.abs(col.field("ENV_GR_CAR_AER")).max() > 0
     for l in range(p.max_levels_mg):
         wm = wall_mask(p, l)
         for f in ("WALLF_CARBON", "WALLF_WASTE", "WALLF_OXYGEN", "WALLF_ACETATE",
