@@ -338,10 +338,10 @@ __global__ void k_pack(int n, bcg_cell* __restrict__ out, const CellRec* __restr
     out[i] = c;
 }
 
-void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s)
+void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s, int moved)
 {
     if (c->n <= 0) return;
-    k_pack<<<(c->n + 255) / 256, 256, 0, s>>>(c->n, dst, c->rec[c->cur], c->soa);
+    k_pack<<<(c->n + 255) / 256, 256, 0, s>>>(c->n, dst, c->rec[moved ? c->cur ^ 1 : c->cur], c->soa);
     c->launches++;
 }
 
@@ -363,6 +363,7 @@ extern "C" int bcg_upload_cells(bcg_ctx* c, const bcg_cell* cells, int n)
     c->n = n;
     c->n_binned = 0;
     c->last_ndiv = 0;
+    c->move_pending = 0;
     return ctx_check_status(c);
 }
 

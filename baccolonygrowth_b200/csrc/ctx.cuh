@@ -76,6 +76,9 @@ struct bcg_ctx {
     int* div_order;        /* divisions grouped, ascending inside a group */
     int* div_grp;          /* (start, length) per group */
     int last_ndiv;
+    /* set by MoveCell/GrowCell, cleared by the division loop: meanwhile the
+     * moved, grown records (the reference's new_cells) are rec[cur ^ 1] */
+    int move_pending;
     /* status */
     DevStatus* status;     /* device */
     /* pinned host staging */
@@ -124,10 +127,10 @@ int bcg_kernel_config_generation();
 void bcg_kernel_config_changed();
 void nutrient_graphs_drop(bcg_ctx* c);
 int launch_move_grow(bcg_ctx* c, double dt, int group);
-/* output-step kernels queued on `s`: the colony as reference records
- * (ctx.cu), mean_stress's 5 stress components per cell with the F_cw count
+/* output-step kernels queued on `s`: the colony as reference records,
+ * old_cells or (moved != 0) new_cells (ctx.cu), mean_stress's 5 stress components per cell with the F_cw count
  * added to `fcw` (mech.cu), F_surf_tension's force, 3 per cell (mech.cu) */
-void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s);
+void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s, int moved);
 void launch_mean_stress(bcg_ctx* c, double* stress, unsigned long long* fcw, cudaStream_t s);
 void launch_surface_force(bcg_ctx* c, double* force, cudaStream_t s);
 int mg_tune_smoother(bcg_ctx* c, int* choice);

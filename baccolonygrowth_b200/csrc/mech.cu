@@ -452,6 +452,7 @@ int move_grow_finish(bcg_ctx* c, int* n_div, int64_t* fcw_calls)
 {
     int rc = ctx_check_status(c);
     if (rc) return rc;
+    c->move_pending = 1;
     int* hp = (int*)c->pinned;
     c->last_ndiv = hp[0];
     if (n_div) *n_div = hp[0];
@@ -820,6 +821,7 @@ int divide_finish(bcg_ctx* c, int* n_done, int* lineage)
         c->n += done;
     }
     c->cur ^= 1;
+    c->move_pending = 0;
     c->last_ndiv = 0;
     if (n_done) *n_done = done;
     return rc;

@@ -10,7 +10,8 @@
  *   - the colony as reference records (k_pack);
  *   - mean_stress's five stress components per cell, or F_surf_tension's
  *     force in the initial block;
- *   - the restart records (the moved, grown, undivided colony);
+ *   - the restart records (the moved, grown, undivided colony: the
+ *     second record buffer while a move waits for its division loop);
  *   - the field planes: DensityShiftP and the 17 Environment members by
  *     device-to-device copies; the agar levels as z-major rows straight out
  *     of the multigrid solution (rows 1..Box_z_agar, copyFromMG); the four
@@ -101,12 +102,14 @@ extern "C" int bcg_int_out_snapshot(bcg_ctx* c, const bcg_out_layout* L, void* h
     if (L->bytes) BCG_CUDA_TRY(cudaMallocAsync((void**)&d, L->bytes, s));
     if (stress) BCG_CUDA_TRY(cudaMemsetAsync(c->fcw_count, 0, sizeof(unsigned long long), s));
     if (L->what & BCG_OUT_CELLS) {
-        launch_pack_cells(c, (bcg_cell*)(d + L->off_cells), s);
+        launch_pack_cells(c, (bcg_cell*)(d + L->off_cells), s, 0);
         if (L->initial) launch_surface_force(c, (double*)(d + L->off_force), s);
         else launch_mean_stress(c, (double*)(d + L->off_force), c->fcw_count, s);
     }
     if (L->what & BCG_OUT_FIELDS) {
-        if (L->n_restart > 0) launch_pack_cells(c, (bcg_cell*)(d + L->off_restart), s);
+        /* SaveCells(new_cells): between MoveCell and the division loop the
+         * moved records are the other buffer */
+        if (L->n_restart > 0) launch_pack_cells(c, (bcg_cell*)(d + L->off_restart), s, c->move_pending);
         int rc = snapshot_fields(c, L, d);
         if (rc) return rc;
     }

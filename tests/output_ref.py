@@ -156,3 +156,29 @@ def restart_close(a, b, rel=1e-9):
         x, y = ca[f].astype(np.float64), cb[f].astype(np.float64)
         scale = max(np.abs(x).max() if x.size else 0.0, 1e-300)
         assert np.abs(x - y).max(initial=0.0) <= rel * scale, f
+
+
+def field_rows(text):
+    """The rows of a field file as a float array (one row per non-empty
+    line; each line holds Box_x values, each followed by a tab)."""
+    rows = [l for l in text.split(b"\n") if l]
+    return np.array([[float(v) for v in l.split(b"\t") if v] for l in rows])
+
+
+def density_close(a, b, bbox, rel=1e-9):
+    """Two Density files (rows z of Box_x values).  BoxAverage writes
+    DensityShiftP only inside the bounding box (Compute.cpp:669-738); outside
+    it the reference's array holds whatever its scratch memory held, which is
+    not compared.  Inside the box the printed values agree within one unit
+    of the last printed digit plus `rel` of the largest value; outside it
+    `a` must be 0."""
+    minx, maxx, maxz = bbox
+    assert a.count(b"\n") == b.count(b"\n")
+    ra, rb = field_rows(a), field_rows(b)
+    assert ra.shape == rb.shape
+    inside = np.zeros(ra.shape, dtype=bool)
+    inside[:maxz, minx:maxx] = True
+    scale = max(np.abs(rb[inside]).max(initial=0.0), 1e-300)
+    ulp = 10.0 ** (np.floor(np.log10(np.maximum(np.abs(rb), 1e-300))) - 6)
+    assert (np.abs(ra - rb)[inside] <= 1.0001 * ulp[inside] + rel * scale).all()
+    assert (ra[~inside] == 0).all()
