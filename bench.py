@@ -254,6 +254,30 @@ def output_step_bench(lib, sim, ctx, p, stream, steps=100):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def profiled_traffic(summary, workload):
+    """DRAM bytes (read + write) of one launch from the committed ncu
+    summary of the kernel (profiles/<summary>), when it was captured on this
+    workload; else None."""
+    path = os.path.join(ROOT, "profiles", summary)
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    if workload not in summary:
+        return None
+    unit = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    total = 0.0
+    for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+        for line in text.splitlines():
+            if line.startswith("- " + key + ":"):
+                v, u = line.split(":", 1)[1].split()[:2]
+                total += float(v) * unit.get(u, float("nan"))
+                break
+        else:
+            return None
+    return total
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -571,7 +595,9 @@ def b200_arm(args):
         sm_gbs = sm_bytes / (sm_ms / 1e3) / 1e9
         roof = {"kernel": "k_mg_smooth<double,3> (finest agar level, 3 fused zebra sweeps)", "bound": "hbm",
                 "achieved": sm_gbs, "peak": peak_gbs, "unit": "GB/s", "frac": sm_gbs / peak_gbs,
-                "traffic": None, "peak_source": peak_src, "algorithmic_bytes_per_launch": sm_bytes,
+                "traffic": profiled_traffic("k_mg_smooth_mixed_1m.md", args.workload),
+                "traffic_source": "profiles/k_mg_smooth_mixed_1m.md (ncu, one level-0 launch)",
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": sm_bytes,
                 "launch_ms": sm_ms, "unit_work": "%d points x 3 species, 24 B each" % (lvl0_pts // 3)}
     elif mg_ms >= mech_ms:
         roof = roof_mg
