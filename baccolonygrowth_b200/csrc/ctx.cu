@@ -518,6 +518,7 @@ extern "C" int bcg_get_field(bcg_ctx* c, int f, int level, double* out, size_t n
         BCG_CUDA_TRY(cudaMemcpyAsync(out, v.ptr, v.n * 8, cudaMemcpyDeviceToHost, c->stream));
         return ctx_check_status(c);
     }
+    mg_res0_materialise(c);
     int nz1 = v.mg == 1 ? v.nz + 1 : (int)(v.n / (v.nx + 1));   /* rows delivered */
     int k0 = v.mg == 1 ? 0 : 1;
     size_t rows = (size_t)nz1 + k0;
@@ -540,6 +541,7 @@ extern "C" int bcg_set_field(bcg_ctx* c, int f, int level, const double* in, siz
     if (rc) return rc;
     if (n < v.n) return BCG_E_ARG;
     if (v.mg == 2) return BCG_E_UNSUPPORTED;  /* the agar view is derived */
+    mg_res0_materialise(c);                    /* before its inputs change */
     if (v.mg == 1) { c->mg_clean = 0; nutrient_graphs_drop(c); }   /* Err/Res may no longer be zero */
     if (!v.mg) {
         BCG_CUDA_TRY(cudaMemcpy(v.ptr, in, v.n * 8, cudaMemcpyHostToDevice));

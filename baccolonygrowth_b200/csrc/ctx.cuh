@@ -112,6 +112,8 @@ struct bcg_ctx {
     /* multigrid Err (all levels) and Res (levels > 0) are zero, as the last
      * reset() left them; setup() then skips its resetZero */
     int mg_clean;
+    /* level 0's Res of the last reset() not computed yet (done on demand) */
+    int mg_res0_stale;
     int pair_f32;          /* contact geometry in FP32 local to cell i (bcg_set_pair_precision) */
     double smooth_tune_ms; /* device time of one level-0 fused smoother launch at the tuned shape */
 };
@@ -134,4 +136,7 @@ void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s, int moved);
 void launch_mean_stress(bcg_ctx* c, double* stress, unsigned long long* fcw, cudaStream_t s);
 void launch_surface_force(bcg_ctx* c, double* force, cudaStream_t s);
 int mg_tune_smoother(bcg_ctx* c, int* choice);
+/* compute level 0's multigrid Res left pending by the last reset() (mg.cu);
+ * called before its inputs (Sol, insideColonyDen) change or it is read */
+void mg_res0_materialise(bcg_ctx* c);
 int mg_kernel_attributes();

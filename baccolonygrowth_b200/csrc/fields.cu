@@ -232,6 +232,7 @@ static int deposit(bcg_ctx* c, bool smooth)
 {
     const bcg_params& P = c->P;
     if (P.filter_len > 8 || P.refinement_grid_height > 8) return BCG_E_UNSUPPORTED;
+    mg_res0_materialise(c);            /* it reads insideColonyDen, rewritten here */
     timer_begin(c, BCG_T_DENSITY);
     int rc = bin_cells(c, c->cur);
     if (rc) return rc;

@@ -425,12 +425,18 @@ __device__ __forceinline__ void relax_smem(const RelaxK<T>& K, bool oxy, bool to
 }
 
 /* All mu2 relaxations of a level of nz >= 1 held in shared memory, as a
- * wavefront over the sweeps: at step t sweep s relaxes row k = t - 2s, its
- * even columns in one phase and its odd columns in the next.  Two rows of
- * lag keep every read on the value the sequential order gives it: row k+1
- * still holds sweep s-1's value, row k-1 already holds sweep s's, and no
- * other sweep writes row k or its neighbours in the same phase.  About
- * (nz+1)/2 sweeps progress per step instead of one. */
+ * wavefront over the sweeps: at step t sweep s relaxes the even columns of
+ * row t - 2s and the odd columns of row t - 2s - 1, one barrier per step.
+ * The lags keep every read on the value the sequential order gives it:
+ *   even (k, s) reads its column at k-1 (sweep s, step t-1) and k+1 (sweep
+ *   s-1, not rewritten before step t+1) and the odd columns of row k
+ *   (sweep s-1's, written at step t-1, rewritten at step t+1);
+ *   odd (k, s) reads its column at k-1 (sweep s, step t-1) and k+1 (sweep
+ *   s-1) and the even columns of row k (sweep s's, written at step t-1;
+ *   sweep s+1 rewrites them at step t+1);
+ * and in one step the even writes (rows t - 2s) and odd writes (rows
+ * t - 2s - 1) never meet a location another item of the step reads.
+ * About (nz+1)/2 sweeps progress per step instead of one. */
 template <class T>
 __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L, int l, int sweeps,
                                                          const double* __restrict__ inside0)
@@ -467,25 +473,28 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
         const int ncol = (W - par + 1) / 2;
         for (int j = 0; j < 2; j++) { int q = th + j * nth; a_[par][j] = q / ncol; c_[par][j] = q % ncol; }
     }
-    const int steps = nz + 1 + 2 * (sweeps - 1);
+    const int steps = nz + 1 + 2 * (sweeps - 1) + 1;
     for (int t = 0; t < steps; t++) {
-        const int s_lo = t > nz ? (t - nz + 1) / 2 : 0;
-        const int s_hi = min(sweeps - 1, t / 2);
-        const int na = s_hi - s_lo + 1;
 #pragma unroll
         for (int par = 0; par < 2; par++) {
+            /* parity par relaxes row tp - 2s for the sweeps s with that row in 0..nz */
+            const int tp = t - par;
+            if (tp < 0) continue;
+            const int s_lo = tp > nz ? (tp - nz + 1) / 2 : 0;
+            const int s_hi = min(sweeps - 1, tp / 2);
+            const int na = s_hi - s_lo + 1;
 #pragma unroll
             for (int j = 0; j < 2; j++)
                 if (a_[par][j] < na)
-                    relax_smem<T>(K, oxy, top_levels, nx, nz, 2 * c_[par][j] + par, t - 2 * (s_lo + a_[par][j]), Es, Rs, ins);
+                    relax_smem<T>(K, oxy, top_levels, nx, nz, 2 * c_[par][j] + par, tp - 2 * (s_lo + a_[par][j]), Es, Rs, ins);
             /* more active sweeps than two items per thread cover (large levels) */
             const int ncol = (W - par + 1) / 2;
             for (int q = th + 2 * nth; q < na * ncol; q += nth) {
                 const int sw = s_lo + q / ncol;
-                relax_smem<T>(K, oxy, top_levels, nx, nz, 2 * (q % ncol) + par, t - 2 * sw, Es, Rs, ins);
+                relax_smem<T>(K, oxy, top_levels, nx, nz, 2 * (q % ncol) + par, tp - 2 * sw, Es, Rs, ins);
             }
-            __syncthreads();
         }
+        __syncthreads();
     }
     for (int q = th; q < np; q += nth) {
         int i = q % W, k = q / W;
@@ -775,11 +784,9 @@ __global__ void __launch_bounds__(32 * SMOOTH_WARPS) k_mg_smooth(MgConst m, MgLv
 template <class T>
 __global__ void k_mg_restrict(MgConst m, MgLvlT<T> Lc, MgLvlT<T> Lf, int l, const double* __restrict__ inside0)
 {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    int sp = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y, sp = blockIdx.z;
     const int nx = Lc.nx, nz = Lc.nz;
-    if (idx >= (nx + 1) * (nz + 1)) return;
-    int i = idx % (nx + 1), k = idx / (nx + 1);
+    if (i > nx) return;
     const int X = m.box_x, ZA = m.box_z_agar;
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d < X ? X * d0 / d : X;
@@ -850,57 +857,71 @@ __global__ void k_mg_restrict(MgConst m, MgLvlT<T> Lc, MgLvlT<T> Lf, int l, cons
 #undef ALv
 }
 
-/* interpolationAga, Multigrid.cpp:407-467 (Err of level l += from l+1) */
+/* interpolationAga, Multigrid.cpp:407-467 (Err of level l += from l+1).
+ * A thread takes the fine columns 2j and 2j+1 of one row: both read the
+ * coarse column ip = nxp/2 - nx/4 + j (the odd one also ip + 1), so the
+ * coarse values are loaded once and the pair is read and written as one
+ * 16-byte (FP32: 8-byte) access. */
 template <class T>
 __global__ void k_mg_interp(MgConst m, MgLvlT<T> Lf, MgLvlT<T> Lc, int l)
 {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    int sp = blockIdx.y;
-    const int nx = Lf.nx, nz = Lf.nz;
-    if (idx >= (nx + 1) * (nz + 1)) return;
-    int i = idx % (nx + 1), k = idx / (nx + 1);
+    typedef typename Pair2<T>::type T2;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y, sp = blockIdx.z;
+    const int nx = Lf.nx, i = 2 * j;
+    if (i > nx) return;
+    const bool has_odd = i + 1 <= nx;
     const int X = m.box_x;
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
     const T* C = SP(Lc.e);
-    T& e = AT(SP(Lf.e), Lf, i, k);
+    T* e = SP(Lf.e) + (size_t)k * Lf.pitch + i;
     const T half = (T)0.5, quarter = (T)0.25;
+    const int ip = nxp / 2 - nx / 4 + j;
 #define CV(a, b) at_ref(C, Lc, a, b)
-    if (i % 2 == 0) {
-        int ip = nxp / 2 - nx / 4 + i / 2;
-        if (k % 2 == 0) e += CV(ip, k / 2);
-        else { int kp = (k - 1) / 2; e += half * (CV(ip, kp) + CV(ip, kp + 1)); }
+    T inc_e, inc_o = T(0);
+    if (k % 2 == 0) {
+        const int kp = k / 2;
+        const T c0 = CV(ip, kp);
+        inc_e = c0;
+        if (has_odd) inc_o = half * (c0 + CV(ip + 1, kp));
     } else {
-        int ip = nxp / 2 - nx / 4 + (i - 1) / 2;
-        if (k % 2 == 0) { int kp = k / 2; e += half * (CV(ip, kp) + CV(ip + 1, kp)); }
-        else {
-            int kp = (k - 1) / 2;
-            e += quarter * (CV(ip, kp) + CV(ip, kp + 1) + CV(ip + 1, kp) + CV(ip + 1, kp + 1));
-        }
+        const int kp = (k - 1) / 2;
+        const T c00 = CV(ip, kp), c01 = CV(ip, kp + 1);
+        inc_e = half * (c00 + c01);
+        if (has_odd) inc_o = quarter * (c00 + c01 + CV(ip + 1, kp) + CV(ip + 1, kp + 1));
     }
 #undef CV
+    if (has_odd) {
+        T2 v = *reinterpret_cast<T2*>(e);
+        v.x += inc_e; v.y += inc_o;
+        *reinterpret_cast<T2*>(e) = v;
+    } else {
+        e[0] += inc_e;
+    }
 }
 
 /* resetZero, Multigrid.cpp:47-82 */
 template <class T>
 __global__ void k_mg_reset_zero(MgLvlT<T> L, int zero_res)
 {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    int sp = blockIdx.y;
-    if (idx >= (L.nx + 1) * (L.nz + 1)) return;
-    int i = idx % (L.nx + 1), k = idx / (L.nx + 1);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y, sp = blockIdx.z;
+    if (i > L.nx) return;
     AT(SP(L.e), L, i, k) = 0;
     if (zero_res) AT(SP(L.r), L, i, k) = 0;
 }
 
 /* updateSolAgaElementwise, Multigrid.cpp:544-568 */
-__global__ void k_mg_update_sol(MgConst m, MgLvl L, int l)
+/* With `nest` set it also does NestSolAgaElementwise
+ * (Multigrid.cpp:724-737) for level l+1 (Ln): a point (i, k) of this level
+ * that level l+1 nests, Sol_{l+1}(i', k') = Sol_l(2i' - nx' + nxp'/2, 2k'),
+ * writes its updated value there.  That is the value the separate pass
+ * would copy: between the two only the boundary rewrite and Res change,
+ * and neither touches a nested point. */
+__global__ void k_mg_update_sol(MgConst m, MgLvl L, int l, MgLvl Ln, int nest)
 {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    int sp = blockIdx.y;
-    const int nx = L.nx, nz = L.nz;
-    if (idx >= (nx + 1) * (nz + 1)) return;
-    int i = idx % (nx + 1), k = idx / (nx + 1);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y, sp = blockIdx.z;
+    const int nx = L.nx;
+    if (i > nx) return;
     const int X = m.box_x, ZA = m.box_z_agar;
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d < X ? X * d0 / d : X;
@@ -908,14 +929,24 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l)
     AT(SP(L.r), L, i, k) = 0;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     double& e = AT(SP(L.e), L, i, k);
+    double& a = AT(SP(L.s), L, i, k);
     if (l < m.A && (l == 0 || ip <= 0 || ip >= nxp || kp >= nzp)) {
-        double& a = AT(SP(L.s), L, i, k);
         a += e;
         if (sp == 0) a = dmaxd(dmind(a, m.max_carbon), 0.0);
         else if (sp == 1) a = dmaxd(dmind(a, m.max_o2_agar), 0.0);
         else a = dmaxd(a, 0.0);
     }
     e = 0;
+    if (nest) {
+        const int dn = 2 * d;
+        const int nxpn = X * d0 / dn < X ? X * d0 / dn : X;
+        const int nzpn = ZA * d0 / dn < ZA ? ZA * d0 / dn : ZA;
+        const int t = i + Ln.nx - nxpn / 2;
+        if ((k & 1) == 0 && (t & 1) == 0 && i > 0 && i < nxpn && k < nzpn) {
+            const int in = t >> 1, kn = k >> 1;
+            if (in >= 0 && in <= Ln.nx && kn <= Ln.nz) AT(SP(Ln.s), Ln, in, kn) = a;
+        }
+    }
 }
 
 /* updateResAgaElementwise, Multigrid.cpp:570-701.  SETUP: the setup()
@@ -924,7 +955,7 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l)
  * zeroes Res, so one pass clamps the stencil values as it reads them,
  * stores the point's clamped value where the clamp changed it, and
  * writes Res (0 where updateResAga leaves it). */
-template <bool SETUP>
+template <bool SETUP, bool LEVEL0>
 __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const double* __restrict__ inside0)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
@@ -943,20 +974,27 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
     const bool oxy = sp == 1;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     const double* A = SP(L.s);
+    const double* ctr = A + (size_t)k * L.pitch + i;
+    const ptrdiff_t P = L.pitch;
     double* R = &AT(SP(L.r), L, i, k);
     const double hi = sp == 0 ? m.max_carbon : (sp == 1 ? m.max_o2_agar : 1e300);
-    /* the solution value updateSolAga leaves at (a, b): clamped where uncovered */
-    auto sol = [&](int a, int b) -> double {
-        double v = AT(A, L, a, b);
+    /* the solution value updateSolAga leaves at (i + di, k + dk): clamped
+     * where uncovered (everywhere on level 0) */
+    auto sol = [&](int di, int dk) -> double {
+        double v = ctr[di + dk * P];
         if (SETUP) {
-            int ipa = 2 * a - nx + nxp / 2, kpa = 2 * b;
-            if (l == 0 || ipa <= 0 || ipa >= nxp || kpa >= nzp) v = dmaxd(dmind(v, hi), 0.0);
+            bool clamp = LEVEL0;
+            if (!LEVEL0) {
+                const int ipa = ip + 2 * di, kpa = kp + 2 * dk;
+                clamp = ipa <= 0 || ipa >= nxp || kpa >= nzp;
+            }
+            if (clamp) v = dmaxd(dmind(v, hi), 0.0);
         }
         return v;
     };
     double res = 0.0;
     bool set = SETUP;
-#define AL(a, b) sol(a, b)
+#define AL(a, b) sol((a) - i, (b) - k)
 #define APv(a, b) AT(SP(Lp.s), Lp, a, b)
     if (i == 0 || i == nx) {
         if (l == m.A - 1) {
@@ -973,7 +1011,7 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
             else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k - 1) - 4 * AL(i, k)) * cdt;
         }
     } else if (k == 0) {
-        if (l == 0) {
+        if (LEVEL0) {
             if (inside0[(size_t)i * m.box_z] > 0) set = true, res = 0;
             else if (oxy) set = true, res = m.max_o2_agar - AL(i, k);
             else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * cdt;
@@ -984,7 +1022,7 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
             else set = true, res = (AL(i + 1, k) + AL(i - 1, k) + 2 * AL(i, k + 1) - 4 * AL(i, k)) * cdt;
         }
     } else {
-        if (l > 0) {
+        if (!LEVEL0) {
             if (kp == nzp && ip > 0 && ip < nxp)
                 set = true, res = (AL(i + 1, k) + AL(i - 1, k) + APv(ip, kp - 2) + AL(i, k + 1) - 4 * AL(i, k)) * cdt;
             else if (ip == 0 && kp < nzp)
@@ -1001,7 +1039,7 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
 #undef APv
     if (set) *R = res;
     if (SETUP) {
-        double v = AT(A, L, i, k), w = sol(i, k);
+        double v = ctr[0], w = sol(0, 0);
         if (w != v) AT(SP(L.s), L, i, k) = w;
     }
 }
@@ -1027,22 +1065,6 @@ __global__ void k_mg_rewrite_bdry(MgConst m, MgLvl L, MgLvl Lc, int l)
         int i2 = nx2 / 2 + i / 2 - nx / 4;
         AT(SP(L.s), L, i, k) = (AT(C, Lc, i2, k / 2) + AT(C, Lc, i2, (k + 1) / 2)) / 2;
     }
-}
-
-/* NestSolAgaElementwise, Multigrid.cpp:724-737 */
-__global__ void k_mg_nest(MgConst m, MgLvl L, MgLvl Lf, int l)
-{
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    int sp = blockIdx.y;
-    const int nx = L.nx, nz = L.nz;
-    if (idx >= (nx + 1) * (nz + 1)) return;
-    int i = idx % (nx + 1), k = idx / (nx + 1);
-    const int X = m.box_x, ZA = m.box_z_agar;
-    int d = 1 << l, d0 = 1 << m.A;
-    int nxp = X * d0 / d < X ? X * d0 / d : X;
-    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
-    int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
-    if (ip > 0 && ip < nxp && kp < nzp) AT(SP(L.s), L, i, k) = AT(SP(Lf.s), Lf, ip, kp);
 }
 
 /* copyToMG, Multigrid.cpp:891-907: wall-under-colony values into level 0,
@@ -1078,6 +1100,9 @@ __global__ void k_mg_copy_from(MgLvl L, int X, double* cC, double* cO, double* c
 
 /* ------------------------------------------------------------------------ */
 static inline dim3 grid2(int n, int threads) { return dim3((unsigned)((n + threads - 1) / threads), 3); }
+/* 2-D launch over a level: x = columns, y = rows, z = species */
+static inline dim3 grid_rows(int ncols, int nrows, int threads)
+{ return dim3((unsigned)((ncols + threads - 1) / threads), (unsigned)nrows, 3); }
 
 /* 0 = one thread per column and half-sweep, 1 = segmented half-sweeps,
  * 2 = fused sweeps (k_mg_smooth) on levels taller than 96 rows */
@@ -1301,13 +1326,13 @@ void mg_vcycle_t(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
     for (int l = 0; l < Lv - 1; l++) {
         smooth_level<T>(c, m, l, mu1);
         MgLvlT<T> Lc = lvl<T>(c, l + 1), Lf = lvl<T>(c, l);
-        k_mg_restrict<T><<<grid2((Lc.nx + 1) * (Lc.nz + 1), 256), 256, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
+        k_mg_restrict<T><<<grid_rows(Lc.nx + 1, Lc.nz + 1, 128), 128, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
         c->launches++;
     }
     relax_coarsest<T>(c, m, Lv - 1, mu2);
     for (int l = Lv - 2; l >= 0; l--) {
         MgLvlT<T> Lf = lvl<T>(c, l), Lc = lvl<T>(c, l + 1);
-        k_mg_interp<T><<<grid2((Lf.nx + 1) * (Lf.nz + 1), 256), 256, 0, c->stream>>>(m, Lf, Lc, l);
+        k_mg_interp<T><<<grid_rows(Lf.nx / 2 + 1, Lf.nz + 1, 128), 128, 0, c->stream>>>(m, Lf, Lc, l);
         c->launches++;
         smooth_level<T>(c, m, l, mu1);
     }
@@ -1321,28 +1346,36 @@ static void reset_zero(bcg_ctx* c, int from_level = 0)
 {
     for (int l = from_level; l < c->mg_levels; l++) {
         MgLvl L = mg_lvl(c, l);
-        k_mg_reset_zero<double><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(L, l > 0);
+        k_mg_reset_zero<double><<<grid_rows(L.nx + 1, L.nz + 1, 256), 256, 0, c->stream>>>(L, l > 0);
         c->launches++;
     }
 }
-static void update_sol(bcg_ctx* c, const MgConst& m, int l)
+static void update_sol(bcg_ctx* c, const MgConst& m, int l, bool nest = false)
 {
     MgLvl L = mg_lvl(c, l);
-    k_mg_update_sol<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, l);
+    const bool n = nest && l + 1 < m.A;
+    MgLvl Ln = n ? mg_lvl(c, l + 1) : L;
+    k_mg_update_sol<<<grid_rows(L.nx + 1, L.nz + 1, 256), 256, 0, c->stream>>>(m, L, l, Ln, n ? 1 : 0);
     c->launches++;
 }
 static void update_res(bcg_ctx* c, const MgConst& m, int l, bool setup_clean = false)
 {
     MgLvl L = mg_lvl(c, l), Lp = mg_lvl(c, l > 0 ? l - 1 : 0);
     dim3 grid((unsigned)((L.nx + 1 + 127) / 128), (unsigned)(L.nz + 1), 3);
-    if (setup_clean) k_mg_update_res<true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
-    else k_mg_update_res<false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    if (l == 0) {
+        if (setup_clean) k_mg_update_res<true, true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+        else k_mg_update_res<false, true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    } else {
+        if (setup_clean) k_mg_update_res<true, false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+        else k_mg_update_res<false, false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+    }
     c->launches++;
 }
 
-/* setup(), Multigrid.cpp:818-825 */
+/* setup(), Multigrid.cpp:818-825 (both forms recompute level 0's Res) */
 void mg_setup(bcg_ctx* c, const MgConst& m)
 {
+    c->mg_res0_stale = 0;
     if (c->mg_clean) {
         /* resetZero and updateSolAga have nothing to do but the clamp */
         c->mg_clean = 0;
@@ -1354,10 +1387,14 @@ void mg_setup(bcg_ctx* c, const MgConst& m)
     for (int l = 0; l <= m.A - 1; l++) update_res(c, m, l);
 }
 
-/* reset(), Multigrid.cpp:827-841 (evalUpdateRes's result is discarded there) */
+/* reset(), Multigrid.cpp:827-841 (evalUpdateRes's result is discarded there).
+ * updateSolAga and NestSolAga run as one pass per level (update_sol with
+ * nest).  Level 0's Res, which reset() recomputes last, is read by nothing
+ * before the next setup() recomputes it: it is computed only when a caller
+ * reads a multigrid array or changes its inputs (mg_res0_materialise). */
 void mg_reset(bcg_ctx* c, const MgConst& m)
 {
-    for (int l = 0; l <= m.A - 1; l++) update_sol(c, m, l);
+    for (int l = 0; l <= m.A - 1; l++) update_sol(c, m, l, true);
     for (int l = 0; l < m.A - 1; l++) {
         MgLvl L = mg_lvl(c, l), Lc = mg_lvl(c, l + 1);
         int n = L.nx + 1 + 2 * L.nz;
@@ -1365,16 +1402,21 @@ void mg_reset(bcg_ctx* c, const MgConst& m)
         c->launches++;
     }
     /* the reference recomputes Res on every composite level here, and the
-     * resetZero below clears it again on levels > 0: only level 0's stays */
-    update_res(c, m, 0);
+     * resetZero below clears it again on levels > 0: only level 0's stays,
+     * computed on demand */
+    c->mg_res0_stale = 1;
     /* updateSolAga already zeroed Err and Res on the composite levels */
     reset_zero(c, m.A);
-    for (int l = 1; l < m.A; l++) {
-        MgLvl L = mg_lvl(c, l), Lf = mg_lvl(c, l - 1);
-        k_mg_nest<<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(m, L, Lf, l);
-        c->launches++;
-    }
     c->mg_clean = 1;
+}
+
+/* level 0's Res as reset() leaves it, before a caller reads or writes a
+ * multigrid array or rewrites insideColonyDen */
+void mg_res0_materialise(bcg_ctx* c)
+{
+    if (!c->mg_res0_stale) return;
+    c->mg_res0_stale = 0;
+    update_res(c, mg_const(c, c->P.mg_dt), 0);
 }
 
 void mg_copy_to(bcg_ctx* c, const MgConst& m, int wall_buf)
@@ -1542,7 +1584,7 @@ extern "C" int bcg_mg_solve_tol(bcg_ctx* c, double rel_tol, int precision, int m
             mg_convert_levels(c, true, true);
             for (int l = 0; l < c->mg_levels; l++) {
                 MgLvlF L = mg_lvl_f(c, l);
-                k_mg_reset_zero<float><<<grid2((L.nx + 1) * (L.nz + 1), 256), 256, 0, c->stream>>>(L, 0);
+                k_mg_reset_zero<float><<<grid_rows(L.nx + 1, L.nz + 1, 256), 256, 0, c->stream>>>(L, 0);
                 c->launches++;
             }
             double best = 1.0;
