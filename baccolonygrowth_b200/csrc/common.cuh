@@ -39,6 +39,7 @@ struct DevStatus {
  * pairs its planner records before falling back to one sequential group */
 #define DIV_SORT_MAX 8192
 #define DIV_PAIR_CAP 65536
+#define DIV_PLAN_SMEM (3 * DIV_SORT_MAX * 4)   /* k_div_plan's dynamic shared memory */
 
 struct MechParams {
     int box_x, box_y, box_z, rgh;

@@ -254,7 +254,7 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
         }
     }
     DALLOC(c->mg_scratch, 1 << 20);
-    if ((rc = mg_kernel_attributes())) { bcg_destroy(c); return rc; }
+    if ((rc = mg_kernel_attributes()) || (rc = mech_kernel_attributes())) { bcg_destroy(c); return rc; }
     rc = ensure_pinned(c, 1 << 16);
     if (rc) { bcg_destroy(c); return rc; }
     rc = ctx_check_status(c);

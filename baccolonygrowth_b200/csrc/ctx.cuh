@@ -140,3 +140,4 @@ int mg_tune_smoother(bcg_ctx* c, int* choice);
  * called before its inputs (Sol, insideColonyDen) change or it is read */
 void mg_res0_materialise(bcg_ctx* c);
 int mg_kernel_attributes();
+int mech_kernel_attributes();

@@ -629,10 +629,15 @@ __global__ void __launch_bounds__(1024) k_div_plan(int n_start, int ndiv, int ca
         const int* __restrict__ div_list, const int* __restrict__ cell_box,
         const int* __restrict__ nbr, const int* __restrict__ ncount,
         CellRec* __restrict__ new_rec, int* __restrict__ new_box, int4* __restrict__ rect,
-        int2* __restrict__ pairs, int* __restrict__ par, int* __restrict__ order, int* __restrict__ grp,
+        int2* __restrict__ pairs, int* __restrict__ par_out, int* __restrict__ order, int* __restrict__ grp,
         int* __restrict__ lineage, int* __restrict__ out, DevStatus* st)
 {
-    __shared__ int sd[DIV_SORT_MAX];
+    /* dynamic shared memory: the sorted parents (later the group of each
+     * root), the union-find parents, the groups' fill counters */
+    extern __shared__ int div_smem[];
+    int* sd = div_smem;
+    int* par = div_smem + DIV_SORT_MAX;
+    int* fill = div_smem + 2 * DIV_SORT_MAX;
     __shared__ int s_npairs;
     int P2 = 1;
     while (P2 < ndiv) P2 <<= 1;
@@ -672,21 +677,45 @@ __global__ void __launch_bounds__(1024) k_div_plan(int n_start, int ndiv, int ca
         int b0 = cell_box[m];
         int x0 = b0 / YZ, z0 = b0 % mp.box_z;
         int xlo = x0, xhi = x0, zlo = z0, zhi = z0;
-        auto grow_rect = [&](int bb) {
-            int x = bb / YZ, z = bb % mp.box_z;
-            xlo = min(xlo, x); xhi = max(xhi, x); zlo = min(zlo, z); zhi = max(zhi, z);
-        };
-        grow_rect(bm); grow_rect(bd);
-        const int cnt = ncount[m];
-        for (int j = 0; j < cnt; j++) grow_rect(cell_box[nbr[(size_t)m * mp.kmax + j]]);
-        rect[d] = make_int4(xlo - 2, xhi + 2, zlo - 2, zhi + 2);
+        int x = bm / YZ, z = bm % mp.box_z;
+        xlo = min(xlo, x); xhi = max(xhi, x); zlo = min(zlo, z); zhi = max(zhi, z);
+        x = bd / YZ; z = bd % mp.box_z;
+        xlo = min(xlo, x); xhi = max(xhi, x); zlo = min(zlo, z); zhi = max(zhi, z);
+        rect[d] = make_int4(xlo, xhi, zlo, zhi);
         par[d] = d;
     }
     __syncthreads();
+    /* the boxes of the mother's listed neighbours, one warp per division,
+     * then the footprint's margin of 2 boxes */
+    {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int d = wid; d < nd; d += nw) {
+            const int m = sd[d];
+            const int cnt = ncount[m];
+            int xlo = 0x7fffffff, xhi = -0x7fffffff, zlo = 0x7fffffff, zhi = -0x7fffffff;
+            for (int j = lane; j < cnt; j += 32) {
+                const int bb = cell_box[nbr[(size_t)m * mp.kmax + j]];
+                const int x = bb / YZ, z = bb % mp.box_z;
+                xlo = min(xlo, x); xhi = max(xhi, x); zlo = min(zlo, z); zhi = max(zhi, z);
+            }
+            for (int o = 16; o >= 1; o >>= 1) {
+                xlo = min(xlo, __shfl_xor_sync(0xffffffffu, xlo, o));
+                xhi = max(xhi, __shfl_xor_sync(0xffffffffu, xhi, o));
+                zlo = min(zlo, __shfl_xor_sync(0xffffffffu, zlo, o));
+                zhi = max(zhi, __shfl_xor_sync(0xffffffffu, zhi, o));
+            }
+            if (lane == 0) {
+                int4 r = rect[d];
+                r.x = min(r.x, xlo); r.y = max(r.y, xhi); r.z = min(r.z, zlo); r.w = max(r.w, zhi);
+                rect[d] = make_int4(r.x - 2, r.y + 2, r.z - 2, r.w + 2);
+            }
+        }
+    }
+    __syncthreads();
     /* overlapping footprints */
-    const long np2 = (long)nd * nd;
-    for (long q = threadIdx.x; q < np2; q += blockDim.x) {
-        int a = (int)(q / nd), b = (int)(q % nd);
+    const int np2 = nd * nd;
+    for (int q = threadIdx.x; q < np2; q += blockDim.x) {
+        int a = q / nd, b = q - a * nd;
         if (a >= b) continue;
         int4 ra = rect[a], rb = rect[b];
         if (ra.x <= rb.y && rb.x <= ra.y && ra.z <= rb.w && rb.z <= ra.w) {
@@ -716,15 +745,12 @@ __global__ void __launch_bounds__(1024) k_div_plan(int n_start, int ndiv, int ca
         for (int d = 0; d < nd; d++) sd[par[d]]++;
         int pos = 0;
         for (int d = 0; d < nd; d++)
-            if (par[d] == d) { grp[2 * ng] = pos; grp[2 * ng + 1] = sd[d]; sd[d] = ng; pos += grp[2 * ng + 1]; ng++; }
+            if (par[d] == d) { grp[2 * ng] = pos; grp[2 * ng + 1] = sd[d]; fill[ng] = pos; sd[d] = ng; pos += grp[2 * ng + 1]; ng++; }
         /* members in ascending d */
-        for (int g = 0; g < ng; g++) grp[2 * g + 1] = 0;
-        for (int d = 0; d < nd; d++) {
-            int g = sd[par[d]];
-            order[grp[2 * g] + grp[2 * g + 1]++] = d;
-        }
+        for (int d = 0; d < nd; d++) order[fill[sd[par[d]]]++] = d;
         out[0] = nd; out[1] = n_start + nd; out[2] = ng;
     }
+    (void)par_out;
 }
 
 __global__ void __launch_bounds__(128) k_div_groups(int n_start, const int* __restrict__ div_out,
@@ -765,6 +791,18 @@ __global__ void __launch_bounds__(128) k_div_groups(int n_start, const int* __re
     for (int j = lane; j < gl; j += 32) moved[lineage[2 * order[gs + j]]] = 0;
 }
 
+/* the division planner's shared memory: sorted parents, union-find
+ * parents and group fill counters, DIV_SORT_MAX ints each */
+int mech_kernel_attributes()
+{
+    static bool done = false;
+    if (done) return BCG_OK;
+    if (cudaFuncSetAttribute(k_div_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, DIV_PLAN_SMEM) != cudaSuccess)
+        return BCG_E_CUDA;
+    done = true;
+    return BCG_OK;
+}
+
 extern "C" int bcg_get_dividing(bcg_ctx* c, int* ids, int capacity)
 {
     if (!c || (!ids && capacity > 0)) return BCG_E_ARG;
@@ -797,7 +835,7 @@ int divide_launch(bcg_ctx* c, const float* draws, int n_draw_sets, double t)
     memcpy(c->pinned, draws, db);
     BCG_CUDA_TRY(cudaMemcpyAsync(c->draws_dev, c->pinned, db, cudaMemcpyHostToDevice, c->stream));
     MechParams mp = mech_params(c);
-    k_div_plan<<<1, 1024, 0, c->stream>>>(c->n, ndiv, c->cap, t, c->draws_dev, c->rec[nb], c->soa, mp,
+    k_div_plan<<<1, 1024, DIV_PLAN_SMEM, c->stream>>>(c->n, ndiv, c->cap, t, c->draws_dev, c->rec[nb], c->soa, mp,
         c->div_list, c->cell_box, c->nbr, c->ncount, c->div_rec, c->div_box, c->div_rect, c->div_pairs,
         c->div_par, c->div_order, c->div_grp, c->lineage, c->n_done_dev, c->status);
     k_div_groups<<<(ndiv + 3) / 4, 128, 0, c->stream>>>(c->n, c->n_done_dev, c->div_grp, c->div_order,

@@ -14,6 +14,9 @@
 #include "mg.cuh"
 #include "internal.h"
 #include <string.h>
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 __device__ __forceinline__ double dmaxd(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double dmind(double a, double b) { return a < b ? a : b; }
@@ -502,6 +505,126 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
     }
 }
 
+/* The point update of relax_smem with the neighbour columns i-1 and i+1
+ * read from the arrays El and Er (the block's own shared memory, or the
+ * shared memory of the cluster block that owns that column). */
+template <class T>
+__device__ __forceinline__ void relax_cl(const RelaxK<T>& K, bool oxy, bool top_levels,
+                                         int nx, int nz, int i, int k, T* Es, const T* El, const T* Er,
+                                         const T* Rs, const unsigned char* ins_row0)
+{
+    const int W = nx + 1;
+    const bool side = (i == 0 || i == nx);
+    const T r = Rs[k * W + i];
+    T out = Es[k * W + i];
+    if (k == 0) {
+        if (ins_row0[i]) out = r;
+        else if (side) {
+            if (top_levels) out = oxy ? r : rx_corner(r, (i == 0) ? Er[i + 1] : El[i - 1], at_s(Es, nx, nz, i, 1), K);
+        } else out = oxy ? r : rx_k0(r, at_s(Es, nx, nz, i, 1), El[i - 1], Er[i + 1], K);
+    } else {
+        const T below = Es[(k - 1) * W + i];
+        if (k == nz) {
+            if (top_levels) {
+                if (side) out = oxy ? r : rx_corner(r, (i == 0) ? Er[k * W + i + 1] : El[k * W + i - 1], below, K);
+                else out = rx_top(r, below, El[k * W + i - 1], Er[k * W + i + 1], K);
+            }
+        } else if (side) {
+            if (top_levels) out = oxy ? r : rx_side(r, below, Es[(k + 1) * W + i], (i == 0) ? Er[k * W + i + 1] : El[k * W + i - 1], K);
+        } else {
+            out = rx_in(r, below, Es[(k + 1) * W + i], El[k * W + i - 1], Er[k * W + i + 1], K);
+        }
+    }
+    Es[k * W + i] = out;
+}
+
+/* k_mg_coarse_wave spread over a thread-block cluster per species: block
+ * `rank` of the cluster owns the columns [rank W / C, (rank+1) W / C) and
+ * relaxes only those, in the same wavefront order; a neighbour column
+ * owned by the next block is read from that block's shared memory.  One
+ * cluster barrier per step orders the steps (the wavefront never writes,
+ * in a step, a value another item of the step reads).  Every block keeps
+ * the whole level in its shared memory (loaded once); only its own columns
+ * of it are kept current and written back.  Every block runs the same
+ * number of barriers and none leaves before the last one, after which no
+ * block reads another's shared memory. */
+template <class T>
+__global__ void __launch_bounds__(256) k_mg_coarse_cluster(MgConst m, MgLvlT<T> L, int l, int sweeps,
+                                                            const double* __restrict__ inside0)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int sp = blockIdx.x / C;
+    const int nx = L.nx, nz = L.nz, W = nx + 1;
+    const int np = W * (nz + 1);
+    T* Es = reinterpret_cast<T*>(smem_raw);
+    T* Rs = Es + np;
+    unsigned char* ins = reinterpret_cast<unsigned char*>(Rs + np);
+    T* E = SP(L.e);
+    const T* R = SP(L.r);
+    const int nth = blockDim.x, th = threadIdx.x;
+    for (int q = th; q < np; q += nth) {
+        int i = q % W, k = q / W;
+        Es[q] = AT(E, L, i, k);
+        Rs[q] = AT(R, L, i, k);
+    }
+    for (int i = th; i < W; i += nth) {
+        int d = 1 << l;
+        int i0 = (i - nx / 2) * d + m.box_x / 2;
+        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
+        ins[i] = inside0[(size_t)i0 * m.box_z] > 0;
+    }
+    cluster.sync();              /* every block loaded before any reads another */
+    const T* El = rank > 0 ? cluster.map_shared_rank(Es, rank - 1) : Es;
+    const T* Er = rank < C - 1 ? cluster.map_shared_rank(Es, rank + 1) : Es;
+    const int c0 = rank * W / C, c1 = (rank + 1) * W / C;
+    const RelaxK<T> K = relax_k<T>(m, l, sp);
+    const bool oxy = (sp == 1);
+    const bool top_levels = l >= m.A - 1;
+    /* the block's columns of each parity: first, first + 2, ... below c1 */
+    int first[2], ncol[2], a0[2], cc0[2];
+    for (int par = 0; par < 2; par++) {
+        first[par] = c0 + ((c0 & 1) != par ? 1 : 0);
+        ncol[par] = first[par] < c1 ? (c1 - first[par] + 1) / 2 : 0;
+        a0[par] = ncol[par] ? th / ncol[par] : 0x7fffffff;
+        cc0[par] = ncol[par] ? th % ncol[par] : 0;
+    }
+    const int steps = nz + 1 + 2 * (sweeps - 1) + 1;
+    for (int t = 0; t < steps; t++) {
+#pragma unroll
+        for (int par = 0; par < 2; par++) {
+            const int tp = t - par;
+            if (tp >= 0 && ncol[par]) {
+                const int s_lo = tp > nz ? (tp - nz + 1) / 2 : 0;
+                const int s_hi = min(sweeps - 1, tp / 2);
+                const int na = s_hi - s_lo + 1;
+                const int i = first[par] + 2 * cc0[par];
+                if (a0[par] < na) {
+                    const int k = tp - 2 * (s_lo + a0[par]);
+                    const T* xl = (i - 1 < c0) ? El : Es;
+                    const T* xr = (i + 1 >= c1) ? Er : Es;
+                    relax_cl<T>(K, oxy, top_levels, nx, nz, i, k, Es, xl, xr, Rs, ins);
+                }
+                /* more items than threads (large levels) */
+                for (int q = th + nth; q < na * ncol[par]; q += nth) {
+                    const int ii = first[par] + 2 * (q % ncol[par]);
+                    const int k = tp - 2 * (s_lo + q / ncol[par]);
+                    const T* xl = (ii - 1 < c0) ? El : Es;
+                    const T* xr = (ii + 1 >= c1) ? Er : Es;
+                    relax_cl<T>(K, oxy, top_levels, nx, nz, ii, k, Es, xl, xr, Rs, ins);
+                }
+            }
+        }
+        cluster.sync();
+    }
+    for (int q = th; q < (c1 - c0) * (nz + 1); q += nth) {
+        const int i = c0 + q % (c1 - c0), k = q / (c1 - c0);
+        AT(E, L, i, k) = Es[k * W + i];
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Fused zebra smoother: S full sweeps (even columns, then odd columns, each */
 /* bottom to top) in one pass over the rows, out of place (E -> E2).        */
@@ -791,13 +914,17 @@ __global__ void k_mg_restrict(MgConst m, MgLvlT<T> Lc, MgLvlT<T> Lf, int l, cons
     int d = 1 << l, d0 = 1 << m.A;
     int nxp = X * d0 / d < X ? X * d0 / d : X;
     int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
+    /* on a composite level only row 0 and the points over the finer level
+     * (0 <= ip <= nxp, kp <= nzp) are written; the launch already stops at
+     * row nzp/2 */
+    if (l < m.A && k > 0 && !(ip >= 0 && ip <= nxp && kp <= nzp)) return;
     const T h2 = (T)(m.bl2 * d * d);
     const T dt = (T)m.dt, D = (T)SP(m.D);
     const T half = (T)0.5;
     const bool oxy = sp == 1;
     int i0 = (i - nx / 2) * d + X / 2;
     i0 = i0 < 0 ? 0 : (i0 > X ? X : i0);   /* clamped to BoxX as in the reference */
-    int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     const T* EP = SP(Lf.e);
     const T* RP = SP(Lf.r);
     const double* AP = SP(Lf.s);
@@ -1295,13 +1422,62 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     return ctx_check_status(c);
 }
 
+/* blocks per cluster of the coarsest-level solve */
+#define COARSE_CLUSTER 8
+/* whether clusters of COARSE_CLUSTER blocks with `smem` bytes each can be
+ * resident (checked once per shared-memory size) */
+template <class T>
+static bool coarse_cluster_ok(size_t smem)
+{
+    static size_t checked = 0;
+    static bool ok = false;
+    if (checked == smem) return ok;
+    checked = smem;
+    ok = false;
+    if (cudaFuncSetAttribute(k_mg_coarse_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return ok;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(3 * COARSE_CLUSTER, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = COARSE_CLUSTER;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_mg_coarse_cluster<T>, &cfg) == cudaSuccess && n >= 3) ok = true;
+    cudaGetLastError();
+    return ok;
+}
+
 /* mu2 sweeps on the coarsest level: fused when it fits one block */
 template <class T>
 static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
     MgLvlT<T> L = lvl<T>(c, l);
     const size_t smem = 2 * sizeof(T) * (size_t)(L.nx + 1) * (L.nz + 1);
-    if (g_relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1) {
+    if (g_relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1 &&
+        L.nx + 1 >= 2 * COARSE_CLUSTER && coarse_cluster_ok<T>(smem + L.nx + 1)) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(3 * COARSE_CLUSTER, 1, 1);
+        cfg.blockDim = dim3(256, 1, 1);
+        cfg.dynamicSmemBytes = smem + L.nx + 1;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = COARSE_CLUSTER;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<T>, m, L, l, sweeps, (const double*)c->inside);
+        c->launches++;
+    } else if (g_relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1) {
         k_mg_coarse_wave<T><<<3, 1024, smem + (L.nx + 1), c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
     } else if (g_relax_mode >= 1 && smem <= 200 * 1024) {
@@ -1318,6 +1494,21 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
     }
 }
 
+/* rows of coarse level l that restrictionAgaElementwise writes: on a
+ * composite level row 0 and the rows over the finer level (2k <= nzp),
+ * on a plain coarsening all of them */
+template <class T>
+static int restrict_rows(const MgConst& m, const MgLvlT<T>& Lc, int l)
+{
+    if (l >= m.A) return Lc.nz + 1;
+    const int d = 1 << l, d0 = 1 << m.A;
+    const int nzp = m.box_z_agar * d0 / d < m.box_z_agar ? m.box_z_agar * d0 / d : m.box_z_agar;
+    int last = nzp / 2;
+    if (last > Lc.nz - 1) last = Lc.nz - 1;
+    if (last < 0) last = 0;
+    return last + 1;
+}
+
 /* Vcycle, Multigrid.cpp:843-862 */
 template <class T>
 void mg_vcycle_t(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
@@ -1326,7 +1517,7 @@ void mg_vcycle_t(bcg_ctx* c, const MgConst& m, int mu1, int mu2)
     for (int l = 0; l < Lv - 1; l++) {
         smooth_level<T>(c, m, l, mu1);
         MgLvlT<T> Lc = lvl<T>(c, l + 1), Lf = lvl<T>(c, l);
-        k_mg_restrict<T><<<grid_rows(Lc.nx + 1, Lc.nz + 1, 128), 128, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
+        k_mg_restrict<T><<<grid_rows(Lc.nx + 1, restrict_rows(m, Lc, l + 1), 128), 128, 0, c->stream>>>(m, Lc, Lf, l + 1, c->inside);
         c->launches++;
     }
     relax_coarsest<T>(c, m, Lv - 1, mu2);

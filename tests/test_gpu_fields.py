@@ -20,8 +20,11 @@ TOL = 1e-12
 pytestmark = pytest.mark.gpu
 
 
-def make(n=4096, workload="small_4k", seed=12345):
+def make(n=4096, workload="small_4k", seed=12345, mg_levels=None):
     p = params.workload_params(workload)
+    if mg_levels:
+        p.mg_levels = mg_levels
+        params.finalize(p)
     cells = workload_colony(workload, n=n)
     orc = ck.Oracle(p, seed=seed)
     orc.load(cells)
@@ -83,8 +86,12 @@ def test_height_chain(gpu):
         assert np.array_equal(orc.field(F[f]), col.field(f)), f
 
 
-def test_mg_solve(gpu):
-    p, orc, col = make()
+@pytest.mark.parametrize("mg_levels", [None, 5])
+def test_mg_solve(gpu, mg_levels):
+    """Multigrid::solve, 3 V-cycles, against the oracle on every level.  With
+    5 levels the coarsest level is 33 x 5, wide enough for the cluster form
+    of the coarsest-level relaxation; with the reference's 8 it is 5 x 1."""
+    p, orc, col = make(mg_levels=mg_levels)
     orc.update_density()
     col.update_density()
     deplete(p, orc, col)
