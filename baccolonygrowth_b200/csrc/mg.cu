@@ -505,51 +505,23 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
     }
 }
 
-/* The point update of relax_smem with the neighbour columns i-1 and i+1
- * read from the arrays El and Er (the block's own shared memory, or the
- * shared memory of the cluster block that owns that column). */
+/* k_mg_coarse_wave spread over a thread-block cluster per species.  Block
+ * `rank` owns the columns [c0, c1) = [rank W / C, (rank+1) W / C) and keeps
+ * the whole level in its shared memory.  The wavefront steps run in
+ * blocks of H steps: in a block, a cluster block relaxes its own columns
+ * and H columns on each side (a halo), all from its own shared memory, with
+ * a block barrier between steps.  A value can only move one column per
+ * step (no item of a step reads what another writes), so the stale values
+ * beyond the halo reach at most H columns in, and the owned columns stay
+ * exact.  Between blocks every cluster block publishes its first and last H
+ * owned columns to a publish buffer (two, alternating, so a slow reader of
+ * the previous ones is never overwritten), one cluster barrier, and each
+ * block copies its halos from its neighbours' buffers.  Every block runs
+ * the same barriers; the last one comes after every read of another
+ * block's shared memory, so no block leaves while read.  H <= W / C keeps
+ * a halo inside the neighbouring block's columns. */
 template <class T>
-__device__ __forceinline__ void relax_cl(const RelaxK<T>& K, bool oxy, bool top_levels,
-                                         int nx, int nz, int i, int k, T* Es, const T* El, const T* Er,
-                                         const T* Rs, const unsigned char* ins_row0)
-{
-    const int W = nx + 1;
-    const bool side = (i == 0 || i == nx);
-    const T r = Rs[k * W + i];
-    T out = Es[k * W + i];
-    if (k == 0) {
-        if (ins_row0[i]) out = r;
-        else if (side) {
-            if (top_levels) out = oxy ? r : rx_corner(r, (i == 0) ? Er[i + 1] : El[i - 1], at_s(Es, nx, nz, i, 1), K);
-        } else out = oxy ? r : rx_k0(r, at_s(Es, nx, nz, i, 1), El[i - 1], Er[i + 1], K);
-    } else {
-        const T below = Es[(k - 1) * W + i];
-        if (k == nz) {
-            if (top_levels) {
-                if (side) out = oxy ? r : rx_corner(r, (i == 0) ? Er[k * W + i + 1] : El[k * W + i - 1], below, K);
-                else out = rx_top(r, below, El[k * W + i - 1], Er[k * W + i + 1], K);
-            }
-        } else if (side) {
-            if (top_levels) out = oxy ? r : rx_side(r, below, Es[(k + 1) * W + i], (i == 0) ? Er[k * W + i + 1] : El[k * W + i - 1], K);
-        } else {
-            out = rx_in(r, below, Es[(k + 1) * W + i], El[k * W + i - 1], Er[k * W + i + 1], K);
-        }
-    }
-    Es[k * W + i] = out;
-}
-
-/* k_mg_coarse_wave spread over a thread-block cluster per species: block
- * `rank` of the cluster owns the columns [rank W / C, (rank+1) W / C) and
- * relaxes only those, in the same wavefront order; a neighbour column
- * owned by the next block is read from that block's shared memory.  One
- * cluster barrier per step orders the steps (the wavefront never writes,
- * in a step, a value another item of the step reads).  Every block keeps
- * the whole level in its shared memory (loaded once); only its own columns
- * of it are kept current and written back.  Every block runs the same
- * number of barriers and none leaves before the last one, after which no
- * block reads another's shared memory. */
-template <class T>
-__global__ void __launch_bounds__(256) k_mg_coarse_cluster(MgConst m, MgLvlT<T> L, int l, int sweeps,
+__global__ void __launch_bounds__(384) k_mg_coarse_cluster(MgConst m, MgLvlT<T> L, int l, int sweeps, int H,
                                                             const double* __restrict__ inside0)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -557,11 +529,12 @@ __global__ void __launch_bounds__(256) k_mg_coarse_cluster(MgConst m, MgLvlT<T> 
     const int C = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
     const int sp = blockIdx.x / C;
-    const int nx = L.nx, nz = L.nz, W = nx + 1;
-    const int np = W * (nz + 1);
+    const int nx = L.nx, nz = L.nz, W = nx + 1, NZ = nz + 1;
+    const int np = W * NZ;
     T* Es = reinterpret_cast<T*>(smem_raw);
     T* Rs = Es + np;
-    unsigned char* ins = reinterpret_cast<unsigned char*>(Rs + np);
+    T* pub = Rs + np;                      /* [2 buffers][left, right][H][NZ] */
+    unsigned char* ins = reinterpret_cast<unsigned char*>(pub + 4 * H * NZ);
     T* E = SP(L.e);
     const T* R = SP(L.r);
     const int nth = blockDim.x, th = threadIdx.x;
@@ -576,50 +549,63 @@ __global__ void __launch_bounds__(256) k_mg_coarse_cluster(MgConst m, MgLvlT<T> 
         i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
         ins[i] = inside0[(size_t)i0 * m.box_z] > 0;
     }
-    cluster.sync();              /* every block loaded before any reads another */
-    const T* El = rank > 0 ? cluster.map_shared_rank(Es, rank - 1) : Es;
-    const T* Er = rank < C - 1 ? cluster.map_shared_rank(Es, rank + 1) : Es;
+    __syncthreads();
     const int c0 = rank * W / C, c1 = (rank + 1) * W / C;
+    const int e0 = max(0, c0 - H), e1 = min(W, c1 + H);
+    const T* pubL_left = rank > 0 ? cluster.map_shared_rank(pub, rank - 1) : pub;   /* left neighbour's buffers */
+    const T* pubR_right = rank < C - 1 ? cluster.map_shared_rank(pub, rank + 1) : pub;
     const RelaxK<T> K = relax_k<T>(m, l, sp);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
-    /* the block's columns of each parity: first, first + 2, ... below c1 */
     int first[2], ncol[2], a0[2], cc0[2];
     for (int par = 0; par < 2; par++) {
-        first[par] = c0 + ((c0 & 1) != par ? 1 : 0);
-        ncol[par] = first[par] < c1 ? (c1 - first[par] + 1) / 2 : 0;
+        first[par] = e0 + ((e0 & 1) != par ? 1 : 0);
+        ncol[par] = first[par] < e1 ? (e1 - first[par] + 1) / 2 : 0;
         a0[par] = ncol[par] ? th / ncol[par] : 0x7fffffff;
         cc0[par] = ncol[par] ? th % ncol[par] : 0;
     }
     const int steps = nz + 1 + 2 * (sweeps - 1) + 1;
-    for (int t = 0; t < steps; t++) {
+    for (int b = 0, t0 = 0; t0 < steps; b++, t0 += H) {
+        const int t_end = min(steps, t0 + H);
+        for (int t = t0; t < t_end; t++) {
 #pragma unroll
-        for (int par = 0; par < 2; par++) {
-            const int tp = t - par;
-            if (tp >= 0 && ncol[par]) {
-                const int s_lo = tp > nz ? (tp - nz + 1) / 2 : 0;
-                const int s_hi = min(sweeps - 1, tp / 2);
-                const int na = s_hi - s_lo + 1;
-                const int i = first[par] + 2 * cc0[par];
-                if (a0[par] < na) {
-                    const int k = tp - 2 * (s_lo + a0[par]);
-                    const T* xl = (i - 1 < c0) ? El : Es;
-                    const T* xr = (i + 1 >= c1) ? Er : Es;
-                    relax_cl<T>(K, oxy, top_levels, nx, nz, i, k, Es, xl, xr, Rs, ins);
-                }
-                /* more items than threads (large levels) */
-                for (int q = th + nth; q < na * ncol[par]; q += nth) {
-                    const int ii = first[par] + 2 * (q % ncol[par]);
-                    const int k = tp - 2 * (s_lo + q / ncol[par]);
-                    const T* xl = (ii - 1 < c0) ? El : Es;
-                    const T* xr = (ii + 1 >= c1) ? Er : Es;
-                    relax_cl<T>(K, oxy, top_levels, nx, nz, ii, k, Es, xl, xr, Rs, ins);
+            for (int par = 0; par < 2; par++) {
+                const int tp = t - par;
+                if (tp >= 0 && ncol[par]) {
+                    const int s_lo = tp > nz ? (tp - nz + 1) / 2 : 0;
+                    const int s_hi = min(sweeps - 1, tp / 2);
+                    const int na = s_hi - s_lo + 1;
+                    if (a0[par] < na)
+                        relax_smem<T>(K, oxy, top_levels, nx, nz, first[par] + 2 * cc0[par], tp - 2 * (s_lo + a0[par]), Es, Rs, ins);
+                    for (int q = th + nth; q < na * ncol[par]; q += nth)
+                        relax_smem<T>(K, oxy, top_levels, nx, nz, first[par] + 2 * (q % ncol[par]),
+                                      tp - 2 * (s_lo + q / ncol[par]), Es, Rs, ins);
                 }
             }
+            __syncthreads();
         }
-        cluster.sync();
+        if (t_end < steps) {
+            /* publish the first and last H owned columns, then take the halos */
+            T* mine = pub + (b & 1) * 2 * H * NZ;
+            for (int q = th; q < H * NZ; q += nth) {
+                const int h = q / NZ, k = q % NZ;
+                mine[q] = Es[k * W + c0 + h];
+                mine[H * NZ + q] = Es[k * W + c1 - H + h];
+            }
+            cluster.sync();
+            const T* lsrc = pubL_left + (b & 1) * 2 * H * NZ + H * NZ;   /* left neighbour's last H columns */
+            const T* rsrc = pubR_right + (b & 1) * 2 * H * NZ;           /* right neighbour's first H columns */
+            for (int q = th; q < H * NZ; q += nth) {
+                const int h = q / NZ, k = q % NZ;
+                const int xl = c0 - H + h, xr = c1 + h;
+                if (xl >= e0) Es[k * W + xl] = lsrc[q];
+                if (xr < e1) Es[k * W + xr] = rsrc[q];
+            }
+            __syncthreads();
+        }
     }
-    for (int q = th; q < (c1 - c0) * (nz + 1); q += nth) {
+    cluster.sync();              /* no block leaves while another may read its buffers */
+    for (int q = th; q < (c1 - c0) * NZ; q += nth) {
         const int i = c0 + q % (c1 - c0), k = q / (c1 - c0);
         AT(E, L, i, k) = Es[k * W + i];
     }
@@ -1422,8 +1408,16 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     return ctx_check_status(c);
 }
 
-/* blocks per cluster of the coarsest-level solve */
+/* blocks per cluster of the coarsest-level solve, threads per block */
 #define COARSE_CLUSTER 8
+#define COARSE_THREADS 384
+/* wavefront steps between cluster barriers (the halo width): at most 8,
+ * and no wider than the narrowest block's columns */
+static int coarse_halo(int W)
+{
+    int h = W / COARSE_CLUSTER;
+    return h < 8 ? h : 8;
+}
 /* whether clusters of COARSE_CLUSTER blocks with `smem` bytes each can be
  * resident (checked once per shared-memory size) */
 template <class T>
@@ -1440,7 +1434,7 @@ static bool coarse_cluster_ok(size_t smem)
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(3 * COARSE_CLUSTER, 1, 1);
-    cfg.blockDim = dim3(256, 1, 1);
+    cfg.blockDim = dim3(COARSE_THREADS, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1461,12 +1455,14 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
 {
     MgLvlT<T> L = lvl<T>(c, l);
     const size_t smem = 2 * sizeof(T) * (size_t)(L.nx + 1) * (L.nz + 1);
-    if (g_relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1 &&
-        L.nx + 1 >= 2 * COARSE_CLUSTER && coarse_cluster_ok<T>(smem + L.nx + 1)) {
+    const int H = coarse_halo(L.nx + 1);
+    const size_t csmem = smem + 4 * (size_t)H * (L.nz + 1) * sizeof(T) + L.nx + 1;
+    if (g_relax_mode >= 1 && csmem <= 200 * 1024 && L.nz >= 1 &&
+        L.nx + 1 >= 2 * COARSE_CLUSTER && coarse_cluster_ok<T>(csmem)) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(3 * COARSE_CLUSTER, 1, 1);
-        cfg.blockDim = dim3(256, 1, 1);
-        cfg.dynamicSmemBytes = smem + L.nx + 1;
+        cfg.blockDim = dim3(COARSE_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = csmem;
         cfg.stream = c->stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1475,7 +1471,7 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<T>, m, L, l, sweeps, (const double*)c->inside);
+        cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<T>, m, L, l, sweeps, H, (const double*)c->inside);
         c->launches++;
     } else if (g_relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1) {
         k_mg_coarse_wave<T><<<3, 1024, smem + (L.nx + 1), c->stream>>>(m, L, l, sweeps, c->inside);
