@@ -521,7 +521,7 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_wave(MgConst m, MgLvlT<T> L,
  * block's shared memory, so no block leaves while read.  H <= W / C keeps
  * a halo inside the neighbouring block's columns. */
 template <class T>
-__global__ void __launch_bounds__(384) k_mg_coarse_cluster(MgConst m, MgLvlT<T> L, int l, int sweeps, int H,
+__global__ void __launch_bounds__(768) k_mg_coarse_cluster(MgConst m, MgLvlT<T> L, int l, int sweeps, int H,
                                                             const double* __restrict__ inside0)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -557,30 +557,26 @@ __global__ void __launch_bounds__(384) k_mg_coarse_cluster(MgConst m, MgLvlT<T> 
     const RelaxK<T> K = relax_k<T>(m, l, sp);
     const bool oxy = (sp == 1);
     const bool top_levels = l >= m.A - 1;
-    int first[2], ncol[2], a0[2], cc0[2];
-    for (int par = 0; par < 2; par++) {
-        first[par] = e0 + ((e0 & 1) != par ? 1 : 0);
-        ncol[par] = first[par] < e1 ? (e1 - first[par] + 1) / 2 : 0;
-        a0[par] = ncol[par] ? th / ncol[par] : 0x7fffffff;
-        cc0[par] = ncol[par] ? th % ncol[par] : 0;
-    }
+    /* the first half of the threads relaxes the even columns, the second
+     * half the odd ones: the two halves of a step run side by side */
+    const int nhalf = nth / 2;
+    const int par = th < nhalf ? 0 : 1, tl = th - par * nhalf;
+    const int first = e0 + ((e0 & 1) != par ? 1 : 0);
+    const int ncol = first < e1 ? (e1 - first + 1) / 2 : 0;
+    const int a0 = ncol ? tl / ncol : 0x7fffffff, cc0 = ncol ? tl % ncol : 0;
     const int steps = nz + 1 + 2 * (sweeps - 1) + 1;
     for (int b = 0, t0 = 0; t0 < steps; b++, t0 += H) {
         const int t_end = min(steps, t0 + H);
         for (int t = t0; t < t_end; t++) {
-#pragma unroll
-            for (int par = 0; par < 2; par++) {
-                const int tp = t - par;
-                if (tp >= 0 && ncol[par]) {
-                    const int s_lo = tp > nz ? (tp - nz + 1) / 2 : 0;
-                    const int s_hi = min(sweeps - 1, tp / 2);
-                    const int na = s_hi - s_lo + 1;
-                    if (a0[par] < na)
-                        relax_smem<T>(K, oxy, top_levels, nx, nz, first[par] + 2 * cc0[par], tp - 2 * (s_lo + a0[par]), Es, Rs, ins);
-                    for (int q = th + nth; q < na * ncol[par]; q += nth)
-                        relax_smem<T>(K, oxy, top_levels, nx, nz, first[par] + 2 * (q % ncol[par]),
-                                      tp - 2 * (s_lo + q / ncol[par]), Es, Rs, ins);
-                }
+            const int tp = t - par;
+            if (tp >= 0 && ncol) {
+                const int s_lo = tp > nz ? (tp - nz + 1) / 2 : 0;
+                const int s_hi = min(sweeps - 1, tp / 2);
+                const int na = s_hi - s_lo + 1;
+                if (a0 < na)
+                    relax_smem<T>(K, oxy, top_levels, nx, nz, first + 2 * cc0, tp - 2 * (s_lo + a0), Es, Rs, ins);
+                for (int q = tl + nhalf; q < na * ncol; q += nhalf)
+                    relax_smem<T>(K, oxy, top_levels, nx, nz, first + 2 * (q % ncol), tp - 2 * (s_lo + q / ncol), Es, Rs, ins);
             }
             __syncthreads();
         }
@@ -1410,7 +1406,7 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
 
 /* blocks per cluster of the coarsest-level solve, threads per block */
 #define COARSE_CLUSTER 8
-#define COARSE_THREADS 384
+#define COARSE_THREADS 768
 /* wavefront steps between cluster barriers (the halo width): at most 8,
  * and no wider than the narrowest block's columns */
 static int coarse_halo(int W)
