@@ -1087,16 +1087,17 @@ __global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const doubl
     const ptrdiff_t P = L.pitch;
     double* R = &AT(SP(L.r), L, i, k);
     const double hi = sp == 0 ? m.max_carbon : (sp == 1 ? m.max_o2_agar : 1e300);
-    /* the solution value updateSolAga leaves at (i + di, k + dk): clamped
-     * where uncovered (everywhere on level 0) */
+    /* the solution value updateSolAga leaves at (i + di, k + dk), |di|,
+     * |dk| <= 1: clamped where uncovered (everywhere on level 0); the
+     * coverage of the three columns and rows is worked out once */
+    const bool cu_m = ip - 2 <= 0 || ip - 2 >= nxp, cu_0 = ip <= 0 || ip >= nxp, cu_p = ip + 2 <= 0 || ip + 2 >= nxp;
+    const bool ru_m = kp - 2 >= nzp, ru_0 = kp >= nzp, ru_p = kp + 2 >= nzp;
     auto sol = [&](int di, int dk) -> double {
         double v = ctr[di + dk * P];
         if (SETUP) {
-            bool clamp = LEVEL0;
-            if (!LEVEL0) {
-                const int ipa = ip + 2 * di, kpa = kp + 2 * dk;
-                clamp = ipa <= 0 || ipa >= nxp || kpa >= nzp;
-            }
+            const bool cu = di < 0 ? cu_m : (di > 0 ? cu_p : cu_0);
+            const bool ru = dk < 0 ? ru_m : (dk > 0 ? ru_p : ru_0);
+            const bool clamp = LEVEL0 || cu || ru;
             if (clamp) v = dmaxd(dmind(v, hi), 0.0);
         }
         return v;
