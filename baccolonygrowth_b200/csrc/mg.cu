@@ -1058,6 +1058,25 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l, MgLvl Ln, int nest)
     }
 }
 
+/* per-level constants of the residual pass, worked out on the host with
+ * the same operations the point code used: the finer level's extent nxp,
+ * nzp and, per species, D/h^2 and dt*D/h^2 (h^2 = BoxLength^2 4^l) */
+struct ResConst { int nxp, nzp; double cD[3], cdt[3]; };
+static ResConst res_const(const MgConst& m, int l)
+{
+    ResConst r;
+    const int X = m.box_x, ZA = m.box_z_agar;
+    const int d = 1 << l, d0 = 1 << m.A;
+    r.nxp = X * d0 / d < X ? X * d0 / d : X;
+    r.nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    const double h2 = m.bl2 * d * d;
+    for (int sp = 0; sp < 3; sp++) {
+        r.cD[sp] = m.D[sp] / h2;
+        r.cdt[sp] = m.dt * m.D[sp] / h2;
+    }
+    return r;
+}
+
 /* updateResAgaElementwise, Multigrid.cpp:570-701.  SETUP: the setup()
  * form after a reset() (Err zero everywhere, Res zero on levels > 0):
  * updateSolAga then only clamps the solution at the uncovered points and
@@ -1065,21 +1084,16 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l, MgLvl Ln, int nest)
  * stores the point's clamped value where the clamp changed it, and
  * writes Res (0 where updateResAga leaves it). */
 template <bool SETUP, bool LEVEL0>
-__global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, const double* __restrict__ inside0)
+__global__ void k_mg_update_res(MgConst m, MgLvl L, MgLvl Lp, int l, ResConst rc, const double* __restrict__ inside0)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     const int sp = blockIdx.z;
     const int nx = L.nx, nz = L.nz;
     if (i > nx || l >= m.A) return;
-    const int X = m.box_x, ZA = m.box_z_agar;
-    int d = 1 << l, d0 = 1 << m.A;
-    int nxp = X * d0 / d < X ? X * d0 / d : X;
-    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
-    const double h2 = m.bl2 * d * d;
-    const double D = SP(m.D);
+    const int nxp = rc.nxp, nzp = rc.nzp;
     /* the reference scales each residual by dt*D/h^2 (D/h^2 for oxygen's
-     * top row) per point; here once per level */
-    const double cD = D / h2, cdt = m.dt * D / h2;
+     * top row) per point; here once per level and species, on the host */
+    const double cD = SP(rc.cD), cdt = SP(rc.cdt);
     const bool oxy = sp == 1;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     const double* A = SP(L.s);
@@ -1546,12 +1560,13 @@ static void update_res(bcg_ctx* c, const MgConst& m, int l, bool setup_clean = f
 {
     MgLvl L = mg_lvl(c, l), Lp = mg_lvl(c, l > 0 ? l - 1 : 0);
     dim3 grid((unsigned)((L.nx + 1 + 127) / 128), (unsigned)(L.nz + 1), 3);
+    const ResConst rc = res_const(m, l);
     if (l == 0) {
-        if (setup_clean) k_mg_update_res<true, true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
-        else k_mg_update_res<false, true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+        if (setup_clean) k_mg_update_res<true, true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, rc, c->inside);
+        else k_mg_update_res<false, true><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, rc, c->inside);
     } else {
-        if (setup_clean) k_mg_update_res<true, false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
-        else k_mg_update_res<false, false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, c->inside);
+        if (setup_clean) k_mg_update_res<true, false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, rc, c->inside);
+        else k_mg_update_res<false, false><<<grid, 128, 0, c->stream>>>(m, L, Lp, l, rc, c->inside);
     }
     c->launches++;
 }
