@@ -894,8 +894,9 @@ __global__ void k_mg_restrict(MgConst m, MgLvlT<T> Lc, MgLvlT<T> Lf, int l, cons
     if (i > nx) return;
     const int X = m.box_x, ZA = m.box_z_agar;
     int d = 1 << l, d0 = 1 << m.A;
-    int nxp = X * d0 / d < X ? X * d0 / d : X;
-    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    /* X d0 / d with d = 2^l, as a shift */
+    int nxp = (X * d0) >> l < X ? (X * d0) >> l : X;
+    int nzp = (ZA * d0) >> l < ZA ? (ZA * d0) >> l : ZA;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     /* on a composite level only row 0 and the points over the finer level
      * (0 <= ip <= nxp, kp <= nzp) are written; the launch already stops at
@@ -980,8 +981,9 @@ __global__ void k_mg_interp(MgConst m, MgLvlT<T> Lf, MgLvlT<T> Lc, int l)
     if (i > nx) return;
     const bool has_odd = i + 1 <= nx;
     const int X = m.box_x;
-    int d = 1 << l, d0 = 1 << m.A;
-    int nxp = X * d0 / d / 4 < X ? X * d0 / d / 4 : X;
+    int d0 = 1 << m.A;
+    /* X d0 / 2^l / 4, as a shift */
+    int nxp = (X * d0) >> (l + 2) < X ? (X * d0) >> (l + 2) : X;
     const T* C = SP(Lc.e);
     T* e = SP(Lf.e) + (size_t)k * Lf.pitch + i;
     const T half = (T)0.5, quarter = (T)0.25;
@@ -1032,9 +1034,10 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l, MgLvl Ln, int nest)
     const int nx = L.nx;
     if (i > nx) return;
     const int X = m.box_x, ZA = m.box_z_agar;
-    int d = 1 << l, d0 = 1 << m.A;
-    int nxp = X * d0 / d < X ? X * d0 / d : X;
-    int nzp = ZA * d0 / d < ZA ? ZA * d0 / d : ZA;
+    int d0 = 1 << m.A;
+    /* X d0 / 2^l, as a shift */
+    int nxp = (X * d0) >> l < X ? (X * d0) >> l : X;
+    int nzp = (ZA * d0) >> l < ZA ? (ZA * d0) >> l : ZA;
     AT(SP(L.r), L, i, k) = 0;
     int ip = 2 * i - nx + nxp / 2, kp = 2 * k;
     double& e = AT(SP(L.e), L, i, k);
@@ -1047,9 +1050,8 @@ __global__ void k_mg_update_sol(MgConst m, MgLvl L, int l, MgLvl Ln, int nest)
     }
     e = 0;
     if (nest) {
-        const int dn = 2 * d;
-        const int nxpn = X * d0 / dn < X ? X * d0 / dn : X;
-        const int nzpn = ZA * d0 / dn < ZA ? ZA * d0 / dn : ZA;
+        const int nxpn = (X * d0) >> (l + 1) < X ? (X * d0) >> (l + 1) : X;
+        const int nzpn = (ZA * d0) >> (l + 1) < ZA ? (ZA * d0) >> (l + 1) : ZA;
         const int t = i + Ln.nx - nxpn / 2;
         if ((k & 1) == 0 && (t & 1) == 0 && i > 0 && i < nxpn && k < nzpn) {
             const int in = t >> 1, kn = k >> 1;
