@@ -278,6 +278,32 @@ def profiled_traffic(summary, workload):
     return total
 
 
+def colony_sweep_bench(lib, ctx, sweeps=200):
+    """The colony sweeps of the nutrient update (UpdateEnvironment_OxygenAcetate
+    and the wall rows, Multigrid.cpp:1017-1120) on the bench colony: points
+    of the field chain's bounding box x sweeps per second, with 73 B per
+    point-sweep (read C, W, A, O, DensityShiftP and the inside flag, write
+    the four species) against the HBM peak.  Reported, not required."""
+    from baccolonygrowth_b200 import _abi
+    try:
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _abi.check(lib.bcg_get_bbox(ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "bcg_get_bbox")
+        pts = (b.value - a.value + 1) * (c.value + 1)
+        _abi.check(lib.bcg_colony_sweeps(ctx, 2, 0), "sweep warm-up")
+        _abi.check(lib.bcg_enable_timers(ctx, 1), "timers")
+        _abi.check(lib.bcg_colony_sweeps(ctx, sweeps, 0), "sweeps")
+        ms = ctypes.c_double(); nl = ctypes.c_int64()
+        lib.bcg_get_timer(ctx, _abi.TIMERS["SWEEPS"], ctypes.byref(ms), ctypes.byref(nl))
+        _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
+        rate = pts * sweeps / (ms.value / 1e3)
+        peak, src = measured_peaks()
+        return {"points_in_bbox": pts, "sweeps": sweeps, "ms_per_sweep": ms.value / sweeps,
+                "point_sweeps_per_s": rate, "achieved_gb_s": 73.0 * rate / 1e9,
+                "frac": 73.0 * rate / 1e9 / peak, "peak_source": src}
+    except Exception as e:      # reported, not required
+        return {"error": str(e)}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -474,6 +500,7 @@ def b200_arm(args):
     _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
     n_now = ctypes.c_int()
     lib.bcg_num_cells(ctx, ctypes.byref(n_now))
+    colony = colony_sweep_bench(lib, ctx) if world == 1 else None
     lib.bcg_sim_destroy(sim)
 
     # end to end through the C ABI with host buffers: upload of the colony
@@ -628,6 +655,7 @@ def b200_arm(args):
         "mg_tolerance_solve": mg_tol,
         "ensemble": ens,
         "output_step": out_step,
+        "colony_sweeps": colony,
         "kernel_ms_per_step": timers,
         "divisions": d_.value,
         "roofline": roof,
