@@ -31,6 +31,7 @@ struct NutConst {
     double dac, dao, daa, daw;        /* agar diffusivities */
     double max_carbon, max_o2;
     double kw_ph, ka_ph, kb_ph, cb_ph, c1_ph;
+    double inv_bl2, inv_g1s, inv_g2s, inv_g3s;   /* 1/BoxLength^2, 1/g1s, 1/g2s, 1/g3s */
 };
 
 static NutConst nut_const(const bcg_ctx* c)
@@ -57,6 +58,8 @@ static NutConst nut_const(const bcg_ctx* c)
     n.dac = P.diff_agar_carbon; n.dao = P.diff_agar_o2; n.daa = P.diff_agar_ace; n.daw = P.diff_agar;
     n.max_carbon = P.max_carbon; n.max_o2 = P.max_o2;
     n.kw_ph = P.kw_ph; n.ka_ph = P.ka_ph; n.kb_ph = P.kb_ph; n.cb_ph = P.cb_ph; n.c1_ph = P.c1_ph;
+    n.inv_bl2 = 1.0 / (P.box_length * P.box_length);
+    n.inv_g1s = 1.0 / n.g1s; n.inv_g2s = 1.0 / n.g2s; n.inv_g3s = 1.0 / n.g3s;
     return n;
 }
 
@@ -108,22 +111,33 @@ struct EnvX { double *gca, *gcn, *gaa, *qcm, *qam, *pam, *qom; };
 
 /* UpdateEnvironment_OxygenAcetate (Nutrients.cpp:200-506), crossFeeding = 0,
  * for x in [minx, maxx], z in [0, maxz] where DensityShiftP > DBL_EPSILON
- * (Multigrid.cpp:1037-1047). */
-__global__ void k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur, EnvP prev, WallP pw0,
-                         const double* __restrict__ inside, const double* __restrict__ ds, int diag, EnvX ex,
-                         DevStatus* st)
+ * (Multigrid.cpp:1037-1047).
+ *
+ * Block (32, COLONY_COLS): a warp runs 32 consecutive z of one column (the
+ * contiguous direction), blockIdx.x the z chunk, blockIdx.y the column
+ * group.  DIAG adds the acetate buffer solve and the Environment-only
+ * members; the other sweeps run a variant without them, which needs fewer
+ * registers.  The second differences multiply by 1/BoxLength^2 and the
+ * maintenance caps min(Cgr/g1s, 1) .. by 1/g1s .., reciprocals taken once on
+ * the host, where the reference divides: the results differ from its
+ * quotients by rounding only (one unit in the last place per term). */
+#define COLONY_COLS 8
+template <bool DIAG>
+__global__ void __launch_bounds__(32 * COLONY_COLS) k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur,
+                                                             EnvP prev, WallP pw0, const double* __restrict__ inside,
+                                                             const double* __restrict__ ds, EnvX ex, DevStatus* st)
 {
     const int Z = n.Z;
-    int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= n.X * Z) return;
-    int x = id / Z, z = id % Z;
+    const int z = blockIdx.x * 32 + threadIdx.x;
+    const int x = blockIdx.y * COLONY_COLS + threadIdx.y;
+    if (z >= Z || x >= n.X) return;
+    const size_t id = (size_t)x * Z + z;
     int minx = bbox[0], maxx = bbox[1], maxz = bbox[2];
     if (x < minx || x > maxx || z > maxz) return;
     if (!(ds[id] > DBL_EPSILON)) return;
     /* stencil range guard (the bbox check reports a colony at the edge) */
     if (x < 1 || x > n.X - 2 || z > Z - 2) return;
     const double ins = inside[id];
-    const double BL = n.BL;
 #define IXZ(a, b) ((size_t)(a) * Z + (b))
     if (ins > 0.5) {
         double Cgr = 0, Agr = 0, Ogr = 0;   /* the waste average Wgr feeds nothing here */
@@ -138,7 +152,7 @@ __global__ void k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur, Env
                 Agr = (prev.A[IXZ(x - 1, z - 1)] + prev.A[IXZ(x - 1, z)] + prev.A[IXZ(x, z - 1)] + prev.A[id]) / 4.0;
             }
         }
-        if (diag) {
+        if (DIAG) {
             /* the second solve (for Agr) overwrites the first (for A) */
             double ph, hy, ac, bu;
             buffer_solve(n, Agr, ph, hy, ac, bu);
@@ -149,10 +163,10 @@ __global__ void k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur, Env
         double l1 = mx((n.max_gr_car_aer + n.mgrCarAers) * fCgr_aer - n.mgrCarAers, 0.0);
         double l2 = mx((n.max_gr_car_ana + n.mgrCarAnas) * fCgr_ana - n.mgrCarAnas, 0.0);
         double l3 = mx((n.max_gr_ace_aer + n.mgrAceAers) * fAgr - n.mgrAceAers, 0.0);
-        double qO = (n.q_o2_car * l1 * fCgr_aer + n.q_o2_ace * l3 * (1 - fCgr_aer)) * fOgr * mx(1 - fIgr, 0.0) + n.q_o2_car_nt * mn((Cgr / n.g1s), 1.0) * fCgr_aer * fOgr + n.q_o2_ace_nt * mn((Agr / n.g3s), 1.0) * (1 - fCgr_aer) * fOgr;
-        double qC = (n.q_car_aer * l1 * fCgr_aer * fOgr + n.q_car_ana * l2 * (1 - fOgr)) * mx(1 - fIgr, 0.0) + n.q_car_aer_nt * mn((Cgr / n.g1s), 1.0) * fCgr_aer * fOgr + n.q_car_ana_nt * mn((Cgr / n.g2s), 1.0) * (1 - fOgr);
-        double qA = (n.q_ace_aer * l3 * (1 - fCgr_aer) * fOgr) * mx(1 - fIgr, 0.0) + n.q_ace_aer_nt * mn((Agr / n.g3s), 1.0) * (1 - fCgr_aer) * fOgr;
-        double pA = (n.p_ace_aer * l1 * fCgr_aer * fOgr + n.p_ace_ana * l2 * (1 - fOgr)) * mx(1 - fIgr, 0.0) + n.p_ace_ana_nt * mn((Cgr / n.g2s), 1.0) * (1 - fOgr);
+        double qO = (n.q_o2_car * l1 * fCgr_aer + n.q_o2_ace * l3 * (1 - fCgr_aer)) * fOgr * mx(1 - fIgr, 0.0) + n.q_o2_car_nt * mn((Cgr * n.inv_g1s), 1.0) * fCgr_aer * fOgr + n.q_o2_ace_nt * mn((Agr * n.inv_g3s), 1.0) * (1 - fCgr_aer) * fOgr;
+        double qC = (n.q_car_aer * l1 * fCgr_aer * fOgr + n.q_car_ana * l2 * (1 - fOgr)) * mx(1 - fIgr, 0.0) + n.q_car_aer_nt * mn((Cgr * n.inv_g1s), 1.0) * fCgr_aer * fOgr + n.q_car_ana_nt * mn((Cgr * n.inv_g2s), 1.0) * (1 - fOgr);
+        double qA = (n.q_ace_aer * l3 * (1 - fCgr_aer) * fOgr) * mx(1 - fIgr, 0.0) + n.q_ace_aer_nt * mn((Agr * n.inv_g3s), 1.0) * (1 - fCgr_aer) * fOgr;
+        double pA = (n.p_ace_aer * l1 * fCgr_aer * fOgr + n.p_ace_ana * l2 * (1 - fOgr)) * mx(1 - fIgr, 0.0) + n.p_ace_ana_nt * mn((Cgr * n.inv_g2s), 1.0) * (1 - fOgr);
         double pW = n.carbon_to_waste * qC, qW = 0.0;
         double GrCarAer = l1 * fCgr_aer * fOgr * mx(1 - fIgr, 0.0);
         double GrCarAna = l2 * (1 - fOgr) * mx(1 - fIgr, 0.0);
@@ -160,11 +174,11 @@ __global__ void k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur, Env
         double gr = GrCarAer + GrCarAna + GrAceAer;
         cur.gr1[id] = gr;
         cur.gr2[id] = gr;
-        if (ex.gca) {
-            ex.qcm[id] = n.q_car_aer_nt * mn((Cgr / n.g1s), 1.0) * fCgr_aer * fOgr + n.q_car_ana_nt * mn((Cgr / n.g2s), 1.0) * (1 - fOgr);
-            ex.qam[id] = n.q_ace_aer_nt * mn((Agr / n.g3s), 1.0) * (1 - fCgr_aer) * fOgr;
-            ex.pam[id] = n.p_ace_ana_nt * mn((Cgr / n.g2s), 1.0) * (1 - fOgr);
-            ex.qom[id] = n.q_o2_car_nt * mn((Cgr / n.g1s), 1.0) * fCgr_aer * fOgr + n.q_o2_ace_nt * mn((Agr / n.g3s), 1.0) * (1 - fCgr_aer) * fOgr;
+        if (DIAG && ex.gca) {
+            ex.qcm[id] = n.q_car_aer_nt * mn((Cgr * n.inv_g1s), 1.0) * fCgr_aer * fOgr + n.q_car_ana_nt * mn((Cgr * n.inv_g2s), 1.0) * (1 - fOgr);
+            ex.qam[id] = n.q_ace_aer_nt * mn((Agr * n.inv_g3s), 1.0) * (1 - fCgr_aer) * fOgr;
+            ex.pam[id] = n.p_ace_ana_nt * mn((Cgr * n.inv_g2s), 1.0) * (1 - fOgr);
+            ex.qom[id] = n.q_o2_car_nt * mn((Cgr * n.inv_g1s), 1.0) * fCgr_aer * fOgr + n.q_o2_ace_nt * mn((Agr * n.inv_g3s), 1.0) * (1 - fCgr_aer) * fOgr;
             ex.gca[id] = GrCarAer; ex.gcn[id] = GrCarAna; ex.gaa[id] = GrAceAer;
         }
         if (!(x > 2)) { dev_error(st, BCG_E_NEED_MORE_BOXES, x); return; }
@@ -172,22 +186,22 @@ __global__ void k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur, Env
         const size_t up = IXZ(x, z + 1);
         double Czz, Wzz, Azz, Ozz;
         if (z == 0) {
-            Wzz = (prev.W[up] + pw0.W[x] - 2.0 * c0W) / (BL * BL);
-            Czz = (prev.C[up] + pw0.C[x] - 2.0 * c0C) / (BL * BL);
-            Azz = (prev.A[up] + pw0.A[x] - 2.0 * c0A) / (BL * BL);
-            Ozz = (prev.O[up] + pw0.O[x] - 2.0 * c0O) / (BL * BL);
+            Wzz = (prev.W[up] + pw0.W[x] - 2.0 * c0W) * n.inv_bl2;
+            Czz = (prev.C[up] + pw0.C[x] - 2.0 * c0C) * n.inv_bl2;
+            Azz = (prev.A[up] + pw0.A[x] - 2.0 * c0A) * n.inv_bl2;
+            Ozz = (prev.O[up] + pw0.O[x] - 2.0 * c0O) * n.inv_bl2;
         } else {
             const size_t dn = IXZ(x, z - 1);
-            Wzz = (prev.W[up] + prev.W[dn] - 2.0 * c0W) / (BL * BL);
-            Czz = (prev.C[up] + prev.C[dn] - 2.0 * c0C) / (BL * BL);
-            Azz = (prev.A[up] + prev.A[dn] - 2.0 * c0A) / (BL * BL);
-            Ozz = (prev.O[up] + prev.O[dn] - 2.0 * c0O) / (BL * BL);
+            Wzz = (prev.W[up] + prev.W[dn] - 2.0 * c0W) * n.inv_bl2;
+            Czz = (prev.C[up] + prev.C[dn] - 2.0 * c0C) * n.inv_bl2;
+            Azz = (prev.A[up] + prev.A[dn] - 2.0 * c0A) * n.inv_bl2;
+            Ozz = (prev.O[up] + prev.O[dn] - 2.0 * c0O) * n.inv_bl2;
         }
         const size_t xp = IXZ(x + 1, z), xm = IXZ(x - 1, z);
-        double Cxx = (prev.C[xp] + prev.C[xm] - 2.0 * c0C) / (BL * BL);
-        double Wxx = (prev.W[xp] + prev.W[xm] - 2.0 * c0W) / (BL * BL);
-        double Axx = (prev.A[xp] + prev.A[xm] - 2.0 * c0A) / (BL * BL);
-        double Oxx = (prev.O[xp] + prev.O[xm] - 2.0 * c0O) / (BL * BL);
+        double Cxx = (prev.C[xp] + prev.C[xm] - 2.0 * c0C) * n.inv_bl2;
+        double Wxx = (prev.W[xp] + prev.W[xm] - 2.0 * c0W) * n.inv_bl2;
+        double Axx = (prev.A[xp] + prev.A[xm] - 2.0 * c0A) * n.inv_bl2;
+        double Oxx = (prev.O[xp] + prev.O[xm] - 2.0 * c0O) * n.inv_bl2;
         double DS = ds[id];
         double Cnew = c0C + (n.dcc * (Cxx + Czz) - qC * 0.25 * DS) * n.cdt;
         double CAcenew = c0A + (n.dca * (Axx + Azz) + pA * 0.25 * DS - qA * 0.25 * DS) * n.cdt;
@@ -318,6 +332,13 @@ static AgarRow agar_rows(bcg_ctx* c)
     return a;
 }
 
+static void colony(dim3 grid, dim3 block, bcg_ctx* c, const NutConst& n, EnvP cur, EnvP prev, WallP pw0, int diag,
+                   EnvX ex)
+{
+    if (diag) k_colony<true><<<grid, block, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, ex, c->status);
+    else k_colony<false><<<grid, block, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, ex, c->status);
+}
+
 /* `nsweeps` sweeps with the local buffer indices (ce = current colony
  * buffer, cw = current wall buffer) and sweep counter, as the reference's
  * loop keeps them (Multigrid.cpp:1017-1120); diag_from = first sweep index
@@ -327,7 +348,8 @@ static void run_sweeps(bcg_ctx* c, int nsweeps, int& ce, int& cwb, int& count, i
     NutConst n = nut_const(c);
     const int X = c->P.box_x, Z = c->P.box_z;
     AgarRow ag = agar_rows(c);
-    unsigned gcol = (unsigned)((X * Z + 255) / 256), gwal = (unsigned)((X * n.A + 255) / 256);
+    const dim3 gcol((unsigned)((Z + 31) / 32), (unsigned)((X + COLONY_COLS - 1) / COLONY_COLS)), bcol(32, COLONY_COLS);
+    unsigned gwal = (unsigned)((X * n.A + 255) / 256);
     for (int j = 0; j < nsweeps; j++) {
         EnvP cur = envp(c, ce), prev = envp(c, ce ^ 1);
         WallAll cw = wall_all(c, cwb), pw = wall_all(c, cwb ^ 1);
@@ -340,9 +362,9 @@ static void run_sweeps(bcg_ctx* c, int nsweeps, int& ce, int& cwb, int& count, i
         }
         if (count % 2 == 0) {
             k_wall<<<gwal, 256, 0, c->stream>>>(n, cur, ag, cw, pw, c->inside);
-            k_colony<<<gcol, 256, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, diag, ex, c->status);
+            colony(gcol, bcol, c, n, cur, prev, pw0, diag, ex);
         } else {
-            k_colony<<<gcol, 256, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, diag, ex, c->status);
+            colony(gcol, bcol, c, n, cur, prev, pw0, diag, ex);
             k_wall<<<gwal, 256, 0, c->stream>>>(n, cur, ag, cw, pw, c->inside);
         }
         c->launches += 2;

@@ -4,8 +4,9 @@ deposition and surface fields (Compute.cpp), the composite-grid multigrid
 
 Tolerance: 1e-12 relative (the sums over a box run in a different order
 than the reference's box lists; everything else keeps the reference's
-operation order).  The level > 0 wall interior, where the reference reads
-uninitialised locals, is excluded.
+operation order); 1e-11 after colony sweeps, which multiply by
+1/BoxLength^2 and 1/g_s where the reference divides.  The level > 0 wall
+interior, where the reference reads uninitialised locals, is excluded.
 """
 import numpy as np
 import pytest
