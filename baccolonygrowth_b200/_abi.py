@@ -219,6 +219,11 @@ PROTOTYPES = {
     "bcg_sim_run": (_I, [_VP, _I]),
     "bcg_sim_ctx": (_VP, [_VP]),
     "bcg_sim_time": (_I, [_VP, _PD, _PI, _PI64]),
+    "bcg_sim_counters": (_I, [_VP, _PI64, _PI64]),
+    "bcg_set_force_group": (_I, [_VP, _I]),
+    "bcg_set_relax_mode": (_I, [_VP, _I]),
+    "bcg_set_smoother_warps": (_I, [_VP, _I]),
+    "bcg_smoother_launch_ms": (_I, [_VP, _PD]),
     "bcg_sim_lineage": (_I, [_VP, _PI, _I, _PI]),
     "bcg_sim_set_step_mode": (_I, [_VP, _I, _I]),
     "bcg_save_restart": (_I, [ctypes.c_char_p, _D, _D, _VP, _I]),
@@ -256,12 +261,8 @@ class OutputData(ctypes.Structure):
 
 # library entry points outside include/bcg.h, used by tests and the benchmark
 EXTRA_PROTOTYPES = {
-    "bcg_set_force_group": (_I, [_I]),
     "bcg_kernel_launches": (ctypes.c_longlong, [_VP]),
     "bcg_set_bbox": (_I, [_VP, _I, _I, _I]),
-    "bcg_set_relax_mode": (_I, [_I]),
-    "bcg_set_smoother_warps": (_I, [_VP, _I]),
-    "bcg_smoother_launch_ms": (_I, [_VP, _PD]),
 }
 
 TUNE = dict(FORCE_GROUP=1, SMOOTHER=2)

@@ -15,24 +15,28 @@ from . import _abi, params as _params
 
 
 def synth_colony(n, width, height, seed=20261203, radius=0.5, len_lo=2.0, len_hi=4.0,
-                 l_divide=3.0, div_phase_spread=0.0):
+                 l_divide=3.0, div_phase_spread=0.0, entry=None):
     """Seeded synthetic colony (bcg_synth_colony): n cells in a half-ellipse
-    dome of width x height um on the agar, as bcg_cell records."""
+    dome of width x height um on the agar, as bcg_cell records.  `entry`
+    replaces the library's bcg_synth_colony by another C function of the
+    same signature (the benchmark's reference arm passes the oracle's)."""
     out = np.zeros(n, dtype=_abi.CELL_DTYPE)
     got = ctypes.c_int(0)
-    rc = _abi.load().bcg_synth_colony(ctypes.c_uint64(seed), n, width, height, radius, len_lo, len_hi,
-                                      l_divide, div_phase_spread, _abi.ptr(out), n, ctypes.byref(got))
+    fn = entry if entry is not None else _abi.load().bcg_synth_colony
+    rc = fn(ctypes.c_uint64(seed), n, ctypes.c_double(width), ctypes.c_double(height), ctypes.c_double(radius),
+            ctypes.c_double(len_lo), ctypes.c_double(len_hi), ctypes.c_double(l_divide),
+            ctypes.c_double(div_phase_spread), _abi.ptr(out), n, ctypes.byref(got))
     _abi.check(rc, "bcg_synth_colony")
     return out[:got.value]
 
 
-def workload_colony(name, seed=None, phi=0.45, div_phase_spread=1.0, n=None):
+def workload_colony(name, seed=None, phi=0.45, div_phase_spread=1.0, n=None, entry=None):
     """Cells of a named workload (params.WORKLOADS)."""
     cells, aspect, *_ = _params.WORKLOADS[name]
     n = n or cells
     w, h = _params.dome_size(n, aspect, phi)
     s = (20261203 + list(_params.WORKLOADS).index(name)) if seed is None else seed
-    return synth_colony(n, w, h, seed=s, div_phase_spread=div_phase_spread)
+    return synth_colony(n, w, h, seed=s, div_phase_spread=div_phase_spread, entry=entry)
 
 
 def depleted_wall(p, inside, depth_c=0.6, depth_o=0.8, acetate=2.0):

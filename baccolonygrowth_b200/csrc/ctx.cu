@@ -107,9 +107,6 @@ extern "C" int bcg_get_timer(bcg_ctx* c, int t, double* ms, int64_t* launches)
     if (launches) *launches = c->timer_launches[t];
     return BCG_OK;
 }
-static int g_kernel_gen = 0;
-int bcg_kernel_config_generation() { return g_kernel_gen; }
-void bcg_kernel_config_changed() { g_kernel_gen++; }
 
 extern "C" void* bcg_stream(bcg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 extern "C" int bcg_synchronize(bcg_ctx* c) { return c ? ctx_check_status(c) : BCG_E_ARG; }
@@ -153,6 +150,7 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
     bcg_ctx* c = (bcg_ctx*)calloc(1, sizeof(bcg_ctx));
     if (!c) return BCG_E_ARG;
     c->P = *p;
+    c->relax_mode = 2;
     cudaGetDevice(&c->device);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { free(c); return BCG_E_CUDA; }
     for (int t = 0; t < BCG_T_COUNT; t++) { cudaEventCreate(&c->ev[t][0]); cudaEventCreate(&c->ev[t][1]); }

@@ -97,8 +97,7 @@ struct bcg_ctx {
     /* captured [solve + sweeps] units of the nutrient update: [0] plain,
      * [1] with the acetate buffer solve in its last two sweeps */
     cudaGraphExec_t nutrient_graph[2];
-    int nutrient_graph_sweeps;
-    int nutrient_graph_gen;              /* kernel-choice generation the graphs were captured under */
+    int nutrient_graph_sweeps;           /* 0: none captured (dropped whenever a kernel choice changes) */
     int nutrient_graph_launches[2];
     /* timers */
     int timers_on;
@@ -106,9 +105,13 @@ struct bcg_ctx {
     double timer_ms[BCG_T_COUNT];
     long long timer_launches[BCG_T_COUNT];
     long long launches;    /* kernels queued by this context (all kinds) */
-    /* kernel shapes chosen by bcg_autotune for this context (0 = default) */
+    /* kernel shapes of this context, chosen by bcg_autotune or set by the
+     * caller (0 = default); no kernel choice is process-wide */
     int force_group;
     int smooth_warps;
+    int relax_mode;        /* agar smoother form, bcg_set_relax_mode (2 by default) */
+    size_t cluster_smem[2];/* coarsest-level cluster kernel: shared-memory size checked */
+    int cluster_ok[2];     /* ... and whether its clusters fit (FP64, FP32) */
     /* multigrid Err (all levels) and Res (levels > 0) are zero, as the last
      * reset() left them; setup() then skips its resetZero */
     int mg_clean;
@@ -124,9 +127,6 @@ int ctx_check_status(bcg_ctx* c);   /* syncs, reads the device status word */
 void timer_begin(bcg_ctx* c, int t);
 void timer_end(bcg_ctx* c, int t, int launches);
 int ensure_pinned(bcg_ctx* c, size_t bytes);
-/* bumped whenever a kernel variant is switched (captured graphs go stale) */
-int bcg_kernel_config_generation();
-void bcg_kernel_config_changed();
 void nutrient_graphs_drop(bcg_ctx* c);
 int launch_move_grow(bcg_ctx* c, double dt, int group);
 /* output-step kernels queued on `s`: the colony as reference records,

@@ -9,7 +9,6 @@
 #include "cellmath.cuh"
 #include "internal.h"
 #include <string.h>
-#include <mutex>
 
 /* ======================================================================= */
 /* binning: counting sort of cell ids by UniformGrid address               */
@@ -384,12 +383,14 @@ __global__ void __launch_bounds__(128, 4) k_move_grow(int n, int nbinned, const 
     }
 }
 
-static int g_group = 4;   /* lanes per cell in the force loop (tunable) */
-extern "C" int bcg_set_force_group(int g)
+/* lanes per cell in the force loop: the context's choice (bcg_autotune or
+ * bcg_set_force_group), else 4 */
+static int force_group_of(const bcg_ctx* c) { return c->force_group ? c->force_group : 4; }
+extern "C" int bcg_set_force_group(bcg_ctx* c, int g)
 {
-    if (g != 1 && g != 2 && g != 4 && g != 8 && g != 16) return BCG_E_ARG;
-    if (g != g_group) bcg_kernel_config_changed();
-    g_group = g;
+    if (!c || (g != 1 && g != 2 && g != 4 && g != 8 && g != 16)) return BCG_E_ARG;
+    if (g != force_group_of(c)) nutrient_graphs_drop(c);
+    c->force_group = g;
     return BCG_OK;
 }
 
@@ -441,7 +442,7 @@ int launch_move_grow(bcg_ctx* c, double dt, int group)
  * finish waits for them */
 int move_grow_launch(bcg_ctx* c, double dt)
 {
-    int rc = launch_move_grow(c, dt, c->force_group ? c->force_group : g_group);
+    int rc = launch_move_grow(c, dt, force_group_of(c));
     if (rc) return rc;
     int* hp = (int*)c->pinned;
     BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->div_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -464,7 +465,7 @@ extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_cal
 {
     if (!c) return BCG_E_ARG;
     timer_begin(c, BCG_T_MOVE_GROW);
-    int rc = launch_move_grow(c, dt, c->force_group ? c->force_group : g_group);
+    int rc = launch_move_grow(c, dt, force_group_of(c));
     if (rc) return rc;
     timer_end(c, BCG_T_MOVE_GROW, c->n > 0 ? 1 : 0);
     /* the two counters are the only values the host needs this step */
@@ -505,7 +506,7 @@ extern "C" int bcg_autotune(bcg_ctx* c, int what, int* choice)
     if (!c) return BCG_E_ARG;
     if (what == BCG_TUNE_SMOOTHER) return mg_tune_smoother(c, choice);
     if (what != BCG_TUNE_FORCE_GROUP) return BCG_E_ARG;
-    if (c->n == 0) { if (choice) *choice = c->force_group ? c->force_group : g_group; return BCG_OK; }
+    if (c->n == 0) { if (choice) *choice = force_group_of(c); return BCG_OK; }
     const int saved_ndiv = c->last_ndiv;
     /* the trial launches rewrite the per-cell outputs of a step (growth
      * rate, friction accumulators): keep a copy and put it back */
@@ -517,7 +518,7 @@ extern "C" int bcg_autotune(bcg_ctx* c, int what, int* choice)
         BCG_CUDA_TRY(cudaMemcpyAsync(save + a * (size_t)c->n, keep[a], nb, cudaMemcpyDeviceToDevice, c->stream));
     const int groups[5] = {1, 2, 4, 8, 16};
     float best = 3.4e38f;
-    int best_g = g_group;
+    int best_g = force_group_of(c);
     int rc = BCG_OK;
     for (int gi = 0; gi < 5 && !rc; gi++) {
         float ms = 0;
@@ -532,7 +533,6 @@ extern "C" int bcg_autotune(bcg_ctx* c, int what, int* choice)
     if (rc) return rc;
     if (rc2) return rc2;
     if (best_g != c->force_group) { c->force_group = best_g; nutrient_graphs_drop(c); }
-    if (best_g != g_group) { g_group = best_g; bcg_kernel_config_changed(); }   /* default for new contexts */
     if (choice) *choice = best_g;
     return BCG_OK;
 }
@@ -795,11 +795,10 @@ __global__ void __launch_bounds__(128) k_div_groups(int n_start, const int* __re
  * parents and group fill counters, DIV_SORT_MAX ints each */
 int mech_kernel_attributes()
 {
-    static bool done = false;
-    if (done) return BCG_OK;
+    /* set on every context creation: the attribute belongs to the current
+     * device, and the call is cheap and thread-safe */
     if (cudaFuncSetAttribute(k_div_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, DIV_PLAN_SMEM) != cudaSuccess)
         return BCG_E_CUDA;
-    done = true;
     return BCG_OK;
 }
 
@@ -1003,22 +1002,17 @@ extern "C" int bcg_mean_stress(bcg_ctx* c, double* stress, double* fnet, int64_t
 /* 5 stress + 3 force doubles per cell, then the F_cw counter */
 static __device__ __align__(256) double g_noalloc_stress[8 * BCG_NOALLOC_MAX_CELLS + 32];
 
-#define NOALLOC_MAX_DEVICES 64
-static std::mutex g_noalloc_mu;
-static double* g_noalloc_addr[NOALLOC_MAX_DEVICES];
-
-/* the array's device address on device `dev` (current), looked up once */
-static int noalloc_staging(int dev, double** out)
+/* The array's device address on the current device.  Looked up on every
+ * call rather than kept: the lookup allocates nothing, and an address kept
+ * from before a cudaDeviceReset would point into a released context.  In
+ * host code the array's name is only a host-side stand-in; kernels must be
+ * given this address. */
+static int noalloc_staging(double** out)
 {
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return BCG_E_ARG;
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_stress);
-        if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
-        g_noalloc_addr[dev] = (double*)p;
-    }
-    *out = g_noalloc_addr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_stress);
+    if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
+    *out = (double*)p;
     return BCG_OK;
 }
 
@@ -1031,7 +1025,7 @@ extern "C" int bcg_mean_stress_noalloc(bcg_ctx* c, double* stress, double* fnet,
     BCG_CUDA_TRY(cudaGetDevice(&dev));
     if (dev != c->device) return BCG_E_ARG;
     double* base = nullptr;
-    int rc = noalloc_staging(dev, &base);
+    int rc = noalloc_staging(&base);
     if (rc) return rc;
     double* ds = base;
     double* df = base + 5 * (size_t)BCG_NOALLOC_MAX_CELLS;

@@ -1230,14 +1230,14 @@ static inline dim3 grid2(int n, int threads) { return dim3((unsigned)((n + threa
 static inline dim3 grid_rows(int ncols, int nrows, int threads)
 { return dim3((unsigned)((ncols + threads - 1) / threads), (unsigned)nrows, 3); }
 
-/* 0 = one thread per column and half-sweep, 1 = segmented half-sweeps,
- * 2 = fused sweeps (k_mg_smooth) on levels taller than 96 rows */
-static int g_relax_mode = 2;
-extern "C" int bcg_set_relax_mode(int mode)
+/* The context's smoother form: 0 = one thread per column and half-sweep,
+ * 1 = segmented half-sweeps, 2 = fused sweeps (k_mg_smooth) on levels
+ * taller than 96 rows (the default, set by bcg_create) */
+extern "C" int bcg_set_relax_mode(bcg_ctx* c, int mode)
 {
-    if (mode < 0 || mode > 2) return BCG_E_ARG;
-    if (mode != g_relax_mode) bcg_kernel_config_changed();
-    g_relax_mode = mode;
+    if (!c || mode < 0 || mode > 2) return BCG_E_ARG;
+    if (mode != c->relax_mode) nutrient_graphs_drop(c);
+    c->relax_mode = mode;
     return BCG_OK;
 }
 
@@ -1250,7 +1250,7 @@ static void relax_level(bcg_ctx* c, const MgConst& m, int l)
 {
     MgLvlT<T> L = lvl<T>(c, l);
     const int rows = L.nz + 1;
-    if (g_relax_mode == 0 || rows <= 96) {
+    if (c->relax_mode == 0 || rows <= 96) {
         for (int par = 0; par < 2; par++) {
             int ncol = (L.nx + 1 - par + 1) / 2;
             k_mg_relax<T><<<grid2(ncol, 64), 64, 0, c->stream>>>(m, L, l, par, c->inside);
@@ -1268,7 +1268,7 @@ static void relax_level(bcg_ctx* c, const MgConst& m, int l)
     c->launches += 2;
 }
 
-static int g_smooth_warps = 1400;   /* default resident-warp target of the fused smoother */
+#define SMOOTH_WARPS_DEFAULT 1400   /* resident-warp target of the fused smoother before tuning */
 
 template <class T> static void swap_err(bcg_ctx* c, int l);
 template <> void swap_err<double>(bcg_ctx* c, int l)
@@ -1313,7 +1313,7 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
     const int rows = c->mg[l].nz + 1;
     /* levels of 0-1 interior rows read across columns through the flat
      * index (at_ref); they keep the in-place kernels */
-    if (g_relax_mode != 2 || rows < 3) {
+    if (c->relax_mode != 2 || rows < 3) {
         for (int j = 0; j < sweeps; j++) relax_level<T>(c, m, l);
         return;
     }
@@ -1322,7 +1322,7 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         MgLvlT<T> L = lvl<T>(c, l);
         const int outp = 32 - 2 * S;
         const int nwx = (L.nx + 1 + 2 * outp - 1) / (2 * outp);
-        const int target = c->smooth_warps > 0 ? c->smooth_warps : g_smooth_warps;
+        const int target = c->smooth_warps > 0 ? c->smooth_warps : SMOOTH_WARPS_DEFAULT;
         const int warm = warm_rows(m, l);
         int nseg = (target + 3 * nwx - 1) / (3 * nwx);
         /* segments of at least 16 rows and no shorter than half the warm-up */
@@ -1342,7 +1342,6 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
     }
 }
 
-/* kernel attributes set once per process, outside any stream capture */
 /* device time (ms) of one level-0 launch of the fused 3-sweep smoother at
  * the shape bcg_autotune chose (0 before tuning) */
 extern "C" int bcg_smoother_launch_ms(bcg_ctx* c, double* ms)
@@ -1364,8 +1363,8 @@ extern "C" int bcg_set_smoother_warps(bcg_ctx* c, int warps)
 
 int mg_kernel_attributes()
 {
-    static bool done = false;
-    if (done) return BCG_OK;
+    /* set on every context creation: attributes belong to the current
+     * device, and the calls are cheap and thread-safe */
     if (cudaFuncSetAttribute(k_mg_coarse_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_coarse_smem<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_coarse_wave<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
@@ -1379,7 +1378,6 @@ int mg_kernel_attributes()
         cudaFuncSetAttribute(k_mg_smooth<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_f) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_smooth<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_f) != cudaSuccess)
         return BCG_E_CUDA;
-    done = true;
     return BCG_OK;
 }
 
@@ -1389,7 +1387,7 @@ int mg_kernel_attributes()
 int mg_tune_smoother(bcg_ctx* c, int* choice)
 {
     const int rows = c->mg[0].nz + 1;
-    if (g_relax_mode != 2 || rows <= 96) { if (choice) *choice = 0; return BCG_OK; }
+    if (c->relax_mode != 2 || rows <= 96) { if (choice) *choice = 0; return BCG_OK; }
     MgConst m = mg_const(c, c->P.mg_dt);
     const int targets[6] = {700, 1400, 2800, 5600, 8400, 11200};
     const int saved = c->smooth_warps;
@@ -1397,7 +1395,7 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     BCG_CUDA_TRY(cudaEventCreate(&a));
     BCG_CUDA_TRY(cudaEventCreate(&b));
     float best = 3.4e38f;
-    int best_t = saved > 0 ? saved : g_smooth_warps;
+    int best_t = saved > 0 ? saved : SMOOTH_WARPS_DEFAULT;
     for (int ti = 0; ti < 6; ti++) {
         c->smooth_warps = targets[ti];
         smooth_level<double>(c, m, 0, 3);                  /* warm-up */
@@ -1416,7 +1414,6 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     c->smooth_warps = best_t;
     c->mg_clean = 0;                 /* the trial sweeps wrote Err */
     nutrient_graphs_drop(c);
-    if (best_t != g_smooth_warps) { g_smooth_warps = best_t; bcg_kernel_config_changed(); }   /* default for new contexts */
     if (choice) *choice = best_t;
     return ctx_check_status(c);
 }
@@ -1432,18 +1429,18 @@ static int coarse_halo(int W)
     return h < 8 ? h : 8;
 }
 /* whether clusters of COARSE_CLUSTER blocks with `smem` bytes each can be
- * resident (checked once per shared-memory size) */
+ * resident on the context's device; the answer is kept on the context per
+ * precision and shared-memory size */
 template <class T>
-static bool coarse_cluster_ok(size_t smem)
+static bool coarse_cluster_ok(bcg_ctx* c, size_t smem)
 {
-    static size_t checked = 0;
-    static bool ok = false;
-    if (checked == smem) return ok;
-    checked = smem;
-    ok = false;
+    const int ti = sizeof(T) == 8 ? 0 : 1;
+    if (c->cluster_smem[ti] == smem) return c->cluster_ok[ti] != 0;
+    c->cluster_smem[ti] = smem;
+    c->cluster_ok[ti] = 0;
     if (cudaFuncSetAttribute(k_mg_coarse_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
-        return ok;
+        return false;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(3 * COARSE_CLUSTER, 1, 1);
@@ -1457,9 +1454,9 @@ static bool coarse_cluster_ok(size_t smem)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_mg_coarse_cluster<T>, &cfg) == cudaSuccess && n >= 3) ok = true;
+    if (cudaOccupancyMaxActiveClusters(&n, k_mg_coarse_cluster<T>, &cfg) == cudaSuccess && n >= 3) c->cluster_ok[ti] = 1;
     cudaGetLastError();
-    return ok;
+    return c->cluster_ok[ti] != 0;
 }
 
 /* mu2 sweeps on the coarsest level: fused when it fits one block */
@@ -1470,8 +1467,9 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
     const size_t smem = 2 * sizeof(T) * (size_t)(L.nx + 1) * (L.nz + 1);
     const int H = coarse_halo(L.nx + 1);
     const size_t csmem = smem + 4 * (size_t)H * (L.nz + 1) * sizeof(T) + L.nx + 1;
-    if (g_relax_mode >= 1 && csmem <= 200 * 1024 && L.nz >= 1 &&
-        L.nx + 1 >= 2 * COARSE_CLUSTER && coarse_cluster_ok<T>(csmem)) {
+    bool done = false;
+    if (c->relax_mode >= 1 && csmem <= 200 * 1024 && L.nz >= 1 &&
+        L.nx + 1 >= 2 * COARSE_CLUSTER && coarse_cluster_ok<T>(c, csmem)) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(3 * COARSE_CLUSTER, 1, 1);
         cfg.blockDim = dim3(COARSE_THREADS, 1, 1);
@@ -1484,18 +1482,26 @@ static void relax_coarsest(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<T>, m, L, l, sweeps, H, (const double*)c->inside);
-        c->launches++;
-    } else if (g_relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1) {
+        if (cudaLaunchKernelEx(&cfg, k_mg_coarse_cluster<T>, m, L, l, sweeps, H, (const double*)c->inside) == cudaSuccess) {
+            c->launches++;
+            done = true;
+        } else {
+            /* not launchable after all: use the one-block form from now on */
+            cudaGetLastError();
+            c->cluster_ok[sizeof(T) == 8 ? 0 : 1] = 0;
+        }
+    }
+    if (done) return;
+    if (c->relax_mode >= 1 && smem + L.nx + 1 <= 200 * 1024 && L.nz >= 1) {
         k_mg_coarse_wave<T><<<3, 1024, smem + (L.nx + 1), c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
-    } else if (g_relax_mode >= 1 && smem <= 200 * 1024) {
+    } else if (c->relax_mode >= 1 && smem <= 200 * 1024) {
         int ncol = (L.nx + 2) / 2;
         int threads = ((ncol + 31) / 32) * 32;
         if (threads > 1024) threads = 1024;
         k_mg_coarse_smem<T><<<3, threads, smem, c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
-    } else if (g_relax_mode >= 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
+    } else if (c->relax_mode >= 1 && 3 * ((L.nx + 2) / 2) <= 4096 && L.nz + 1 <= 96) {
         k_mg_relax_coarse<T><<<1, 1024, 0, c->stream>>>(m, L, l, sweeps, c->inside);
         c->launches++;
     } else {

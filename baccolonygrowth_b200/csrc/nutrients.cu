@@ -401,11 +401,9 @@ void nutrient_graphs_drop(bcg_ctx* c)
 
 static int nutrient_unit_graph(bcg_ctx* c, int sweeps, int last, cudaGraphExec_t* out)
 {
-    if (c->nutrient_graph_sweeps != sweeps || c->nutrient_graph_gen != bcg_kernel_config_generation()) {
-        for (int g = 0; g < 2; g++)
-            if (c->nutrient_graph[g]) { cudaGraphExecDestroy(c->nutrient_graph[g]); c->nutrient_graph[g] = nullptr; }
+    if (c->nutrient_graph_sweeps != sweeps) {
+        nutrient_graphs_drop(c);
         c->nutrient_graph_sweeps = sweeps;
-        c->nutrient_graph_gen = bcg_kernel_config_generation();
     }
     if (!c->nutrient_graph[last]) {
         cudaGraph_t g;

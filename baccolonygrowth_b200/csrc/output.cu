@@ -92,14 +92,12 @@ static int snapshot_fields(bcg_ctx* c, const bcg_out_layout* L, char* d)
     return BCG_OK;
 }
 
-extern "C" int bcg_int_out_snapshot(bcg_ctx* c, const bcg_out_layout* L, void* host, void* copy_stream,
-                                    void* done_event, int64_t* fcw_calls)
+/* queues the snapshot of one output step into the device staging buffer
+ * `d` on the context's stream (cells, stress or surface force, restart
+ * records, field planes) */
+static int snapshot_queue(bcg_ctx* c, const bcg_out_layout* L, char* d, bool stress)
 {
-    if (!c || !L || !host || !copy_stream || !done_event) return BCG_E_ARG;
-    cudaStream_t s = c->stream, cs = (cudaStream_t)copy_stream;
-    const bool stress = (L->what & BCG_OUT_CELLS) && !L->initial;
-    char* d = nullptr;
-    if (L->bytes) BCG_CUDA_TRY(cudaMallocAsync((void**)&d, L->bytes, s));
+    cudaStream_t s = c->stream;
     if (stress) BCG_CUDA_TRY(cudaMemsetAsync(c->fcw_count, 0, sizeof(unsigned long long), s));
     if (L->what & BCG_OUT_CELLS) {
         launch_pack_cells(c, (bcg_cell*)(d + L->off_cells), s, 0);
@@ -114,22 +112,46 @@ extern "C" int bcg_int_out_snapshot(bcg_ctx* c, const bcg_out_layout* L, void* h
         if (rc) return rc;
     }
     BCG_CUDA_TRY(cudaGetLastError());
-    /* hand the staging buffer to the copy stream */
+    return BCG_OK;
+}
+
+/* hands the staging buffer to the copy stream: device-to-host copy into
+ * `host`, then the buffer is released on that stream */
+static int snapshot_hand_over(bcg_ctx* c, const bcg_out_layout* L, char* d, void* host, cudaStream_t cs)
+{
     cudaEvent_t snap;
     BCG_CUDA_TRY(cudaEventCreateWithFlags(&snap, cudaEventDisableTiming));
-    cudaError_t e = cudaEventRecord(snap, s);
+    cudaError_t e = cudaEventRecord(snap, c->stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, snap, 0);
     cudaEventDestroy(snap);
     if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
-    if (L->bytes) {
-        BCG_CUDA_TRY(cudaMemcpyAsync(host, d, L->bytes, cudaMemcpyDeviceToHost, cs));
-        BCG_CUDA_TRY(cudaFreeAsync(d, cs));
+    if (L->bytes) BCG_CUDA_TRY(cudaMemcpyAsync(host, d, L->bytes, cudaMemcpyDeviceToHost, cs));
+    return BCG_OK;
+}
+
+extern "C" int bcg_int_out_snapshot(bcg_ctx* c, const bcg_out_layout* L, void* host, void* copy_stream,
+                                    void* done_event, int64_t* fcw_calls)
+{
+    if (!c || !L || !host || !copy_stream || !done_event) return BCG_E_ARG;
+    cudaStream_t s = c->stream, cs = (cudaStream_t)copy_stream;
+    const bool stress = (L->what & BCG_OUT_CELLS) && !L->initial;
+    char* d = nullptr;
+    if (L->bytes) BCG_CUDA_TRY(cudaMallocAsync((void**)&d, L->bytes, s));
+    int rc = snapshot_queue(c, L, d, stress);
+    if (rc == BCG_OK) rc = snapshot_hand_over(c, L, d, host, cs);
+    /* the one release of the staging buffer: on the copy stream after its
+     * copy, or on the context's stream (after what was queued there) when
+     * the hand-over did not happen */
+    if (d) {
+        cudaError_t e = cudaFreeAsync(d, rc == BCG_OK ? cs : s);
+        if (e != cudaSuccess && rc == BCG_OK) { bcg_set_cuda_error(e); rc = BCG_E_CUDA; }
     }
+    if (rc) return rc;
     BCG_CUDA_TRY(cudaEventRecord((cudaEvent_t)done_event, cs));
     if (!stress) return BCG_OK;
     unsigned long long h = 0;
     BCG_CUDA_TRY(cudaMemcpyAsync(&h, c->fcw_count, sizeof(h), cudaMemcpyDeviceToHost, s));
-    int rc = ctx_check_status(c);
+    rc = ctx_check_status(c);
     if (fcw_calls) *fcw_calls = (int64_t)h;
     return rc;
 }

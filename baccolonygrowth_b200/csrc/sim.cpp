@@ -29,8 +29,13 @@ struct bcg_sim {
     int vcycles_per_step;
     bool first_step;
     long long divisions;
+    long long rebuilds;            /* full neighbour rebuilds run */
+    long long field_updates;       /* field updates (UpdateFlag blocks) run */
     std::vector<int> lineage;
     std::vector<float> draws;
+    /* status of a step that failed part-way (the colony may be between
+     * MoveCell and the division loop): every later run returns it */
+    int failed;
 };
 
 static float frand(bcg_rng* g) { return (float)bcg_rng_next(g) / (float)2147483647; }
@@ -74,6 +79,9 @@ extern "C" int bcg_sim_create(const bcg_params* p, const bcg_cell* cells, int n,
     s->vcycles_per_step = 0;
     s->first_step = true;
     s->divisions = 0;
+    s->rebuilds = 0;
+    s->field_updates = 0;
+    s->failed = BCG_OK;
     *out = s;
     return BCG_OK;
 }
@@ -145,6 +153,8 @@ static int sim_step(bcg_sim* s)
             if ((rc = bcg_update_density(s->ctx))) return rc;
             if ((rc = bcg_nutrient_update(s->ctx, 0, -1))) return rc;
             if ((rc = bcg_rebuild_neighbours(s->ctx))) return rc;
+            s->field_updates++;
+            s->rebuilds++;
         }
         if (s->hd_update_flag) {
             s->hd_update_flag = false;
@@ -156,6 +166,7 @@ static int sim_step(bcg_sim* s)
         if (s->update_flag || s->first_step) {
             s->update_flag = false;
             if ((rc = bcg_rebuild_neighbours(s->ctx))) return rc;
+            s->rebuilds++;
         }
         if (s->vcycles_per_step > 0 && (rc = bcg_mg_solve(s->ctx, s->vcycles_per_step))) return rc;
     }
@@ -188,9 +199,10 @@ static int sim_step(bcg_sim* s)
 extern "C" int bcg_sim_run(bcg_sim* s, int steps)
 {
     if (!s || steps < 0) return BCG_E_ARG;
+    if (s->failed) return s->failed;
     for (int i = 0; i < steps; i++) {
         int rc = sim_step(s);
-        if (rc) return rc;
+        if (rc) { s->failed = rc; return rc; }
     }
     return BCG_OK;
 }
@@ -201,6 +213,14 @@ extern "C" int bcg_sim_time(bcg_sim* s, double* t, int* n_cells, int64_t* divisi
     if (t) *t = s->t;
     if (n_cells) bcg_num_cells(s->ctx, n_cells);
     if (divisions) *divisions = s->divisions;
+    return BCG_OK;
+}
+
+extern "C" int bcg_sim_counters(bcg_sim* s, int64_t* neighbour_rebuilds, int64_t* field_updates)
+{
+    if (!s) return BCG_E_ARG;
+    if (neighbour_rebuilds) *neighbour_rebuilds = s->rebuilds;
+    if (field_updates) *field_updates = s->field_updates;
     return BCG_OK;
 }
 
@@ -230,6 +250,7 @@ struct bcg_ensemble {
     std::vector<int> nd;
     std::vector<int64_t> calls;
     std::vector<size_t> base;
+    std::vector<char> live;        /* members still stepping in this step */
 };
 
 extern "C" int bcg_ensemble_create(bcg_sim* const* members, int n, bcg_ensemble** out)
@@ -253,35 +274,50 @@ extern "C" int bcg_ensemble_destroy(bcg_ensemble* e)
     return BCG_OK;
 }
 
+/* A member whose step fails is marked failed (its later runs, alone or in
+ * an ensemble, return the error); every other member still completes the
+ * step, so none is left between MoveCell and its division loop. */
 static int ens_step(bcg_ensemble* e)
 {
     const int n = (int)e->m.size();
+    int first_rc = BCG_OK;
+    e->live.assign(n, 1);
+    auto fail = [&](int i, int rc) {
+        e->m[i]->failed = rc;
+        e->live[i] = 0;
+        if (!first_rc) first_rc = rc;
+    };
     int rc;
     for (int i = 0; i < n; i++) {
         bcg_sim* s = e->m[i];
         if (s->update_flag || s->first_step) {
             s->update_flag = false;
-            if ((rc = bcg_rebuild_neighbours(s->ctx))) return rc;
+            if ((rc = bcg_rebuild_neighbours(s->ctx))) { fail(i, rc); continue; }
+            s->rebuilds++;
         }
-        if (s->vcycles_per_step > 0 && (rc = bcg_int_mg_solve_launch(s->ctx, s->vcycles_per_step))) return rc;
+        if (s->vcycles_per_step > 0 && (rc = bcg_int_mg_solve_launch(s->ctx, s->vcycles_per_step))) { fail(i, rc); continue; }
         s->first_step = false;
-        if ((rc = bcg_int_move_grow_launch(s->ctx, s->dt))) return rc;
+        if ((rc = bcg_int_move_grow_launch(s->ctx, s->dt))) fail(i, rc);
     }
     for (int i = 0; i < n; i++) {
+        if (!e->live[i]) continue;
         bcg_sim* s = e->m[i];
-        if ((rc = bcg_int_move_grow_finish(s->ctx, &e->nd[i], &e->calls[i]))) return rc;
+        if ((rc = bcg_int_move_grow_finish(s->ctx, &e->nd[i], &e->calls[i]))) { fail(i, rc); continue; }
         sim_draws(s, e->nd[i], e->calls[i]);
         e->base[i] = s->lineage.size();
         s->lineage.resize(e->base[i] + 2 * (size_t)(e->nd[i] > 0 ? e->nd[i] : 0));
-        if ((rc = bcg_int_divide_launch(s->ctx, s->draws.data(), e->nd[i], s->t))) return rc;
+        if ((rc = bcg_int_divide_launch(s->ctx, s->draws.data(), e->nd[i], s->t))) {
+            s->lineage.resize(e->base[i]);
+            fail(i, rc);
+        }
     }
-    int first_rc = BCG_OK;
     for (int i = 0; i < n; i++) {
+        if (!e->live[i]) continue;
         bcg_sim* s = e->m[i];
         int done = 0;
         rc = bcg_int_divide_finish(s->ctx, &done, e->nd[i] > 0 ? s->lineage.data() + e->base[i] : nullptr);
         rc = sim_advance(s, e->base[i], done, rc);
-        if (rc && !first_rc) first_rc = rc;
+        if (rc) fail(i, rc);
     }
     return first_rc;
 }
@@ -289,6 +325,8 @@ static int ens_step(bcg_ensemble* e)
 extern "C" int bcg_ensemble_run(bcg_ensemble* e, int steps)
 {
     if (!e || steps < 0) return BCG_E_ARG;
+    for (bcg_sim* s : e->m)
+        if (s->failed) return s->failed;
     for (int k = 0; k < steps; k++) {
         int rc = ens_step(e);
         if (rc) return rc;

@@ -2,12 +2,16 @@
 input files (run_sim/inputFile_20mM_{Small,Large}Simulation.txt): the
 "key value" pairs only, in the reference's own key/value format, so that the
 parameter sets travel with the package.  Run where the reference tree is
-mounted:  python baccolonygrowth_b200/data/make_inputs.py [reference_dir]
+mounted:  python baccolonygrowth_b200/data/make_inputs.py <reference_dir>
+(reference_dir = the AgentBasedModel-BacColonyGrowth directory; or set
+BCG_REF_DIR to it).
 """
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/AgentBasedModel-BacColonyGrowth"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BCG_REF_DIR", "")
+if not REF:
+    sys.exit("usage: make_inputs.py <AgentBasedModel-BacColonyGrowth directory> (or set BCG_REF_DIR)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 for src, dst in (("inputFile_20mM_SmallSimulation.txt", "small_input.txt"),

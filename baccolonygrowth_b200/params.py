@@ -69,22 +69,33 @@ def atoi(s):
     return int(m.group(0)) if m else 0
 
 
-def defaults():
+# The two C entries behind defaults() and finalize(): the library's
+# bcg_params_default / bcg_params_finalize unless a caller passes another
+# pair with the same signatures (the benchmark's reference arm passes the
+# oracle's, so that it never loads the CUDA library).
+def _param_entries(entries):
+    if entries is not None:
+        return entries
+    lib = _abi.load()
+    return lib.bcg_params_default, lib.bcg_params_finalize
+
+
+def defaults(entries=None):
     """Reference defaults (Constants.cpp:1-112) from the library."""
     p = _abi.Params()
-    _abi.check(_abi.load().bcg_params_default(ctypes.byref(p)), "bcg_params_default")
+    _abi.check(_param_entries(entries)[0](ctypes.byref(p)), "bcg_params_default")
     return p
 
 
-def finalize(p):
-    _abi.check(_abi.load().bcg_params_finalize(ctypes.byref(p)), "bcg_params_finalize")
+def finalize(p, entries=None):
+    _abi.check(_param_entries(entries)[1](ctypes.byref(p)), "bcg_params_finalize")
     return p
 
 
-def parse_parameters(text, p=None, warn=True):
+def parse_parameters(text, p=None, warn=True, entries=None):
     """Apply "key value" lines to params p (defaults if None)."""
     if p is None:
-        p = defaults()
+        p = defaults(entries)
     for line in re.split(r"[\r\n]", text):
         parts = line.split()
         if not parts:
@@ -140,14 +151,14 @@ def shipped_input_text(which="small"):
         return f.read()
 
 
-def workload_params(name, max_cells=None):
+def workload_params(name, max_cells=None, entries=None):
     """Params of a named workload: the reference's small-simulation physics
     with the workload's grid."""
     cells, aspect, bx, bz, bza, lev = WORKLOADS[name]
-    p = parse_parameters(shipped_input_text("small"))
+    p = parse_parameters(shipped_input_text("small"), entries=entries)
     p.box_x, p.box_y, p.box_z, p.box_z_agar, p.max_levels_mg = bx, 1, bz, bza, lev
     p.max_cells = max_cells if max_cells else int(cells * 1.25) + 1024
-    return finalize(p)
+    return finalize(p, entries)
 
 
 def dome_size(n_cells, aspect, phi=0.45, radius=0.5, mean_len=3.0):

@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--no-output", action="store_true", help="skip the output-step measurement")
+    ap.add_argument("--no-field-update", action="store_true",
+                    help="skip the field update at the reference's cadence (266 solves + 200 sweeps each)")
     ap.add_argument("--smoother-warps", type=int, default=0,
                     help="pin the agar smoother's resident-warp target instead of autotuning it (profiling)")
     return ap.parse_args()
@@ -254,17 +256,38 @@ def output_step_bench(lib, sim, ctx, p, stream, steps=100):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def source_digest(rel):
+    import hashlib
+    with open(os.path.join(ROOT, rel), "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()[:16]
+
+
 def profiled_traffic(summary, workload):
-    """DRAM bytes (read + write) of one launch from the committed ncu
-    summary of the kernel (profiles/<summary>), when it was captured on this
-    workload; else None."""
+    """DRAM bytes (read + write) of one launch from the committed ncu summary
+    of the kernel (profiles/<summary>), and where they come from.  The
+    summary records the digest of the kernel's source file at capture time
+    (a line "- source: <file> sha256[:16] <digest>"); the bytes are used
+    only when it was captured on this workload and the source is unchanged,
+    else (None, reason)."""
     path = os.path.join(ROOT, "profiles", summary)
     try:
         text = open(path).read()
     except OSError:
-        return None
+        return None, "no ncu summary"
     if workload not in summary:
-        return None
+        return None, "no ncu summary of this workload"
+    src = None
+    for line in text.splitlines():
+        if line.startswith("- source: "):
+            f = line.split()
+            src = (f[2], f[-1])
+    if src is None:
+        return None, "ncu summary without a source digest"
+    try:
+        if source_digest(src[0]) != src[1]:
+            return None, "kernel source changed since the ncu capture in profiles/%s" % summary
+    except OSError:
+        return None, "kernel source file missing"
     unit = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
     total = 0.0
     for key in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
@@ -274,8 +297,108 @@ def profiled_traffic(summary, workload):
                 total += float(v) * unit.get(u, float("nan"))
                 break
         else:
-            return None
-    return total
+            return None, "ncu summary without DRAM bytes"
+    return total, "ncu capture of one launch of the same source (profiles/%s), not this run" % summary
+
+
+def sim_rebuilds(lib, sim):
+    r = ctypes.c_int64()
+    f = ctypes.c_int64()
+    lib.bcg_sim_counters(sim, ctypes.byref(r), ctypes.byref(f))
+    return int(r.value)
+
+
+def time_rebuild(lib, ctx, reps=3):
+    """Device time (ms) of one full neighbour rebuild (binning + lists) of
+    the context's colony, the mean of `reps` (the lists do not change)."""
+    from baccolonygrowth_b200 import _abi
+    _abi.check(lib.bcg_rebuild_neighbours(ctx), "rebuild warm-up")
+    _abi.check(lib.bcg_enable_timers(ctx, 1), "timers")
+    for _ in range(reps):
+        _abi.check(lib.bcg_rebuild_neighbours(ctx), "rebuild")
+    ms = ctypes.c_double(); nl = ctypes.c_int64()
+    lib.bcg_get_timer(ctx, _abi.TIMERS["NEIGHBOURS"], ctypes.byref(ms), ctypes.byref(nl))
+    _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
+    return ms.value / reps
+
+
+def field_update_bench(lib, ctx, p, timers, rebuild_ms, n_cells):
+    """The reference's field update (Simulation.cpp:261-294) on the bench
+    colony, each part timed on the device: the density chain
+    (bcg_update_density), UpdateEnvArrayMG_OxygenAcetate at the reference's
+    schedule (bcg_nutrient_update: n solves of 3 V-cycles + 200 colony/wall
+    sweeps each, n = int(3600 UpdateTime 740 / 100)) and the full neighbour
+    rebuild; the height update of every UpdateTime/10 beside it.  The step
+    rate at the reference's cadence puts one update and 10 height updates
+    over the UpdateTime/dt mechanics steps (MoveCell/GrowCell + divisions,
+    no per-step solve) of one period."""
+    from baccolonygrowth_b200 import _abi
+    out = {}
+    try:
+        def timed(fn, tid):
+            _abi.check(lib.bcg_enable_timers(ctx, 1), "timers")
+            fn()
+            ms = ctypes.c_double(); nl = ctypes.c_int64()
+            lib.bcg_get_timer(ctx, _abi.TIMERS[tid], ctypes.byref(ms), ctypes.byref(nl))
+            _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
+            return ms.value, int(nl.value)
+        # capture both [solve + sweeps] graphs before timing
+        _abi.check(lib.bcg_nutrient_update(ctx, 2, -1), "nutrient update warm-up")
+        d_ms, _ = timed(lambda: _abi.check(lib.bcg_update_density(ctx), "density"), "DENSITY")
+        n_ms, n_l = timed(lambda: _abi.check(lib.bcg_nutrient_update(ctx, 0, -1), "nutrient update"), "SWEEPS")
+        h_ms, _ = timed(lambda: _abi.check(lib.bcg_update_height(ctx), "height"), "DENSITY")
+        n_solves = nutrient_solves(p)
+        upd = d_ms + n_ms + rebuild_ms
+        S = steps_per_update(p)
+        mech = timers["MOVE_GROW"] + timers["DIVIDE"]
+        per_step = (S * mech + upd + (S / 10.0) * h_ms) / S
+        out.update(solves_per_update=n_solves, sweeps_per_solve=p.sweeps_per_solve,
+                   vcycles_per_solve=p.mg_vcycles, density_ms=d_ms, nutrient_ms=n_ms, rebuild_ms=rebuild_ms,
+                   height_ms=h_ms, update_ms=upd, nutrient_launches=n_l,
+                   steps_per_update=S, mechanics_ms_per_step=mech,
+                   cell_steps_per_s=n_cells / (per_step / 1e3),
+                   timing="CUDA events on the context's stream, one update")
+    except Exception as e:      # reported, not required
+        out["error"] = str(e)
+    return out
+
+
+def mg_level_points(p):
+    """3 species x (nx+1)(nz+1) per multigrid level (mg_nx/mg_nz of the
+    Multigrid constructor, Multigrid.cpp:5-33)."""
+    A = p.max_levels_mg
+    d0 = 1 << A
+    pts = []
+    for l in range(p.mg_levels):
+        d = 1 << l
+        nx = min(p.box_x * d0 // d // 2, p.box_x)
+        nz = min(p.box_z_agar * d0 // d // 2, p.box_z_agar)
+        pts.append(3 * (nx + 1) * (nz + 1))
+    return pts
+
+
+def mg_solve_bytes(p, vcycles):
+    """Algorithmic DRAM bytes of one Multigrid::solve with `vcycles` V-cycles
+    as the library runs it (FP64): per point and species, the fused
+    3-sweep smoother reads R and E and writes E once (24 B) before and after
+    the coarse correction; the restriction reads E and R (12 B: R is read
+    on the even rows only) and writes 8 B per coarse point; the prolongation
+    reads and writes E (16 B) and reads 8 B per coarse point; the coarsest
+    level's relaxations run in shared memory (E and R in, E out).  Per
+    solve: setup's residual (S in, R out: 16 B) and reset's update (S, E in,
+    S out, E and R zeroed: 40 B) on the composite levels, zeroing (16 B) on
+    the others."""
+    pts = mg_level_points(p)
+    A, L = p.max_levels_mg, len(pts)
+    sweeps = max(1, (p.mg_mu1 + 2) // 3)     # fused launches per smoothing
+    v = 0.0
+    for l in range(L - 1):
+        v += 2 * sweeps * 24.0 * pts[l]
+        v += 12.0 * pts[l] + 8.0 * min(pts[l + 1], pts[l] // 4)
+        v += 16.0 * pts[l] + 8.0 * min(pts[l + 1], pts[l] // 4)
+    v += 24.0 * pts[L - 1]
+    per_solve = sum(56.0 * pts[l] for l in range(A)) + sum(16.0 * pts[l] for l in range(A, L))
+    return vcycles * v + per_solve
 
 
 def colony_sweep_bench(lib, ctx, sweeps=200):
@@ -318,30 +441,36 @@ def measured_peaks():
 # CPU side: the reference's own code (oracle/_ref) or, where it is not built,
 # the C restatement, on a bounded sample of the same workload
 # ---------------------------------------------------------------------------
+def cpu_model(pp, kind, threads):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import checkers
+    if kind == "reference":
+        return checkers.Reference(pp, seed=12345, threads=threads)
+    return checkers.Oracle(pp, seed=12345)
+
+
+def cpu_kind():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import checkers
+    return "reference" if checkers.have_ref() else "port"
+
+
 def cpu_run(p, cells, steps, threads, sample_cells=131072):
     """Time the CPU implementation on a bounded sample of the workload: the
     mechanics on a central x-window of `sample_cells` cells (per-cell cost
     does not depend on the colony size), the agar solve on the full grid.
     Returns per-step time for the whole workload (cells / mechanics rate +
     one 1-V-cycle solve + the neighbour rebuild amortised over 100 steps)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
     import numpy as np
-    import checkers
-    from baccolonygrowth_b200 import _abi, params as _params
-    kind = "reference" if checkers.have_ref() else "port"
+    from baccolonygrowth_b200 import _abi
+    kind = cpu_kind()
     n = len(cells)
     m_cells = min(n, sample_cells)
     order = np.argsort(np.abs(0.5 * (cells["p"][:, 0] + cells["q"][:, 0])), kind="stable")
     sample = np.ascontiguousarray(cells[np.sort(order[:m_cells])])
     ps = p.copy()
     ps.max_cells = int(m_cells * 1.1) + 1024
-
-    def model(pp):
-        if kind == "reference":
-            return checkers.Reference(pp, seed=12345, threads=threads)
-        return checkers.Oracle(pp, seed=12345)
-
-    m = model(ps)
+    m = cpu_model(ps, kind, threads)
     m.load(sample)
     m.set_field(_abi.FIELDS["ENV_GROWTH1"], np.full(p.box_x * p.box_z, 0.9))
     t0 = time.perf_counter()
@@ -357,7 +486,7 @@ def cpu_run(p, cells, steps, threads, sample_cells=131072):
     del m
     pg = p.copy()
     pg.max_cells = 4096
-    g = model(pg)
+    g = cpu_model(pg, kind, threads)
     t0 = time.perf_counter()
     g.mg_solve(1, p.mg_dt)
     t_solve = time.perf_counter() - t0
@@ -369,6 +498,7 @@ def cpu_run(p, cells, steps, threads, sample_cells=131072):
     per_step = n / rate + t_solve
     return dict(kind=kind, threads=threads if kind == "reference" else 1, per_step=per_step,
                 t_mech=t_mech, t_solve=t_solve, t_vcycle=t_v, cell_steps=n / per_step,
+                t_rebuild_full=t_rebuild * n / m_cells, mech_cell_steps=rate,
                 mg_dof_s=mg_dof(p) / t_v,
                 sample="mechanics: %d of the %d cells (central x-window), %d steps + 1 full neighbour rebuild "
                        "(amortised over 100 steps); agar: Multigrid::solve with 1 and 3 V-cycles on the full "
@@ -376,21 +506,94 @@ def cpu_run(p, cells, steps, threads, sample_cells=131072):
                        % (m_cells, n, steps, p.box_x + 1, p.box_z_agar + 1))
 
 
+def cpu_field_update(p, cells, threads, mech=None):
+    """The reference's field update (Simulation.cpp:261-294) on the CPU, on
+    the full colony and grid: the density chain (GetDensity .. GetSurfaceNormal)
+    and one outer iteration of UpdateEnvArrayMG_OxygenAcetate (one
+    Multigrid::solve + 200 colony/wall sweeps) are timed; the update is the
+    density chain + n outer iterations + the full neighbour rebuild (from the
+    mechanics sample, scaled to the colony).  The per-step figure at the
+    reference's cadence adds UpdateTime/dt mechanics steps and the
+    UpdateTime/10 height updates."""
+    import numpy as np
+    kind = cpu_kind()
+    pp = p.copy()
+    pp.max_cells = len(cells) + 1024
+    m = cpu_model(pp, kind, threads)
+    m.load(np.ascontiguousarray(cells))
+    t0 = time.perf_counter()
+    m.update_density()
+    t_density = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    m.update_height()
+    t_height = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    m.nutrient_update(1)
+    t_iter = time.perf_counter() - t0
+    m.close()
+    n_solves = nutrient_solves(p)
+    out = {"kind": kind, "cores": threads if kind == "reference" else 1,
+           "density_ms": t_density * 1e3, "height_ms": t_height * 1e3,
+           "outer_iteration_ms": t_iter * 1e3, "solves_per_update": n_solves,
+           "sample": "density chain + 1 of the %d outer iterations (Multigrid::solve, 3 V-cycles, + %d sweeps) "
+                     "on the full colony and grid, scaled" % (n_solves, p.sweeps_per_solve)}
+    if mech is not None:
+        upd = t_density + n_solves * t_iter + mech["t_rebuild_full"]
+        S = steps_per_update(p)
+        per_step = (S * len(cells) / mech["mech_cell_steps"] + upd + (S / 10.0) * t_height) / S
+        out.update(update_ms=upd * 1e3, cell_steps_per_s=len(cells) / per_step)
+    return out
+
+
+def nutrient_solves(p):
+    """n of UpdateEnvArrayMG_OxygenAcetate: int(3600 UpdateTime 740 / 100)
+    (Multigrid.cpp:995-996)."""
+    return p.solves_per_update if p.solves_per_update > 0 else int(3600 * p.update_time * 740 / p.mg_dt)
+
+
+def steps_per_update(p):
+    return max(1, int(round(p.update_time / p.dt)))
+
+
+def loaded_repo_libraries():
+    """Shared libraries of this repository mapped into this process."""
+    libs = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(ROOT):
+                    libs.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(libs)
+
+
 def reference_arm(args):
+    """The reference's own CPU code on the same workload and metric.  The
+    workload (parameters and colony) is built with the oracle's restatement
+    of bcg_params_default / bcg_synth_colony, so this arm never loads the
+    CUDA library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import checkers
     from baccolonygrowth_b200 import params
     from baccolonygrowth_b200.colony import workload_colony
-    p = params.workload_params(args.workload)
-    cells = workload_colony(args.workload)
+    p = params.workload_params(args.workload, entries=checkers.oracle_param_entries())
+    cells = workload_colony(args.workload, entry=checkers.oracle_synth_entry())
     threads = os.cpu_count() or 1
     steps = max(1, min(args.steps, args.cpu_sample_steps))
     # warm-up sample (page-in), then the timed samples
-    r = None
-    for i in range(max(1, min(args.warmup, 1))):
-        cpu_run(p, cells[:4096], 1, threads)
+    cpu_run(p, cells[:4096], 1, threads)
     r = cpu_run(p, cells, steps, threads)
+    fu = None
+    if not args.no_field_update:
+        try:
+            fu = cpu_field_update(p, cells, threads, mech=r)
+        except Exception as e:      # reported, not required
+            fu = {"error": str(e)}
     v = r["cell_steps"]
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
@@ -398,11 +601,14 @@ def reference_arm(args):
         "ms_per_step": r["per_step"] * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "cells": len(cells), "box": [p.box_x, p.box_y, p.box_z],
-                   "box_z_agar": p.box_z_agar, "agar_levels": p.max_levels_mg, "vcycles_per_step": 1},
+                   "box_z_agar": p.box_z_agar, "agar_levels": p.max_levels_mg, "vcycles_per_step": 1,
+                   "neighbour_rebuild_every": 100},
         "mg_dof_per_s": r["mg_dof_s"],
+        "field_update": fu,
         "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": r["threads"], "kind": r["kind"],
                          "sample": r["sample"]},
         "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "repo_libraries_loaded": loaded_repo_libraries(),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -471,6 +677,7 @@ def b200_arm(args):
         dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
+    rb0 = sim_rebuilds(lib, sim)
     launches0 = int(lib.bcg_kernel_launches(ctx))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -481,7 +688,15 @@ def b200_arm(args):
     torch.cuda.synchronize()
     launches = int(lib.bcg_kernel_launches(ctx)) - launches0
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
+    rebuilds_timed = sim_rebuilds(lib, sim) - rb0
+    ms_raw = e0.elapsed_time(e1)
+    # the full neighbour rebuild runs every UpdateTime/dt steps (100): take
+    # the rebuilds that fell inside the timed steps out and put 1/100 of one
+    # timed rebuild into every step, so that the figure does not depend on
+    # where --steps falls in the rebuild period
+    rebuild_ms = time_rebuild(lib, ctx)
+    every = steps_per_update(p)
+    ms = ms_raw - rebuilds_timed * rebuild_ms + args.steps * rebuild_ms / every
     t_ = ctypes.c_double(); n_ = ctypes.c_int(); d_ = ctypes.c_int64()
     lib.bcg_sim_time(sim, ctypes.byref(t_), ctypes.byref(n_), ctypes.byref(d_))
     n_end = n_.value
@@ -501,6 +716,9 @@ def b200_arm(args):
     n_now = ctypes.c_int()
     lib.bcg_num_cells(ctx, ctypes.byref(n_now))
     colony = colony_sweep_bench(lib, ctx) if world == 1 else None
+    field_update = None
+    if world == 1 and not args.no_field_update:
+        field_update = field_update_bench(lib, ctx, p, timers, rebuild_ms, n_now.value)
     lib.bcg_sim_destroy(sim)
 
     # end to end through the C ABI with host buffers: upload of the colony
@@ -528,6 +746,7 @@ def b200_arm(args):
         _abi.check(lib.bcg_download_cells(ctx2, _abi.ptr(outbuf), len(outbuf), ctypes.byref(got)), "download")
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - w0
+        e2e_s += (e2e_steps / every - sim_rebuilds(lib, sim2)) * rebuild_ms / 1e3
         t2 = ctypes.c_double(); n2 = ctypes.c_int(); d2 = ctypes.c_int64()
         lib.bcg_sim_time(sim2, ctypes.byref(t2), ctypes.byref(n2), ctypes.byref(d2))
         lib.bcg_sim_destroy(sim2)
@@ -600,10 +819,7 @@ def b200_arm(args):
     dof = mg_dof(p)
     mg_ms = timers["MG_SOLVE"]
     mech_ms = timers["MOVE_GROW"]
-    # algorithmic bytes: per finest DOF per V-cycle ~245 B (2*mu1 relaxations
-    # of 24 B, residual/restriction 24 B, prolongation 16 B, x 4/3 for the
-    # coarse levels); per cell-step 280 B of state + 4 B per list entry
-    mg_bytes = 245.0 * dof * args.vcycles
+    mg_bytes = mg_solve_bytes(p, args.vcycles)
     k_mean = float(os.environ.get("BCG_K_MEAN", "0")) or None
     mech_bytes = (280.0 + 4.0 * (k_mean or 2.0)) * cells_mean
     mg_gbs = mg_bytes / (mg_ms / 1e3) / 1e9 if mg_ms > 0 else 0.0
@@ -611,7 +827,11 @@ def b200_arm(args):
     roof_mg = {"kernel": "multigrid solve (Multigrid::solve, %d V-cycle)" % args.vcycles, "bound": "hbm",
                "achieved": mg_gbs, "peak": peak_gbs, "unit": "GB/s", "frac": mg_gbs / peak_gbs,
                "traffic": None, "peak_source": peak_src, "algorithmic_bytes_per_launch": mg_bytes,
-               "launch_ms": mg_ms}
+               "launch_ms": mg_ms,
+               "bytes_model": "per point and species: fused 3-sweep smoothing 24 B before and after, "
+                              "restriction 12 B + 8 B per coarse point written, prolongation 16 B + 8 B per "
+                              "coarse point read, on every level; setup's residual 16 B and reset's update "
+                              "40 B on the composite levels, zeroing 16 B on the others"}
     # the dominant single kernel: the fused 3-sweep smoother on a finest
     # composite level, 24 B per point and species (R and E read, E2
     # written), timed with CUDA events by the autotuner
@@ -620,10 +840,10 @@ def b200_arm(args):
     sm_bytes = 24.0 * lvl0_pts
     if mg_ms >= mech_ms and sm_ms > 0:
         sm_gbs = sm_bytes / (sm_ms / 1e3) / 1e9
+        traffic, traffic_src = profiled_traffic("k_mg_smooth_mixed_1m.md", args.workload)
         roof = {"kernel": "k_mg_smooth<double,3> (finest agar level, 3 fused zebra sweeps)", "bound": "hbm",
                 "achieved": sm_gbs, "peak": peak_gbs, "unit": "GB/s", "frac": sm_gbs / peak_gbs,
-                "traffic": profiled_traffic("k_mg_smooth_mixed_1m.md", args.workload),
-                "traffic_source": "profiles/k_mg_smooth_mixed_1m.md (ncu, one level-0 launch)",
+                "traffic": traffic, "traffic_source": traffic_src,
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": sm_bytes,
                 "launch_ms": sm_ms, "unit_work": "%d points x 3 species, 24 B each" % (lvl0_pts // 3)}
     elif mg_ms >= mech_ms:
@@ -638,6 +858,11 @@ def b200_arm(args):
             r = cpu_run(p, cells, args.cpu_sample_steps, os.cpu_count() or 1)
             cpu = {"value": r["cell_steps"], "unit": "cell-steps/s", "cores": r["threads"], "kind": r["kind"],
                    "sample": r["sample"], "mg_dof_per_s": r["mg_dof_s"]}
+            if field_update is not None:
+                try:
+                    field_update["cpu"] = cpu_field_update(p, cells, os.cpu_count() or 1, mech=r)
+                except Exception as e:      # reported, not required
+                    field_update["cpu"] = {"error": str(e)}
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port", "sample": "failed: %s" % e}
     line = {
@@ -647,7 +872,10 @@ def b200_arm(args):
         "config": {"workload": args.workload, "cells": n0, "cells_end": n_end,
                    "box": [p.box_x, p.box_y, p.box_z], "box_z_agar": p.box_z_agar,
                    "agar_levels": p.max_levels_mg, "mg_levels": p.mg_levels, "mg_dof": dof,
-                   "vcycles_per_step": args.vcycles, "neighbour_rebuild_every": 100,
+                   "vcycles_per_step": args.vcycles, "neighbour_rebuild_every": every,
+                   "neighbour_rebuild": {"ms": rebuild_ms, "in_timed_steps": rebuilds_timed,
+                                         "accounting": "timed steps minus the rebuilds inside them, "
+                                                       "plus 1/%d of one rebuild per step" % every},
                    "autotuned": tuned,
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs larger than L2 (cell records 2x%d MB + fields)" % (n0 * 128 // 2 ** 20)},
@@ -656,6 +884,7 @@ def b200_arm(args):
         "ensemble": ens,
         "output_step": out_step,
         "colony_sweeps": colony,
+        "field_update": field_update,
         "kernel_ms_per_step": timers,
         "divisions": d_.value,
         "roofline": roof,

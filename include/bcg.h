@@ -310,6 +310,13 @@ int bcg_mg_solve_tol(bcg_ctx* ctx, double rel_tol, int precision, int max_iters,
 /* ------------------------------------------------------------------ */
 /* kernel-shape autotuning (no reference counterpart)                    */
 /* ------------------------------------------------------------------ */
+/* Precision of the per-pair contact geometry in MoveCell (no reference
+ * counterpart).  64 (default): the reference's FP64 min_distance.  32: the
+ * closest points and their distance in FP32 on offsets local to cell i
+ * (min_distance's steps unchanged), the contact forces, positions and
+ * force sums in FP64.  Neighbour lists are built in FP64 either way. */
+int bcg_set_pair_precision(bcg_ctx* ctx, int bits);
+
 /* Times the variants of one kernel on the context's current state and
  * keeps the fastest for this context (*choice receives it):
  *   BCG_TUNE_FORCE_GROUP  lanes per cell in MoveCell+GrowCell (1..16);
@@ -318,17 +325,30 @@ int bcg_mg_solve_tol(bcg_ctx* ctx, double rel_tol, int precision, int max_iters,
  *   BCG_TUNE_SMOOTHER     resident-warp target of the fused agar smoother
  *                         (how many row segments a level is cut into);
  *                         changes only the multigrid's correction scratch.
- * The choice also becomes the default of contexts created afterwards.
- * Synchronises the stream; not for use inside a stream capture. */
-/* Precision of the per-pair contact geometry in MoveCell (no reference
- * counterpart).  64 (default): the reference's FP64 min_distance.  32: the
- * closest points and their distance in FP32 on offsets local to cell i
- * (min_distance's steps unchanged), the contact forces, positions and
- * force sums in FP64.  Neighbour lists are built in FP64 either way. */
-int bcg_set_pair_precision(bcg_ctx* ctx, int bits);
-
+ * Every kernel choice belongs to its context: no call changes another
+ * context's kernels.  Synchronises the stream; not for use inside a
+ * stream capture. */
 typedef enum bcg_tune_id { BCG_TUNE_FORCE_GROUP = 1, BCG_TUNE_SMOOTHER = 2 } bcg_tune_id;
 int bcg_autotune(bcg_ctx* ctx, int what, int* choice);
+
+/* Fixed kernel shapes for one context, for profiling and for tests of the
+ * variants (each drops the context's captured graphs):
+ *   bcg_set_force_group    lanes per cell in MoveCell+GrowCell: 1, 2, 4
+ *                          (default), 8 or 16; the results do not depend
+ *                          on it;
+ *   bcg_set_relax_mode     agar smoother form: 0 = one thread per column
+ *                          and half-sweep, 1 = half-sweeps with row
+ *                          segments, 2 = fused sweeps (default); the forms
+ *                          agree to rounding;
+ *   bcg_set_smoother_warps resident-warp target of the fused smoother
+ *                          (0 = default or tuned);
+ *   bcg_smoother_launch_ms device time of one finest-level launch of the
+ *                          fused smoother measured by the last
+ *                          BCG_TUNE_SMOOTHER (0 before). */
+int bcg_set_force_group(bcg_ctx* ctx, int lanes);
+int bcg_set_relax_mode(bcg_ctx* ctx, int mode);
+int bcg_set_smoother_warps(bcg_ctx* ctx, int warps);
+int bcg_smoother_launch_ms(bcg_ctx* ctx, double* ms);
 
 /* ------------------------------------------------------------------ */
 /* steady glucose field and its adjoint (no reference counterpart)       */
@@ -420,9 +440,13 @@ int bcg_mean_stress(bcg_ctx* ctx, double* stress, double* fnet, int64_t* fcw_cal
  *   - A colony of more than BCG_NOALLOC_MAX_CELLS cells returns
  *     BCG_E_UNSUPPORTED; a call whose current device is not the context's
  *     returns BCG_E_ARG.
- *   - The first call on a device looks the array's device address up
- *     (cudaGetSymbolAddress); make that first call before any stream
- *     capture on that device.
+ *   - Every call looks the array's device address up
+ *     (cudaGetSymbolAddress), which allocates nothing.  The array itself
+ *     comes into being when the library's device code is loaded on a
+ *     device, which with lazy loading can be this first call: make the
+ *     first call on a device (or create a context there, which loads the
+ *     code too) before any stream capture on it and before the host's
+ *     allocator reserves that device's memory.
  *   - Every call on a device uses the same array, which keeps the previous
  *     call's contents.  Calls that can overlap on the GPU (other contexts,
  *     other host threads) race on it and must be serialised by the caller. */
@@ -549,7 +573,10 @@ int bcg_sim_destroy(bcg_sim* sim);
  * honouring UpdateFlag / HeightDensityUpdateFlag and OutFlag: an output
  * step runs mean_stress on every cell before MoveCell and skips its
  * rand() draws, as the reference does; with a writer attached it also
- * writes the step's files and the lineage lines. */
+ * writes the step's files and the lineage lines.  A step that fails
+ * returns its status and marks the simulation failed: the colony may be
+ * left between MoveCell and the division loop, so every later run returns
+ * the same status. */
 int bcg_sim_run(bcg_sim* sim, int steps);
 /* Attach (or, with NULL, detach) an output writer; the simulation does not
  * own it.  write_initial also writes the initial block's output
@@ -559,6 +586,10 @@ int bcg_sim_run(bcg_sim* sim, int steps);
 int bcg_sim_set_writer(bcg_sim* sim, bcg_writer* w, int write_initial);
 bcg_ctx* bcg_sim_ctx(bcg_sim* sim);
 int bcg_sim_time(bcg_sim* sim, double* t, int* n_cells, int64_t* divisions);
+/* Work the simulation has run so far: full neighbour rebuilds
+ * (getNeighbours, Simulation.cpp:292, or the benchmark cadence's) and
+ * field updates (the UpdateFlag block, Simulation.cpp:261-294). */
+int bcg_sim_counters(bcg_sim* sim, int64_t* neighbour_rebuilds, int64_t* field_updates);
 /* Lineage pairs recorded so far (parent, daughter), up to capacity pairs. */
 int bcg_sim_lineage(bcg_sim* sim, int* pairs, int capacity, int* n);
 /* Per-step mode used by benchmarks: each step runs the mechanics step and
@@ -572,7 +603,10 @@ int bcg_sim_set_step_mode(bcg_sim* sim, int field_cadence_reference, int vcycles
  * and grids; the ensemble does not own them.  bcg_ensemble_run advances
  * every member by `steps` steps, each exactly as bcg_sim_run would, with
  * every phase queued for all members (one stream each) before any member
- * is waited for.  BCG_E_UNSUPPORTED for a member in the reference cadence. */
+ * is waited for.  BCG_E_UNSUPPORTED for a member in the reference cadence.
+ * A member whose step fails is marked failed (as by bcg_sim_run) and the
+ * run returns the first such status after the other members have finished
+ * the step; a run with a failed member returns its status at once. */
 typedef struct bcg_ensemble bcg_ensemble;
 int bcg_ensemble_create(bcg_sim* const* members, int n, bcg_ensemble** out);
 int bcg_ensemble_run(bcg_ensemble* e, int steps);

@@ -1764,3 +1764,190 @@ long orc_field(orc_state* s, int field, int level, double* buf, long n, int writ
     return -1;
 #undef ACC
 }
+
+/* ------------------------------------------------------------------------
+ * Inputs for the reference arm of the benchmark, so that it builds its
+ * workload without loading the CUDA library: the parameter defaults of
+ * Constants.cpp:1-112, main()'s derived sizes (CellMD3D.cpp:52-54), and the
+ * seeded synthetic colony.  tests/test_oracle.py checks all three against
+ * the library's bcg_params_default, bcg_params_finalize and
+ * bcg_synth_colony byte for byte.
+ * ---------------------------------------------------------------------- */
+int orc_params_default(bcg_params* p)
+{
+    if (!p) return BCG_E_ARG;
+    memset(p, 0, sizeof(*p));
+    /* Constants.cpp:1-112 (maxO2_Agar hard-coded 0.26 at :32; C_rate =
+     * 3.7e-5 * Tortuosity * 5 with Tortuosity 2, :45-49) */
+    p->cell_radius = 0.34; p->l_divide = 5.75; p->k_cc = 100000.0; p->k_wc = 100000.0;
+    p->viscosity = 1.0; p->gamma_t = 10000.0; p->wall_mu = 0.15; p->cell_mu = 0.15;
+    p->density_threshold = 0.6; p->tension = 10.0; p->rc = 3.0;
+    p->t_max = 20.0; p->dt = 0.00001; p->output_time = 100 * 0.00001; p->update_time = 100 * 0.00001;
+    p->box_x = 150; p->box_y = 150; p->box_z = 50; p->box_z_agar = 30; p->max_levels_mg = 1;
+    p->box_length = 2; p->filter_len = 5; p->max_o2_agar = 0.26; p->max_cells = 100000;
+    p->kc_aer = 0.001; p->kc_ana = 0.001; p->kw = 0.001;
+    p->c_rate = 3.7e-5 * 2.0 * 5.0; p->w_rate = p->c_rate; p->carbon_to_waste = 1.0;
+    p->max_growth_rate1 = 1.0; p->max_growth_rate2 = 1.0;
+    p->diff_colony = 1.0; p->diff_agar = 3.0; p->max_carbon = 0.01;
+    p->cross_feeding = 1; p->cdt = 0.1; p->interface_condition = 1;
+    p->refinement_grid_height = 4;
+    p->ko = 1.0; p->ka = 1.0; p->ki = 1.0;
+    p->q_car_aer = 1.0; p->q_car_ana = 1.0; p->q_ace_aer = 1.0; p->q_o2_car = 1.0; p->q_o2_ace = 1.0;
+    p->p_ace_aer = 1.0; p->p_ace_ana = 1.0;
+    p->diff_colony_carbon = 1.0; p->diff_agar_carbon = 1.0; p->diff_colony_o2 = 1.0;
+    p->diff_agar_o2 = 1.0; p->diff_colony_ace = 1.0; p->diff_agar_ace = 1.0;
+    p->max_o2 = 1.0; p->max_gr_car_aer = 1.0; p->max_gr_car_ana = 1.0; p->max_gr_ace_aer = 1.0;
+    p->kw_ph = 1.0; p->ka_ph = 1.0; p->kb_ph = 1.0; p->cb_ph = 1.0; p->c1_ph = 1.0;
+    p->q_car_aer_nt = 1.0; p->q_car_ana_nt = 1.0; p->q_ace_aer_nt = 1.0; p->q_o2_car_nt = 1.0;
+    p->q_o2_ace_nt = 1.0; p->p_ace_ana_nt = 1.0;
+    /* the solve schedule of Multigrid.cpp:995-1017 and Simulation.cpp:157 */
+    p->mg_levels = 8; p->mg_vcycles = 3; p->mg_mu1 = 3; p->mg_mu2 = 100;
+    p->sweeps_per_solve = 200; p->solves_per_update = 0; p->mg_dt = 100.0;
+    return BCG_OK;
+}
+
+int orc_params_finalize(bcg_params* p)
+{
+    if (!p) return BCG_E_ARG;
+    /* BoxLength = L_divide + 2R, maxCellsPerBox (CellMD3D.cpp:52-54) */
+    p->box_length = p->l_divide + 2 * p->cell_radius;
+    double bl = p->box_length;
+    p->max_cells_per_box = (int)ceil(bl * bl * bl / (PI * p->cell_radius * p->cell_radius * p->l_divide * p->density_threshold / 2));
+    if (p->max_neighbours <= 0) p->max_neighbours = 64;
+    if (p->box_x < 8 || p->box_y < 1 || p->box_z < 3 || p->box_z_agar < 2) return BCG_E_ARG;
+    if (p->max_levels_mg < 1 || p->mg_levels < p->max_levels_mg || p->mg_levels > 16) return BCG_E_ARG;
+    if (p->refinement_grid_height < 1 || p->filter_len < 1 || p->max_cells < 1) return BCG_E_ARG;
+    if (p->max_neighbours > 1024) return BCG_E_ARG;
+    return BCG_OK;
+}
+
+/* 64-bit Mersenne twister (Matsumoto and Nishimura's MT19937-64, the
+ * generator std::mt19937_64 names): state of 312 words, seeded by
+ * x[i] = 6364136223846793005 (x[i-1] ^ (x[i-1] >> 62)) + i. */
+typedef struct { uint64_t x[312]; int i; } mt64;
+static void mt64_seed(mt64* g, uint64_t seed)
+{
+    g->x[0] = seed;
+    for (int i = 1; i < 312; i++) g->x[i] = 6364136223846793005ULL * (g->x[i - 1] ^ (g->x[i - 1] >> 62)) + (uint64_t)i;
+    g->i = 312;
+}
+static uint64_t mt64_next(mt64* g)
+{
+    if (g->i >= 312) {
+        for (int k = 0; k < 312; k++) {
+            uint64_t y = (g->x[k] & 0xFFFFFFFF80000000ULL) | (g->x[(k + 1) % 312] & 0x7FFFFFFFULL);
+            uint64_t v = g->x[(k + 156) % 312] ^ (y >> 1);
+            if (y & 1) v ^= 0xB5026F5AA96619E9ULL;
+            g->x[k] = v;
+        }
+        g->i = 0;
+    }
+    uint64_t z = g->x[g->i++];
+    z ^= (z >> 29) & 0x5555555555555555ULL;
+    z ^= (z << 17) & 0x71D67FFFEDA60000ULL;
+    z ^= (z << 37) & 0xFFF7EEE000000000ULL;
+    z ^= z >> 43;
+    return z;
+}
+static double mt64_unit(mt64* g) { return (double)(mt64_next(g) >> 11) * (1.0 / 9007199254740992.0); }
+
+/* squared closest distance of two x-z segments (plain geometry) */
+static double syn_dist2(const double* a, const double* b)
+{
+    double d1x = a[2] - a[0], d1z = a[3] - a[1], d2x = b[2] - b[0], d2z = b[3] - b[1];
+    double rx = a[0] - b[0], rz = a[1] - b[1];
+    double aa = d1x * d1x + d1z * d1z, ee = d2x * d2x + d2z * d2z, ff = d2x * rx + d2z * rz;
+    double cc = d1x * rx + d1z * rz, bb = d1x * d2x + d1z * d2z;
+    double den = aa * ee - bb * bb, s = 0, t;
+    if (den > 1e-300) { s = (bb * ff - cc * ee) / den; s = s < 0 ? 0 : (s > 1 ? 1 : s); }
+    t = (bb * s + ff) / ee;
+    if (t < 0) { t = 0; s = -cc / aa; s = s < 0 ? 0 : (s > 1 ? 1 : s); }
+    else if (t > 1) { t = 1; s = (bb - cc) / aa; s = s < 0 ? 0 : (s > 1 ? 1 : s); }
+    double dx = (a[0] + d1x * s) - (b[0] + d2x * t), dz = (a[1] + d1z * s) - (b[1] + d2z * t);
+    return dx * dx + dz * dz;
+}
+
+/* The seeded colony of the benchmark workloads: random sequential placement
+ * of spherocylinders (length U(len_lo, len_hi), angle U(0, pi), centre
+ * uniform in a half-ellipse dome of width x height on the agar, both poles
+ * at z >= radius, segment distance >= 2 radius to every earlier cell); the
+ * dome widens by 2 % after a bounded run of failed tries.  Records as
+ * AddFirstCells fills them (InputOutput.cpp:319-345) with
+ * Ldiv = Length + (l_divide/2)(1 - spread u).  Same draws, in the same
+ * order, as the library's bcg_synth_colony. */
+int orc_synth_colony(uint64_t seed, int n_target, double width, double height,
+                     double radius, double len_lo, double len_hi,
+                     double l_divide, double div_phase_spread,
+                     bcg_cell* out, int capacity, int* n)
+{
+    if (!out || !n || n_target < 0 || n_target > capacity || width <= 0 || height <= 0 ||
+        radius <= 0 || len_lo <= 0 || len_hi < len_lo)
+        return BCG_E_ARG;
+    mt64* g = (mt64*)malloc(sizeof(mt64));
+    if (!g) return BCG_E_ARG;
+    mt64_seed(g, seed);
+    const double cs = len_hi + 2 * radius;
+    double W = width, H = height;
+    double gx0 = -W, gz0 = -cs;
+    int gnx = (int)ceil(2 * W / cs) + 3, gnz = (int)ceil((2 * H + 2 * cs) / cs) + 3;
+    int* head = (int*)malloc(sizeof(int) * (size_t)gnx * gnz);
+    int* next = (int*)malloc(sizeof(int) * (size_t)(n_target > 0 ? n_target : 1));
+    double* seg = (double*)malloc(sizeof(double) * 4 * (size_t)(n_target > 0 ? n_target : 1));
+    double* len = (double*)malloc(sizeof(double) * (size_t)(n_target > 0 ? n_target : 1));
+    int rc = BCG_OK;
+    if (!head || !next || !seg || !len) { rc = BCG_E_ARG; goto done; }
+    for (long q = 0; q < (long)gnx * gnz; q++) head[q] = -1;
+    const double min2 = (2 * radius) * (2 * radius);
+    long long fails = 0;
+    int cnt = 0;
+    while (cnt < n_target) {
+        double L = len_lo + (len_hi - len_lo) * mt64_unit(g);
+        double th = 3.141592653589793 * mt64_unit(g);
+        double cx = (mt64_unit(g) - 0.5) * W;
+        double cz = mt64_unit(g) * H;
+        double e = 2 * cx / W;
+        int ok = (e * e < 1.0) && (cz <= H * sqrt(1 - e * e));
+        double sg[4];
+        sg[0] = cx + 0.5 * L * cos(th); sg[1] = cz + 0.5 * L * sin(th);
+        sg[2] = cx - 0.5 * L * cos(th); sg[3] = cz - 0.5 * L * sin(th);
+        if (ok && (sg[1] < radius || sg[3] < radius)) ok = 0;
+        int ix = (int)floor((cx - gx0) / cs), iz = (int)floor((cz - gz0) / cs);
+        if (ok && !(ix >= 0 && iz >= 0 && ix < gnx && iz < gnz)) ok = 0;
+        for (int dx = -1; dx <= 1 && ok; dx++)
+            for (int dz = -1; dz <= 1 && ok; dz++) {
+                int jx = ix + dx, jz = iz + dz;
+                if (jx < 0 || jz < 0 || jx >= gnx || jz >= gnz) continue;
+                for (int id = head[(long)jx * gnz + jz]; id >= 0; id = next[id])
+                    if (syn_dist2(sg, seg + 4 * (size_t)id) < min2) { ok = 0; break; }
+            }
+        if (!ok) {
+            if (++fails > 200000LL + 50LL * (long long)cnt) {
+                W *= 1.02; H *= 1.02; fails = 0;
+                if (2 * W / cs + 3 > gnx || (2 * H + 2 * cs) / cs + 3 > gnz) { rc = BCG_E_ARG; goto done; }
+            }
+            continue;
+        }
+        fails = 0;
+        memcpy(seg + 4 * (size_t)cnt, sg, sizeof(sg));
+        len[cnt] = L;
+        next[cnt] = head[(long)ix * gnz + iz];
+        head[(long)ix * gnz + iz] = cnt;
+        cnt++;
+    }
+    for (int i = 0; i < n_target; i++) {
+        bcg_cell* c = &out[i];
+        memset(c, 0, sizeof(*c));
+        c->p.x = seg[4 * i]; c->p.z = seg[4 * i + 1];
+        c->q.x = seg[4 * i + 2]; c->q.z = seg[4 * i + 3];
+        c->length = len[i];
+        c->radius = radius;
+        double u = mt64_unit(g);
+        c->ldiv = len[i] + (l_divide / 2) * (1.0 - div_phase_spread * u);
+        c->type = 1;
+        c->ancestor = i + 1;
+    }
+    *n = n_target;
+done:
+    free(g); free(head); free(next); free(seg); free(len);
+    return rc;
+}

@@ -42,6 +42,13 @@ int  orc_loop_step(orc_state* s, int* lineage);
 long long orc_mean_stress(orc_state* s, double* stress, double* fnet);
 double orc_time(orc_state* s);
 
+/* inputs of the benchmark's reference arm (no CUDA library loaded there) */
+int orc_params_default(bcg_params* p);
+int orc_params_finalize(bcg_params* p);
+int orc_synth_colony(uint64_t seed, int n_target, double width, double height,
+                     double radius, double len_lo, double len_hi, double l_divide,
+                     double div_phase_spread, bcg_cell* out, int capacity, int* n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,8 +66,25 @@ def oracle_lib():
         _proto(lib, "orc_loop_step", ctypes.c_int, [_VP, _PI])
         _proto(lib, "orc_time", ctypes.c_double, [_VP])
         _proto(lib, "orc_mean_stress", ctypes.c_longlong, [_VP, _PD, _PD])
+        _proto(lib, "orc_params_default", ctypes.c_int, [_PP])
+        _proto(lib, "orc_params_finalize", ctypes.c_int, [_PP])
+        _proto(lib, "orc_synth_colony", ctypes.c_int,
+               [ctypes.c_uint64, ctypes.c_int] + [ctypes.c_double] * 7 + [_VP, ctypes.c_int, _PI])
         _oracle = lib
     return _oracle
+
+
+def oracle_param_entries():
+    """The oracle's restatement of bcg_params_default / bcg_params_finalize
+    (for params.workload_params(..., entries=...))."""
+    lib = oracle_lib()
+    return lib.orc_params_default, lib.orc_params_finalize
+
+
+def oracle_synth_entry():
+    """The oracle's restatement of bcg_synth_colony (for
+    colony.workload_colony(..., entry=...))."""
+    return oracle_lib().orc_synth_colony
 
 
 def have_ref():

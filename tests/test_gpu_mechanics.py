@@ -135,14 +135,11 @@ def test_force_group_variants(gpu, group):
     lib = _abi.load()
     p, orc, col, rng = setup_pair(n=2048)
     col.rebuild_neighbours()
-    try:
-        assert lib.bcg_set_force_group(group) == 0
-        _, calls_o, lin_o = orc.step(p.dt, 0.0)
-        lin = col.step(p.dt, 0.0, rng)
-        assert np.array_equal(lin, lin_o)
-        assert_cells_close(orc.cells(), col.cells())
-    finally:
-        lib.bcg_set_force_group(4)
+    assert lib.bcg_set_force_group(col.h, group) == 0
+    _, calls_o, lin_o = orc.step(p.dt, 0.0)
+    lin = col.step(p.dt, 0.0, rng)
+    assert np.array_equal(lin, lin_o)
+    assert_cells_close(orc.cells(), col.cells())
 
 
 def test_out_of_grid_is_reported(gpu):

@@ -169,3 +169,29 @@ def test_restart_roundtrip(tmp_path):
     raw = open(path.decode(), "rb").read()
     assert len(raw) == 16 + 208 * 300
     assert np.frombuffer(raw[:16], dtype=np.float64).tolist() == [9.001, 1e-4]
+
+
+def test_oracle_inputs_equal_library_inputs():
+    """The benchmark's reference arm builds its workload with the oracle's
+    restatement of the parameter defaults and of the synthetic colony (so
+    that it never loads the CUDA library); both must equal the library's
+    byte for byte (host code, no GPU needed)."""
+    entries = ck.oracle_param_entries()
+    for name in params.WORKLOADS:
+        a = params.workload_params(name)
+        b = params.workload_params(name, entries=entries)
+        assert bytes(a) == bytes(b), name
+    for name, n in (("small_4k", 4096), ("scale_262k", 20000), ("mixed_1m", 30000)):
+        a = workload_colony(name, n=n)
+        b = workload_colony(name, n=n, entry=ck.oracle_synth_entry())
+        assert a.tobytes() == b.tobytes(), name
+    # a denser dome, and an over-packed one that both reject
+    from baccolonygrowth_b200.colony import synth_colony
+    w, h = params.dome_size(2000, 0.1, 0.6)
+    a = synth_colony(2000, w, h, seed=99, div_phase_spread=0.5)
+    b = synth_colony(2000, w, h, seed=99, div_phase_spread=0.5, entry=ck.oracle_synth_entry())
+    assert len(a) == 2000 and a.tobytes() == b.tobytes()
+    w, h = params.dome_size(2000, 0.1, 0.8)
+    for entry in (None, ck.oracle_synth_entry()):
+        with pytest.raises(_abi.BcgError):
+            synth_colony(2000, w, h, seed=99, entry=entry)
