@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbcg.so")
 
-CU_SOURCES = ["ctx.cu", "mech.cu", "fields.cu", "mg.cu", "nutrients.cu", "steady.cu", "output.cu"]
+CU_SOURCES = ["ctx.cu", "mech.cu", "fields.cu", "mg.cu", "mg_smooth.cu", "nutrients.cu", "steady.cu", "output.cu"]
 CPP_SOURCES = ["host.cpp", "sim.cpp", "writer.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

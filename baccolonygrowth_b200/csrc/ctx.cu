@@ -54,6 +54,13 @@ FieldPtrs field_ptrs(const bcg_ctx* c)
 
 int ctx_check_status(bcg_ctx* c)
 {
+    if (c->pending_error) {
+        /* a launch that could not be set up (the work after it was queued) */
+        const int rc = c->pending_error;
+        c->pending_error = BCG_OK;
+        cudaStreamSynchronize(c->stream);
+        return rc;
+    }
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { g_last_cuda = e; return BCG_E_CUDA; }
     DevStatus st;
@@ -150,7 +157,7 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
     bcg_ctx* c = (bcg_ctx*)calloc(1, sizeof(bcg_ctx));
     if (!c) return BCG_E_ARG;
     c->P = *p;
-    c->relax_mode = 2;
+    c->relax_mode = 3;
     cudaGetDevice(&c->device);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { free(c); return BCG_E_CUDA; }
     for (int t = 0; t < BCG_T_COUNT; t++) { cudaEventCreate(&c->ev[t][0]); cudaEventCreate(&c->ev[t][1]); }

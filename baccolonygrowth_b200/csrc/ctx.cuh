@@ -109,7 +109,7 @@ struct bcg_ctx {
      * caller (0 = default); no kernel choice is process-wide */
     int force_group;
     int smooth_warps;
-    int relax_mode;        /* agar smoother form, bcg_set_relax_mode (2 by default) */
+    int relax_mode;        /* agar smoother form, bcg_set_relax_mode (3 by default) */
     size_t cluster_smem[2];/* coarsest-level cluster kernel: shared-memory size checked */
     int cluster_ok[2];     /* ... and whether its clusters fit (FP64, FP32) */
     /* multigrid Err (all levels) and Res (levels > 0) are zero, as the last
@@ -118,6 +118,7 @@ struct bcg_ctx {
     /* level 0's Res of the last reset() not computed yet (done on demand) */
     int mg_res0_stale;
     int pair_f32;          /* contact geometry in FP32 local to cell i (bcg_set_pair_precision) */
+    int pending_error;     /* host-side set-up failure of a queued launch, returned by the next status check */
     double smooth_tune_ms; /* device time of one level-0 fused smoother launch at the tuned shape */
 };
 

@@ -38,34 +38,6 @@ __device__ __forceinline__ P at_ref(const P* a, const LV& L, int i, int k)
     return AT(a, L, i2, k2);
 }
 
-/* The relaxation update of relaxationAgarElementwise (Multigrid.cpp:160-249)
- *   E = (R h^2/(dt D) + sum of weighted neighbours) / (h^2/(dt D) + 2)
- * with cf = h^2/(dt D) and 1/(cf + 2) computed once per level and species
- * (the reference divides per point; the results differ by rounding). */
-template <class T> struct RelaxK { T cf, inv; };
-template <class T>
-__device__ __forceinline__ RelaxK<T> relax_k(const MgConst& m, int l, int sp)
-{
-    const double cf = m.bl2 * (double)(1 << (2 * l)) / m.dt / SP(m.D);
-    RelaxK<T> k; k.cf = (T)cf; k.inv = (T)(1.0 / (cf + 2.0));
-    return k;
-}
-/* interior: neighbours below, above, left, right with weight 1/2 */
-template <class T> __device__ __forceinline__ T rx_in(T r, T b, T u, T xm, T xp, const RelaxK<T>& K)
-{ return fma(r, K.cf, T(0.5) * ((b + u) + (xm + xp))) * K.inv; }
-/* bottom row (k = 0): above weight 1, sides 1/2 */
-template <class T> __device__ __forceinline__ T rx_k0(T r, T u, T xm, T xp, const RelaxK<T>& K)
-{ return fma(r, K.cf, u + T(0.5) * (xm + xp)) * K.inv; }
-/* top row (k = nz): below weight 1, sides 1/2 */
-template <class T> __device__ __forceinline__ T rx_top(T r, T b, T xm, T xp, const RelaxK<T>& K)
-{ return fma(r, K.cf, b + T(0.5) * (xm + xp)) * K.inv; }
-/* side column (i = 0 or nx), interior row: inner neighbour weight 1 */
-template <class T> __device__ __forceinline__ T rx_side(T r, T b, T u, T s1, const RelaxK<T>& K)
-{ return fma(r, K.cf, T(0.5) * (b + u) + s1) * K.inv; }
-/* corners: inner neighbour and the one vertical neighbour, weight 1 each */
-template <class T> __device__ __forceinline__ T rx_corner(T r, T s1, T v, const RelaxK<T>& K)
-{ return fma(r, K.cf, s1 + v) * K.inv; }
-
 MgConst mg_const(const bcg_ctx* c, double dt)
 {
     MgConst m;
@@ -611,70 +583,9 @@ __global__ void __launch_bounds__(768) k_mg_coarse_cluster(MgConst m, MgLvlT<T> 
 /* Fused zebra smoother: S full sweeps (even columns, then odd columns, each */
 /* bottom to top) in one pass over the rows, out of place (E -> E2).        */
 /* ------------------------------------------------------------------------ */
-/* The relaxation of relax_point with the stencil values passed in:
- * below = new value at (i, k-1), up = value at (i, k+1) before this sweep,
- * xm/xp = values at (i-1, k)/(i+1, k) as the sweep order sees them, old =
- * the point's value before this sweep (kept where the point is not relaxed).
- * Same operations as relax_point. */
-template <class T>
-__device__ __forceinline__ T relax_val(const MgConst& m, const RelaxK<T>& K, int nx, int nz, int l, int sp, int i, int k,
-                                       T r, T below, T up, T xm, T xp, T old, const double* __restrict__ inside0)
-{
-    const bool oxy = (sp == 1);
-    const bool top_levels = l >= m.A - 1;
-    const bool side = (i == 0 || i == nx);
-    const T s1 = (i == 0) ? xp : xm;
-    if (k == 0) {
-        int d = 1 << l;
-        int i0 = (i - nx / 2) * d + m.box_x / 2;
-        i0 = i0 < 0 ? 0 : (i0 > m.box_x - 1 ? m.box_x - 1 : i0);
-        if (inside0[(size_t)i0 * m.box_z] > 0) return r;
-        if (side) {
-            if (!top_levels) return old;
-            if (oxy) return r;
-            return rx_corner(r, s1, up, K);
-        }
-        if (oxy) return r;
-        return rx_k0(r, up, xm, xp, K);
-    }
-    if (k == nz) {
-        if (!top_levels) return old;
-        if (side) {
-            if (oxy) return r;
-            return rx_corner(r, s1, below, K);
-        }
-        return rx_top(r, below, xm, xp, K);
-    }
-    if (side) {
-        if (!top_levels) return old;
-        if (oxy) return r;
-        return rx_side(r, below, up, s1, K);
-    }
-    return rx_in(r, below, up, xm, xp, K);
-}
-
 template <class T> struct Pair2;
 template <> struct Pair2<double> { typedef double2 type; };
 template <> struct Pair2<float> { typedef float2 type; };
-
-/* Interior rows (0 < k < nz) need only the column's kind, fixed per lane:
- * 0 interior column, 1 left side (i = 0), 2 right side (i = nx), 3 side
- * held at R (oxygen on the top levels), 4 side not relaxed (keeps old). */
-__device__ __forceinline__ int col_kind(int i, int nx, bool oxy, bool top_levels)
-{
-    if (i != 0 && i != nx) return 0;
-    if (!top_levels) return 4;
-    if (oxy) return 3;
-    return i == 0 ? 1 : 2;
-}
-template <class T>
-__device__ __forceinline__ T rx_row(int kind, T r, T below, T up, T xm, T xp, T old, const RelaxK<T>& K)
-{
-    if (kind == 0) return rx_in(r, below, up, xm, xp, K);
-    if (kind == 1) return rx_side(r, below, up, xp, K);
-    if (kind == 2) return rx_side(r, below, up, xm, K);
-    return kind == 3 ? r : old;
-}
 
 /* Each warp owns a strip of column pairs (lane t: columns c0+2t, c0+2t+1)
  * and one segment of rows.  The S sweeps are 2S half-sweeps (even columns,
@@ -1231,11 +1142,12 @@ static inline dim3 grid_rows(int ncols, int nrows, int threads)
 { return dim3((unsigned)((ncols + threads - 1) / threads), (unsigned)nrows, 3); }
 
 /* The context's smoother form: 0 = one thread per column and half-sweep,
- * 1 = segmented half-sweeps, 2 = fused sweeps (k_mg_smooth) on levels
- * taller than 96 rows (the default, set by bcg_create) */
+ * 1 = segmented half-sweeps, 2 = fused sweeps with per-lane row staging
+ * (k_mg_smooth), 3 = fused sweeps with TMA-staged rows (k_mg_smooth_tma,
+ * the default, set by bcg_create); 2 and 3 on levels of 3 rows or more */
 extern "C" int bcg_set_relax_mode(bcg_ctx* c, int mode)
 {
-    if (!c || mode < 0 || mode > 2) return BCG_E_ARG;
+    if (!c || mode < 0 || mode > 3) return BCG_E_ARG;
     if (mode != c->relax_mode) nutrient_graphs_drop(c);
     c->relax_mode = mode;
     return BCG_OK;
@@ -1268,7 +1180,8 @@ static void relax_level(bcg_ctx* c, const MgConst& m, int l)
     c->launches += 2;
 }
 
-#define SMOOTH_WARPS_DEFAULT 1400   /* resident-warp target of the fused smoother before tuning */
+#define SMOOTH_WARPS_DEFAULT 1400    /* resident-warp target of k_mg_smooth before tuning */
+#define SMOOTH_TMA_WARPS_DEFAULT 888 /* warps of k_mg_smooth_tma before tuning: 6 a streaming multiprocessor */
 
 template <class T> static void swap_err(bcg_ctx* c, int l);
 template <> void swap_err<double>(bcg_ctx* c, int l)
@@ -1313,8 +1226,26 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
     const int rows = c->mg[l].nz + 1;
     /* levels of 0-1 interior rows read across columns through the flat
      * index (at_ref); they keep the in-place kernels */
-    if (c->relax_mode != 2 || rows < 3) {
+    if (c->relax_mode < 2 || rows < 3) {
         for (int j = 0; j < sweeps; j++) relax_level<T>(c, m, l);
+        return;
+    }
+    if (c->relax_mode == 3) {
+        const int warm = warm_rows(m, l);
+        const int target = c->smooth_warps > 0 ? c->smooth_warps : SMOOTH_TMA_WARPS_DEFAULT;
+        while (sweeps > 0) {
+            const int S = sweeps >= 3 ? 3 : sweeps;
+            MgLvlT<T> L = lvl<T>(c, l);
+            /* segments no shorter than the warm-up (16 rows at least) */
+            const int per_seg = mg_smooth_tma_warps_per_segment(L.nx);
+            const int min_len = warm > 16 ? warm : 16;
+            const int max_seg = rows / min_len > 1 ? rows / min_len : 1;
+            const int t = target < max_seg * per_seg ? target : max_seg * per_seg;
+            const int rc = mg_smooth_tma(c, m, L, l, S, t, warm);
+            if (rc) { c->pending_error = rc; return; }
+            swap_err<T>(c, l);
+            sweeps -= S;
+        }
         return;
     }
     while (sweeps > 0) {
@@ -1382,21 +1313,31 @@ int mg_kernel_attributes()
 }
 
 /* bcg_autotune(BCG_TUNE_SMOOTHER): time the fused smoother on the finest
- * level for several resident-warp targets (two launches each, so the
- * correction buffers end where they started) and keep the fastest */
+ * level for several warp targets (two launches each, so the correction
+ * buffers end where they started) and keep the fastest.  TMA form: 1 to
+ * 16 row segments; per-lane staging form: its resident-warp targets. */
 int mg_tune_smoother(bcg_ctx* c, int* choice)
 {
     const int rows = c->mg[0].nz + 1;
-    if (c->relax_mode != 2 || rows <= 96) { if (choice) *choice = 0; return BCG_OK; }
+    if (c->relax_mode < 2 || rows <= 96) { if (choice) *choice = 0; return BCG_OK; }
     MgConst m = mg_const(c, c->P.mg_dt);
-    const int targets[6] = {700, 1400, 2800, 5600, 8400, 11200};
+    int targets[10];
+    int nt = 0;
+    if (c->relax_mode == 3) {
+        const int per_seg = mg_smooth_tma_warps_per_segment(c->mg[0].nx);
+        const int segs[10] = {1, 2, 3, 4, 5, 6, 7, 8, 12, 16};
+        for (int i = 0; i < 10; i++) targets[nt++] = per_seg * segs[i];
+    } else {
+        const int t6[6] = {700, 1400, 2800, 5600, 8400, 11200};
+        for (int i = 0; i < 6; i++) targets[nt++] = t6[i];
+    }
     const int saved = c->smooth_warps;
     cudaEvent_t a, b;
     BCG_CUDA_TRY(cudaEventCreate(&a));
     BCG_CUDA_TRY(cudaEventCreate(&b));
     float best = 3.4e38f;
-    int best_t = saved > 0 ? saved : SMOOTH_WARPS_DEFAULT;
-    for (int ti = 0; ti < 6; ti++) {
+    int best_t = saved > 0 ? saved : (c->relax_mode == 3 ? SMOOTH_TMA_WARPS_DEFAULT : SMOOTH_WARPS_DEFAULT);
+    for (int ti = 0; ti < nt; ti++) {
         c->smooth_warps = targets[ti];
         smooth_level<double>(c, m, 0, 3);                  /* warm-up */
         smooth_level<double>(c, m, 0, 3);
@@ -1404,7 +1345,11 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
         smooth_level<double>(c, m, 0, 3);
         smooth_level<double>(c, m, 0, 3);
         cudaEventRecord(b, c->stream);
-        if (cudaEventSynchronize(b) != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); c->smooth_warps = saved; return BCG_E_CUDA; }
+        if (cudaEventSynchronize(b) != cudaSuccess || c->pending_error) {
+            cudaEventDestroy(a); cudaEventDestroy(b); c->smooth_warps = saved;
+            const int rc = ctx_check_status(c);
+            return rc ? rc : BCG_E_CUDA;
+        }
         float ms = 0;
         cudaEventElapsedTime(&ms, a, b);
         if (ms < best) { best = ms; best_t = targets[ti]; c->smooth_tune_ms = ms / 2.0; }
@@ -1657,6 +1602,7 @@ int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf)
     for (int v = 0; v < vcycles; v++) mg_vcycle(c, m, c->P.mg_mu1, c->P.mg_mu2);
     mg_reset(c, m);
     mg_copy_from(c, m, wall_buf);
+    if (c->pending_error) { const int rc = c->pending_error; c->pending_error = BCG_OK; return rc; }
     return cudaGetLastError() == cudaSuccess ? BCG_OK : BCG_E_CUDA;
 }
 

