@@ -3,10 +3,11 @@
  * update driver (AgentBasedModel-BacColonyGrowth/Multigrid.cpp:984-1125,
  * Nutrients.cpp:200-659, 806-855).
  *
- * One sweep = the colony kernel over the bounding box and the wall kernel
- * over (level, x); on even sweep counts the wall goes first and reads the
- * colony row z = 0 left in the current buffer, on odd counts it goes last
- * and reads the row this sweep wrote (the reference's 1-thread order).
+ * One sweep = one launch of k_sweep over the colony grid (the colony
+ * points of the bounding box and the wall rows of every level); on even
+ * sweep counts the wall reads the colony row z = 0 left in the current
+ * buffer, on odd counts the row this sweep wrote (the reference's 1-thread
+ * order).
  * Buffers swap after every sweep.  The acetate buffer solve, whose results
  * (pH, Hydrox, Acetic, Buffer) feed nothing else, runs only in the last two
  * sweeps of a call: those are the values that survive in each buffer.  The
@@ -113,9 +114,9 @@ struct EnvX { double *gca, *gcn, *gaa, *qcm, *qam, *pam, *qom; };
  * for x in [minx, maxx], z in [0, maxz] where DensityShiftP > DBL_EPSILON
  * (Multigrid.cpp:1037-1047).
  *
- * Block (32, COLONY_COLS): a warp runs 32 consecutive z of one column (the
- * contiguous direction), blockIdx.x the z chunk, blockIdx.y the column
- * group.  DIAG adds the acetate buffer solve and the Environment-only
+ * One point (x, z); the sweep kernel below runs a block of 32 z (the
+ * contiguous direction, one warp) x COLONY_COLS columns.  DIAG adds the
+ * acetate buffer solve and the Environment-only
  * members; the other sweeps run a variant without them, which needs fewer
  * registers.  The second differences multiply by 1/BoxLength^2 and the
  * maintenance caps min(Cgr/g1s, 1) .. by 1/g1s .., reciprocals taken once on
@@ -123,13 +124,12 @@ struct EnvX { double *gca, *gcn, *gaa, *qcm, *qam, *pam, *qom; };
  * quotients by rounding only (one unit in the last place per term). */
 #define COLONY_COLS 8
 template <bool DIAG>
-__global__ void __launch_bounds__(32 * COLONY_COLS) k_colony(NutConst n, const int* __restrict__ bbox, EnvP cur,
-                                                             EnvP prev, WallP pw0, const double* __restrict__ inside,
-                                                             const double* __restrict__ ds, EnvX ex, DevStatus* st)
+__device__ __forceinline__ void colony_point(const NutConst& n, int x, int z, const int* __restrict__ bbox,
+                                             const EnvP& cur, const EnvP& prev, const WallP& pw0,
+                                             const double* __restrict__ inside, const double* __restrict__ ds,
+                                             const EnvX& ex, DevStatus* st)
 {
     const int Z = n.Z;
-    const int z = blockIdx.x * 32 + threadIdx.x;
-    const int x = blockIdx.y * COLONY_COLS + threadIdx.y;
     if (z >= Z || x >= n.X) return;
     const size_t id = (size_t)x * Z + z;
     int minx = bbox[0], maxx = bbox[1], maxz = bbox[2];
@@ -251,12 +251,10 @@ struct AgarRow { const double *C[BCG_MAX_AGAR_LEVELS], *O[BCG_MAX_AGAR_LEVELS], 
  * BoxX/4-1 < x < BoxX*3/4 the reference reads uninitialised second
  * differences; here they are 0 (those points are read by no other point
  * before the next solve overwrites them). */
-__global__ void k_wall(NutConst n, EnvP curenv, AgarRow ag, WallAll cw, WallAll pw, const double* __restrict__ inside)
+__device__ __forceinline__ void wall_point(const NutConst& n, int level, int x, const EnvP& curenv, const AgarRow& ag,
+                                           const WallAll& cw, const WallAll& pw, const double* __restrict__ inside)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int X = n.X;
-    if (t >= X * n.A) return;
-    int level = t / X, x = t % X;
     if (level == 0 && inside[(size_t)x * n.Z] > 0.5) {
         size_t i0 = (size_t)x * n.Z;
         double gC = ag.C[0][x], gO = ag.O[0][x], gA = ag.A[0][x], gW = 0.0;
@@ -332,11 +330,39 @@ static AgarRow agar_rows(bcg_ctx* c)
     return a;
 }
 
-static void colony(dim3 grid, dim3 block, bcg_ctx* c, const NutConst& n, EnvP cur, EnvP prev, WallP pw0, int diag,
-                   EnvX ex)
+/* One sweep of Multigrid.cpp:1017-1095 in one launch: the colony points
+ * (x, z) of the grid and the wall rows (level, x).  The only dependence
+ * between the two within a sweep is the level-0 wall of a colony column
+ * reading the column's z = 0 point of the current buffer: before this
+ * sweep writes it on even sweep counts (the reference's wall loop runs
+ * first), after on odd counts (it runs last).  The thread of (x, 0) does
+ * both in that order; threads (x, z) with 1 <= z < A of the first z
+ * block take the wall of level z.  Each wall point reads only the
+ * previous wall buffer, the agar rows and that one colony value, and no
+ * colony point reads the current wall buffer, so nothing else orders
+ * them. */
+template <bool DIAG, bool WALL_FIRST>
+__global__ void __launch_bounds__(32 * COLONY_COLS) k_sweep(NutConst n, const int* __restrict__ bbox, EnvP cur,
+                                                            EnvP prev, WallP pw0, const double* __restrict__ inside,
+                                                            const double* __restrict__ ds, EnvX ex, AgarRow ag,
+                                                            WallAll cw, WallAll pw, DevStatus* st)
 {
-    if (diag) k_colony<true><<<grid, block, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, ex, c->status);
-    else k_colony<false><<<grid, block, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, ex, c->status);
+    const int z = blockIdx.x * 32 + threadIdx.x;
+    const int x = blockIdx.y * COLONY_COLS + threadIdx.y;
+    if (x >= n.X) return;
+    const bool wall = z < n.A;
+    if (wall && (WALL_FIRST || z > 0)) wall_point(n, z, x, cur, ag, cw, pw, inside);
+    colony_point<DIAG>(n, x, z, bbox, cur, prev, pw0, inside, ds, ex, st);
+    if (!WALL_FIRST && z == 0) wall_point(n, 0, x, cur, ag, cw, pw, inside);
+}
+
+static void sweep_launch(dim3 grid, dim3 block, bcg_ctx* c, const NutConst& n, EnvP cur, EnvP prev, WallP pw0,
+                         int diag, EnvX ex, const AgarRow& ag, const WallAll& cw, const WallAll& pw, bool wall_first)
+{
+#define SWEEP(D, W) k_sweep<D, W><<<grid, block, 0, c->stream>>>(n, c->bbox, cur, prev, pw0, c->inside, c->ds, ex, ag, cw, pw, c->status)
+    if (diag) { if (wall_first) SWEEP(true, true); else SWEEP(true, false); }
+    else { if (wall_first) SWEEP(false, true); else SWEEP(false, false); }
+#undef SWEEP
 }
 
 /* `nsweeps` sweeps with the local buffer indices (ce = current colony
@@ -348,8 +374,8 @@ static void run_sweeps(bcg_ctx* c, int nsweeps, int& ce, int& cwb, int& count, i
     NutConst n = nut_const(c);
     const int X = c->P.box_x, Z = c->P.box_z;
     AgarRow ag = agar_rows(c);
+    /* at least one z block: its first A lanes carry the wall rows */
     const dim3 gcol((unsigned)((Z + 31) / 32), (unsigned)((X + COLONY_COLS - 1) / COLONY_COLS)), bcol(32, COLONY_COLS);
-    unsigned gwal = (unsigned)((X * n.A + 255) / 256);
     for (int j = 0; j < nsweeps; j++) {
         EnvP cur = envp(c, ce), prev = envp(c, ce ^ 1);
         WallAll cw = wall_all(c, cwb), pw = wall_all(c, cwb ^ 1);
@@ -360,14 +386,8 @@ static void run_sweeps(bcg_ctx* c, int nsweeps, int& ce, int& cwb, int& count, i
             double* const* x = c->env[0].extra;
             ex = EnvX{x[0], x[1], x[2], x[3], x[4], x[5], x[6]};
         }
-        if (count % 2 == 0) {
-            k_wall<<<gwal, 256, 0, c->stream>>>(n, cur, ag, cw, pw, c->inside);
-            colony(gcol, bcol, c, n, cur, prev, pw0, diag, ex);
-        } else {
-            colony(gcol, bcol, c, n, cur, prev, pw0, diag, ex);
-            k_wall<<<gwal, 256, 0, c->stream>>>(n, cur, ag, cw, pw, c->inside);
-        }
-        c->launches += 2;
+        sweep_launch(gcol, bcol, c, n, cur, prev, pw0, diag, ex, ag, cw, pw, count % 2 == 0);
+        c->launches += 1;
         if (c->P.nutrient_gsi == 0) { ce ^= 1; cwb ^= 1; }
         count++;
     }
