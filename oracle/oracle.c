@@ -1765,6 +1765,288 @@ long orc_field(orc_state* s, int field, int level, double* buf, long n, int writ
 #undef ACC
 }
 
+/* ================================================ legacy agar solver ===== */
+/* The explicit agar solver the reference carries but no longer calls
+ * (Simulation.cpp:215-216, 283-284 are commented out):
+ * UpdateEnvArray_OxygenAcetate (Nutrients.cpp:45-197) -- pseudo-time Jacobi
+ * iterations over the colony, the wall rows and every composite agar level
+ * until a convergence count reaches zero -- and
+ * nutrientDepletionAgar_OxygenAcetate (Nutrients.cpp:857-1074) -- explicit
+ * diffusion with the colony's depletion on the coarsest level, then
+ * interpolation back to the finer levels.
+ *
+ * Points the reference leaves undefined: on levels > 0 the agar points with
+ * BoxX/4 <= x < 3 BoxX/4 and z < BoxZAgar/2 (the part a finer level covers)
+ * take second differences that are never initialised (Nutrients.cpp:
+ * 670-697, 728-747).  No other point reads them.  Here they are not
+ * updated (they keep their value, and so add nothing to the convergence
+ * count). */
+#define AIX(x, z) ((long)(x) * P->box_z_agar + (z))
+static int legacy_covered(const bcg_params* P, int level, int x, int z)
+{
+    return level > 0 && x >= P->box_x / 4 && x < 3 * P->box_x / 4 && z <= P->box_z_agar / 2 - 1;
+}
+
+/* UpdateAgarMultigrid_OxygenAcetate (Nutrients.cpp:661-803), NutrientGSI = 0:
+ * one agar point of `level` from the previous agar levels `pa` and the
+ * current wall row of the level */
+static void legacy_agar_point(orc_state* s, aga_t** ca, aga_t** pa, aga_t** cw, int level, int x, int z)
+{
+    const bcg_params* P = &s->P;
+    const int X = P->box_x, ZA = P->box_z_agar, LM = P->max_levels_mg;
+    if (legacy_covered(P, level, x, z)) return;
+    const aga_t* p = pa[level];
+    const aga_t c0 = p[AIX(x, z)];
+    const double h2l = P->box_length * P->box_length * pow(4.0, level);
+    aga_t up = {0, 0, 0, 0}, dn = {0, 0, 0, 0};
+    double Cxx, Czz, Wxx, Wzz, Axx, Azz, Oxx, Ozz;
+    /* z direction */
+    if (z == 0) {
+        up = p[AIX(x, z + 1)]; dn = cw[level][x];
+        Wzz = (up.W + dn.W - 2.0 * c0.W) / h2l; Czz = (up.C + dn.C - 2.0 * c0.C) / h2l;
+        Azz = (up.A + dn.A - 2.0 * c0.A) / h2l; Ozz = (up.O + dn.O - 2.0 * c0.O) / h2l;
+    } else if (level > 0 && x >= X / 4 && x < 3 * X / 4 && z <= ZA / 2) {
+        /* z == ZA/2 here (the rows below are covered) */
+        up = p[AIX(x, z + 1)]; dn = pa[level - 1][AIX(x * 2 - X / 2, ZA - 1)];
+        Wzz = (up.W + dn.W - 2.0 * c0.W) / h2l; Czz = (up.C + dn.C - 2.0 * c0.C) / h2l;
+        Azz = (up.A + dn.A - 2.0 * c0.A) / h2l; Ozz = (up.O + dn.O - 2.0 * c0.O) / h2l;
+    } else if (level < LM - 1 && z == ZA - 1) {
+        const int lx = x % 2;
+        const aga_t u2 = p[AIX(x, z - 2)];
+        const aga_t q1 = pa[level + 1][AIX(x / 2 + X / 4, ZA / 2)];
+        const aga_t q2 = pa[level + 1][AIX((x / 2 + X / 4 + 1) % X, ZA / 2)];
+        Wzz = (u2.W + 1.0 / (lx + 1) * q1.W + lx * 1.0 / (lx + 1) * q2.W - 2.0 * c0.W) / 4 / h2l;
+        Czz = (u2.C + 1.0 / (lx + 1) * q1.C + lx * 1.0 / (lx + 1) * q2.C - 2.0 * c0.C) / 4 / h2l;
+        Azz = (u2.A + 1.0 / (lx + 1) * q1.A + lx * 1.0 / (lx + 1) * q2.A - 2.0 * c0.A) / 4 / h2l;
+        Ozz = (u2.O + 1.0 / (lx + 1) * q1.O + lx * 1.0 / (lx + 1) * q2.O - 2.0 * c0.O) / 4 / h2l;
+    } else if (level == LM - 1 && z == ZA - 1) {
+        const aga_t u1 = p[AIX(x, z - 1)];
+        Wzz = 2.0 * (u1.W - c0.W) / h2l; Czz = 2.0 * (u1.C - c0.C) / h2l;
+        Azz = 2.0 * (u1.A - c0.A) / h2l; Ozz = 2.0 * (u1.O - c0.O) / h2l;
+    } else {
+        up = p[AIX(x, z + 1)]; dn = p[AIX(x, z - 1)];
+        Wzz = (up.W + dn.W - 2.0 * c0.W) / h2l; Czz = (up.C + dn.C - 2.0 * c0.C) / h2l;
+        Azz = (up.A + dn.A - 2.0 * c0.A) / h2l; Ozz = (up.O + dn.O - 2.0 * c0.O) / h2l;
+    }
+    /* x direction */
+    if (level > 0 && x >= X / 4 - 1 && x <= X * 3 / 4 && z <= ZA / 2 - 1) {
+        /* x == X/4 - 1 or x == 3X/4 here (the columns between are covered) */
+        const int lo = (x == X / 4 - 1);
+        const aga_t s1 = p[AIX(lo ? x - 1 : x + 1, z)];
+        const aga_t q = pa[level - 1][AIX(lo ? 0 : X - 2, z * 2 + 1)];
+        Wxx = (s1.W + q.W - 2 * c0.W) / h2l; Cxx = (s1.C + q.C - 2 * c0.C) / h2l;
+        Axx = (s1.A + q.A - 2 * c0.A) / h2l; Oxx = (s1.O + q.O - 2 * c0.O) / h2l;
+    } else if (level < LM - 1 && (x == 0 || x == X - 1)) {
+        const int lz = (z + 1) % 2;
+        const int zq = (z - 1) / 2;
+        const int xq = (x == 0) ? X / 4 - 1 : X * 3 / 4;
+        const aga_t s1 = p[AIX(x == 0 ? x + 2 : x - 1, z)];
+        const aga_t q1 = pa[level + 1][AIX(xq, zq)], q2 = pa[level + 1][AIX(xq, (zq + 1) % ZA)];
+        Wxx = s1.W + 1.0 / (lz + 1) * q1.W + lz * 1.0 / (lz + 1) * q2.W - 2 * c0.W;
+        Cxx = s1.C + 1.0 / (lz + 1) * q1.C + lz * 1.0 / (lz + 1) * q2.C - 2 * c0.C;
+        Axx = s1.A + 1.0 / (lz + 1) * q1.A + lz * 1.0 / (lz + 1) * q2.A - 2 * c0.A;
+        Oxx = s1.O + 1.0 / (lz + 1) * q1.O + lz * 1.0 / (lz + 1) * q2.O - 2 * c0.O;
+        if (x == 0) { Wxx = Wxx / 4 / h2l; Cxx = Cxx / 4 / h2l; Axx = Axx / 4 / h2l; Oxx = Oxx / 4 / h2l; }
+        else { Wxx = Wxx / h2l; Cxx = Cxx / h2l; Axx = Axx / h2l; Oxx = Oxx / h2l; }
+    } else if (level == LM - 1 && (x == 0 || x == X - 1)) {
+        const aga_t s1 = p[AIX(x == 0 ? x + 1 : x - 1, z)];
+        Wxx = (s1.W - 1 * c0.W) / h2l; Cxx = (s1.C - 1.0 * c0.C) / h2l; Axx = (s1.A - 1.0 * c0.A) / h2l;
+        Oxx = (x == 0) ? (s1.O + P->max_o2 - 2 * c0.O) / h2l : (P->max_o2 + s1.O - 2 * c0.O) / h2l;
+    } else {
+        const aga_t xm = p[AIX(x - 1, z)], xp = p[AIX(x + 1, z)];
+        Wxx = (xm.W + xp.W - 2 * c0.W) / h2l; Cxx = (xm.C + xp.C - 2 * c0.C) / h2l;
+        Axx = (xm.A + xp.A - 2 * c0.A) / h2l; Oxx = (xm.O + xp.O - 2 * c0.O) / h2l;
+    }
+    aga_t* o = &ca[level][AIX(x, z)];
+    double Cnew = c0.C + P->diff_agar_carbon * (Cxx + Czz) * P->cdt;
+    double Onew = c0.O + P->diff_agar_o2 * (Oxx + Ozz) * P->cdt;
+    o->C = dmax(0.0, dmin(Cnew, P->max_carbon));
+    o->O = dmax(0.0, dmin(Onew, P->max_o2));
+    double CAcenew = c0.A + P->diff_agar_ace * (Axx + Azz) * P->cdt;
+    o->A = dmax(0.0, CAcenew);
+    double Wnew = c0.W + P->diff_agar * (Wxx + Wzz) * P->cdt;
+    o->W = dmax(0.0, Wnew);
+}
+
+/* the per-point test of Nutrients.cpp:98-101 (carbon, acetate, oxygen) */
+static int legacy_moved(double cur, double prev, double crit)
+{
+    return fabs(cur - prev) > crit * dmax(0.1, fabs(cur));
+}
+
+/* UpdateEnvArray_OxygenAcetate, Nutrients.cpp:45-197, in the 1-thread
+ * order.  Iterations stop after iteration `count` when count > min_iter
+ * and no point moved by more than conv_crit, or at max_iter.  Returns the
+ * iterations run (NutrientGSI = 0). */
+int orc_legacy_env_update(orc_state* s, int min_iter, int max_iter, double conv_crit)
+{
+    const bcg_params* P = &s->P;
+    const int X = P->box_x, ZA = P->box_z_agar, LM = P->max_levels_mg, maxH = s->maxz;
+    env_t *cur = s->env, *prev = s->oenv;
+    aga_t **ca = s->agar, **pa = s->oagar, **cw = s->wal, **pw = s->owal;
+    int count = 0, nbk = 1;
+    while (count < max_iter && nbk) {
+        long conv = 0;
+        int zmin, zmax, dir;
+        if (count % 2 == 0) { zmin = -ZA; zmax = maxH + 1; dir = 1; }
+        else { zmin = -maxH - 1; zmax = ZA; dir = -1; }
+        for (int zi = zmin; zi <= zmax; zi++) {
+            if (zi * dir > 0) {
+                const int z = zi * dir - 1;
+                for (int x = s->minx; x <= s->maxx; x++) {
+                    const long id = IX3(x, z);
+                    const env_t pv = prev[id];
+                    if (s->ds[id] > DBL_EPSILON) colony_point(s, cur, prev, pw[0], x, z);
+                    conv += legacy_moved(cur[id].Carbon, pv.Carbon, conv_crit);
+                    conv += legacy_moved(cur[id].Acetate, pv.Acetate, conv_crit);
+                    conv += legacy_moved(cur[id].Oxygen, pv.Oxygen, conv_crit);
+                }
+            } else if (zi == 0) {
+                for (int level = 0; level < LM; level++)
+                    for (int x = 0; x < X; x++) {
+                        const aga_t pv = pw[level][x];
+                        wall_point(s, cur, pa, cw, pw, level, x);
+                        conv += legacy_moved(cw[level][x].C, pv.C, conv_crit);
+                        conv += legacy_moved(cw[level][x].O, pv.O, conv_crit);
+                        conv += legacy_moved(cw[level][x].A, pv.A, conv_crit);
+                    }
+            } else {
+                const int z = -(zi * dir + 1);
+                for (int level = 0; level < LM; level++)
+                    for (int x = 0; x < X; x++) {
+                        const aga_t pv = pa[level][AIX(x, z)];
+                        legacy_agar_point(s, ca, pa, cw, level, x, z);
+                        const aga_t* c = &ca[level][AIX(x, z)];
+                        conv += legacy_moved(c->C, pv.C, conv_crit);
+                        conv += legacy_moved(c->O, pv.O, conv_crit);
+                        conv += legacy_moved(c->A, pv.A, conv_crit);
+                    }
+            }
+        }
+        env_t* t1 = prev; prev = cur; cur = t1;
+        aga_t** t2 = pa; pa = ca; ca = t2;
+        aga_t** t3 = pw; pw = cw; cw = t3;
+        if (count > min_iter && conv == 0) nbk = 0;
+        count++;
+    }
+    /* the swaps were of local pointers, as in the reference: the arrays
+     * keep their roles, and iteration k wrote Environment / FieldAgar /
+     * FieldWall when k is even, the old ones when k is odd */
+    return count;
+}
+
+static int ipow_i(int b, int e) { int r = 1; while (e-- > 0) r *= b; return r; }
+
+/* nutrientDepletionAgar_OxygenAcetate, Nutrients.cpp:857-896, with
+ * restrictionAgar (:898-927), UpdateDepletionAgar (:997-1072) and
+ * interpolation (:929-995).  Returns the explicit steps run. */
+int orc_legacy_depletion(orc_state* s)
+{
+    const bcg_params* P = &s->P;
+    const int X = P->box_x, ZA = P->box_z_agar, LM = P->max_levels_mg;
+    aga_t **Aga = s->agar, **prevAga = s->oagar, **Wall = s->wal, **prevWall = s->owal;
+    const int level = LM - 1;
+    const double h2 = P->box_length * P->box_length * ipow_i(4, level);
+    const double dtd = dmin(P->diff_agar_ace, P->diff_agar_carbon) / 10 * h2;
+    const int n = (int)(3600 * P->update_time * 740 / dtd);
+    /* restrictionAgar: the coarsest level takes each point from the finest
+     * level covering it */
+    for (int zi = 0; zi < ZA; zi++)
+        for (int xi = 0; xi < X; xi++) {
+            int l = (int)ceil(log((1 + zi) * ipow_i(2, LM - 1) * 1.0 / ZA) / log(2));
+            if (l < 0) l = 0;
+            int lx = 0;
+            if (xi < X / 2) lx = (int)ceil(log(1 - xi * 2.0 / X) / log(2) + LM - 1);
+            else if (xi > X / 2) lx = (int)floor(log(xi * 2.0 / X - 1) / log(2) + LM - 1) + 1;
+            if (lx > l) l = lx;
+            const int x2 = (xi - X / 2) * ipow_i(2, LM - 1 - l) + X / 2;
+            const int z2 = (zi + 1) * ipow_i(2, LM - 1 - l) - 1;
+            if (l < LM - 1) {
+                Aga[LM - 1][AIX(xi, zi)].C = Aga[l][AIX(x2, z2)].C;
+                Aga[LM - 1][AIX(xi, zi)].A = Aga[l][AIX(x2, z2)].A;
+                prevAga[LM - 1][AIX(xi, zi)].C = prevAga[l][AIX(x2, z2)].C;
+                prevAga[LM - 1][AIX(xi, zi)].A = prevAga[l][AIX(x2, z2)].A;
+            }
+        }
+    aga_t* cur = Aga[level];
+    aga_t* prv = prevAga[level];
+    const double h2l = P->box_length * P->box_length * pow(4.0, level);
+    int count = 0;
+    while (count <= n) {
+        for (int z = 0; z < ZA; z++)
+            for (int x = 0; x < X; x++) {
+                const aga_t c0 = prv[AIX(x, z)];
+                double Cxx, Axx, Czz, Azz;
+                if (x == 0) {
+                    Cxx = (2 * prv[AIX(x + 1, z)].C - 2 * c0.C) / h2l;
+                    Axx = (2 * prv[AIX(x + 1, z)].A - 2 * c0.A) / h2l;
+                } else if (x == X - 1) {
+                    Cxx = (prv[AIX(x - 1, z)].C - c0.C) / h2l;
+                    Axx = (prv[AIX(x - 1, z)].A - c0.A) / h2l;
+                } else {
+                    Cxx = (prv[AIX(x + 1, z)].C + prv[AIX(x - 1, z)].C - 2 * c0.C) / h2l;
+                    Axx = (prv[AIX(x + 1, z)].A + prv[AIX(x - 1, z)].A - 2 * c0.A) / h2l;
+                }
+                if (z == 0) {
+                    int lx = 0;
+                    if (x < X / 2) lx = (int)ceil(log(1 - x * 2.0 / X) / log(2) + LM - 1);
+                    else if (x > X / 2) lx = (int)floor(log(x * 2.0 / X - 1) / log(2) + LM - 1) + 1;
+                    if (lx < 0) lx = 0;
+                    const int xw = (x - X / 2) * ipow_i(2, LM - 1 - lx) + X / 2;
+                    if (lx == 0 && s->inside[IX3(xw, 0)] > 0.5) {
+                        /* the depletion flux is computed and never used
+                         * (Nutrients.cpp:1042-1047): no z flux here */
+                        Czz = 0; Azz = 0;
+                    } else {
+                        Czz = (prv[AIX(x, z + 1)].C + 0.0 * pow(2.0, level) - c0.C) / h2l;
+                        Azz = (prv[AIX(x, z + 1)].A + 0.0 * pow(2.0, level) - c0.A) / h2l;
+                    }
+                } else if (z == ZA - 1) {
+                    Czz = (2 * prv[AIX(x, z - 1)].C - 2 * c0.C) / h2l;
+                    Azz = (2 * prv[AIX(x, z - 1)].A - 2 * c0.A) / h2l;
+                } else {
+                    Czz = (prv[AIX(x, z + 1)].C + prv[AIX(x, z - 1)].C - 2 * c0.C) / h2l;
+                    Azz = (prv[AIX(x, z + 1)].A + prv[AIX(x, z - 1)].A - 2 * c0.A) / h2l;
+                }
+                cur[AIX(x, z)].C += dtd * P->diff_agar_carbon * (Cxx + Czz);
+                cur[AIX(x, z)].A += dtd * P->diff_agar_ace * (Axx + Azz);
+            }
+        for (long i = 0; i < (long)X * ZA; i++) { prv[i].C = cur[i].C; prv[i].A = cur[i].A; }
+        count++;
+    }
+    /* interpolation: every finer level from the next coarser one */
+    for (int l = LM - 1; l > 0; l--)
+        for (int zi = 0; zi < ZA; zi++)
+            for (int xi = 0; xi < X; xi++) {
+                double a1 = 0, a2 = 0, c1 = 0, c2 = 0;
+                if (zi == 0) {
+                    for (int i1 = 0; i1 < 2; i1++) {
+                        const long q = AIX((xi + i1) / 2 + X / 4, 0);
+                        c1 += Aga[l][q].C / 4; c2 += prevAga[l][q].C / 4;
+                        a1 += Aga[l][q].A / 4; a2 += prevAga[l][q].A / 4;
+                    }
+                    int lx = 0;
+                    if (xi < X / 2) lx = (int)ceil(log(1 - xi * 2.0 / X) / log(2) + l);
+                    else if (xi > X / 2) lx = (int)floor(log(xi * 2.0 / X - 1) / log(2) + l) + 1;
+                    if (lx < 0) lx = 0;
+                    const int xw = (xi - X / 2) * ipow_i(2, l - lx) + X / 2;
+                    c1 += Wall[lx][xw].C / 2; c2 += prevWall[lx][xw].C / 2;
+                    a1 += Wall[lx][xw].A / 2; a2 += prevWall[lx][xw].A / 2;
+                } else {
+                    for (int i1 = 0; i1 < 2; i1++)
+                        for (int i2 = 0; i2 < 2; i2++) {
+                            const long q = AIX((xi + i1) / 2 + X / 4, (zi - i2) / 2);
+                            c1 += Aga[l][q].C / 4; c2 += prevAga[l][q].C / 4;
+                            a1 += Aga[l][q].A / 4; a2 += prevAga[l][q].A / 4;
+                        }
+                }
+                Aga[l - 1][AIX(xi, zi)].C = c1; prevAga[l - 1][AIX(xi, zi)].C = c2;
+                Aga[l - 1][AIX(xi, zi)].A = a1; prevAga[l - 1][AIX(xi, zi)].A = a2;
+            }
+    return count;
+}
+#undef AIX
+
 /* ------------------------------------------------------------------------
  * Inputs for the reference arm of the benchmark, so that it builds its
  * workload without loading the CUDA library: the parameter defaults of

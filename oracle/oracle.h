@@ -42,6 +42,11 @@ int  orc_loop_step(orc_state* s, int* lineage);
 long long orc_mean_stress(orc_state* s, double* stress, double* fnet);
 double orc_time(orc_state* s);
 
+/* the legacy explicit agar solver (UpdateEnvArray_OxygenAcetate,
+ * nutrientDepletionAgar_OxygenAcetate) */
+int orc_legacy_env_update(orc_state* s, int min_iter, int max_iter, double conv_crit);
+int orc_legacy_depletion(orc_state* s);
+
 /* inputs of the benchmark's reference arm (no CUDA library loaded there) */
 int orc_params_default(bcg_params* p);
 int orc_params_finalize(bcg_params* p);

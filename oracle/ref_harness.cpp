@@ -406,6 +406,25 @@ void ref_nutrient_update(int n)
     UpdateTime = save;
 }
 
+/* UpdateEnvArray_OxygenAcetate (Nutrients.cpp:45-197), the legacy explicit
+ * solver, for exactly `iters` iterations: minIter = maxIter = iters for the
+ * call, so the convergence count (which also counts the points the
+ * reference leaves undefined) cannot end it early.  Returns its count. */
+int ref_legacy_env_update(int iters)
+{
+    const int save_min = minIter, save_max = maxIter;
+    minIter = iters; maxIter = iters;
+    int n = UpdateEnvArray_OxygenAcetate(S.Env, S.oldEnv, S.FieldAgar, S.oldFieldAgar, S.FieldWall, S.oldFieldWall, *S.DensityShiftP, *S.Density1ShiftP, *S.Density2ShiftP, *S.WallDensityShiftP, *S.WallDensity1ShiftP, *S.WallDensity2ShiftP, S.minx, S.maxx, S.miny, S.maxy, S.maxz, *S.Height, *S.insideColonyDen);
+    minIter = save_min; maxIter = save_max;
+    return n;
+}
+
+/* nutrientDepletionAgar_OxygenAcetate (Nutrients.cpp:857-896); returns its count */
+int ref_legacy_depletion(void)
+{
+    return nutrientDepletionAgar_OxygenAcetate(S.FieldAgar, S.oldFieldAgar, S.FieldWall, S.oldFieldWall, *S.insideColonyDen);
+}
+
 /* Multigrid::solve with a chosen V-cycle count (solve() fixes 3). */
 void ref_mg_solve(int vcycles, double dt)
 {

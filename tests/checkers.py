@@ -66,6 +66,8 @@ def oracle_lib():
         _proto(lib, "orc_loop_step", ctypes.c_int, [_VP, _PI])
         _proto(lib, "orc_time", ctypes.c_double, [_VP])
         _proto(lib, "orc_mean_stress", ctypes.c_longlong, [_VP, _PD, _PD])
+        _proto(lib, "orc_legacy_env_update", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_double])
+        _proto(lib, "orc_legacy_depletion", ctypes.c_int, [_VP])
         _proto(lib, "orc_params_default", ctypes.c_int, [_PP])
         _proto(lib, "orc_params_finalize", ctypes.c_int, [_PP])
         _proto(lib, "orc_synth_colony", ctypes.c_int,
@@ -127,6 +129,8 @@ def ref_lib():
         _proto(lib, "ref_surface_forces", None, [_PD])
         _proto(lib, "ref_output_cells_given", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _PD, ctypes.c_int])
         _proto(lib, "ref_set_new_cells", ctypes.c_int, [_VP, ctypes.c_int])
+        _proto(lib, "ref_legacy_env_update", ctypes.c_int, [ctypes.c_int])
+        _proto(lib, "ref_legacy_depletion", ctypes.c_int, [])
         _ref = lib
     return _ref
 
@@ -246,6 +250,14 @@ class Oracle(_Model):
     def nutrient_update(self, n=0):
         self.lib.orc_nutrient_update(self.h, n)
 
+    def legacy_env_update(self, iters, min_iter=None, conv_crit=1e-4):
+        """UpdateEnvArray_OxygenAcetate: exactly `iters` iterations unless
+        min_iter is given (then the convergence test may end it earlier)."""
+        return self.lib.orc_legacy_env_update(self.h, iters if min_iter is None else min_iter, iters, conv_crit)
+
+    def legacy_depletion(self):
+        return self.lib.orc_legacy_depletion(self.h)
+
     def mg_solve(self, vcycles=3, dt=100.0):
         self.lib.orc_mg_solve(self.h, vcycles, dt)
 
@@ -330,6 +342,12 @@ class Reference(_Model):
 
     def nutrient_update(self, n=0):
         self.lib.ref_nutrient_update(n)
+
+    def legacy_env_update(self, iters):
+        return self.lib.ref_legacy_env_update(iters)
+
+    def legacy_depletion(self):
+        return self.lib.ref_legacy_depletion()
 
     def mg_solve(self, vcycles=3, dt=100.0):
         self.lib.ref_mg_solve(vcycles, dt)

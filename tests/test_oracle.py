@@ -195,3 +195,75 @@ def test_oracle_inputs_equal_library_inputs():
     for entry in (None, ck.oracle_synth_entry()):
         with pytest.raises(_abi.BcgError):
             synth_colony(2000, w, h, seed=99, entry=entry)
+
+
+def legacy_masks(p):
+    """Points of the legacy explicit agar solver that the reference defines:
+    on levels > 0 the agar points with BoxX/4 <= x < 3 BoxX/4, z < BoxZAgar/2
+    and the wall points with BoxX/4 <= x < 3 BoxX/4 read second differences
+    that are never initialised (Nutrients.cpp:509-803); nothing else reads
+    them."""
+    X, ZA = p.box_x, p.box_z_agar
+    agar, wall = [], []
+    for l in range(p.max_levels_mg):
+        a = np.ones((X, ZA), dtype=bool)
+        w = np.ones(X, dtype=bool)
+        if l > 0:
+            a[X // 4:3 * X // 4, :ZA // 2] = False
+            w[X // 4:3 * X // 4] = False
+        agar.append(a.reshape(-1))
+        wall.append(w)
+    return agar, wall
+
+
+def legacy_pair(n=4096):
+    p = params.workload_params("small_4k")
+    cells = workload_colony("small_4k", n=n)
+    models = [ck.Oracle(p, seed=12345), ck.Reference(p, seed=12345)]
+    for m in models:
+        m.load(cells)
+        m.update_density()
+    rows = depleted_wall(p, models[0].field(F["INSIDE"]))
+    for m in models:
+        for name, v in zip(("WALLF_CARBON", "WALLF_OXYGEN", "WALLF_ACETATE"), rows):
+            m.set_field(F[name], v, 0)
+            m.set_field(F["OLD" + name], v, 0)
+    return p, models
+
+
+def legacy_compare(p, a, b):
+    agar, wall = legacy_masks(p)
+    for f in ("ENV_CARBON", "ENV_WASTE", "ENV_OXYGEN", "ENV_ACETATE", "OLDENV_CARBON", "OLDENV_ACETATE"):
+        assert np.array_equal(a.field(F[f]), b.field(F[f])), f
+    for l in range(p.max_levels_mg):
+        for sp in ("CARBON", "OXYGEN", "ACETATE"):
+            f = "AGARF_" + sp
+            assert np.array_equal(a.field(F[f], l)[agar[l]], b.field(F[f], l)[agar[l]]), (f, l)
+            for f in ("WALLF_" + sp, "OLDWALLF_" + sp):
+                assert np.array_equal(a.field(F[f], l)[wall[l]], b.field(F[f], l)[wall[l]]), (f, l)
+
+
+@needs_ref
+@pytest.mark.parametrize("iters", [7, 30])
+def test_oracle_legacy_env_update_matches_reference(iters):
+    """UpdateEnvArray_OxygenAcetate (the legacy explicit colony + wall + agar
+    iterations) for a fixed count: the restatement equals the reference bit
+    for bit at every point the reference defines."""
+    p, (orc, ref) = legacy_pair()
+    assert orc.legacy_env_update(iters) == ref.legacy_env_update(iters) == iters
+    legacy_compare(p, orc, ref)
+    # the agar moved (the wall under the colony is depleted)
+    assert np.abs(orc.field(F["AGARF_CARBON"], 0) - p.max_carbon).max() > 0
+
+
+@needs_ref
+def test_oracle_legacy_depletion_matches_reference():
+    """nutrientDepletionAgar_OxygenAcetate after a few legacy iterations:
+    restriction to the coarsest level, its explicit steps, interpolation
+    back; bit for bit at the defined points."""
+    p, (orc, ref) = legacy_pair()
+    orc.legacy_env_update(5)
+    ref.legacy_env_update(5)
+    n = orc.legacy_depletion()
+    assert n == ref.legacy_depletion() and n > 100
+    legacy_compare(p, orc, ref)
