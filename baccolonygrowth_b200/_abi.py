@@ -220,6 +220,8 @@ PROTOTYPES = {
     "bcg_sim_ctx": (_VP, [_VP]),
     "bcg_sim_time": (_I, [_VP, _PD, _PI, _PI64]),
     "bcg_sim_counters": (_I, [_VP, _PI64, _PI64]),
+    "bcg_legacy_env_update": (_I, [_VP, _I, _I, _D, _PI]),
+    "bcg_legacy_agar_depletion": (_I, [_VP, _PI]),
     "bcg_set_force_group": (_I, [_VP, _I]),
     "bcg_set_relax_mode": (_I, [_VP, _I]),
     "bcg_set_smoother_warps": (_I, [_VP, _I]),

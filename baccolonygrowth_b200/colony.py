@@ -216,6 +216,20 @@ class Colony:
     def mg_solve(self, vcycles=0):
         _abi.check(self.lib.bcg_mg_solve(self.h, vcycles), "bcg_mg_solve")
 
+    def legacy_env_update(self, max_iter, min_iter=None, conv_crit=1e-4):
+        """bcg_legacy_env_update (UpdateEnvArray_OxygenAcetate): exactly
+        max_iter iterations unless min_iter is given; returns the count."""
+        n = ctypes.c_int()
+        _abi.check(self.lib.bcg_legacy_env_update(self.h, max_iter if min_iter is None else min_iter, max_iter,
+                                                  conv_crit, ctypes.byref(n)), "bcg_legacy_env_update")
+        return n.value
+
+    def legacy_depletion(self):
+        """bcg_legacy_agar_depletion (nutrientDepletionAgar_OxygenAcetate); returns the steps run."""
+        n = ctypes.c_int()
+        _abi.check(self.lib.bcg_legacy_agar_depletion(self.h, ctypes.byref(n)), "bcg_legacy_agar_depletion")
+        return n.value
+
     def colony_sweeps(self, sweeps, count0=0):
         _abi.check(self.lib.bcg_colony_sweeps(self.h, sweeps, count0), "bcg_colony_sweeps")
 

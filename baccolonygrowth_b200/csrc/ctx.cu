@@ -297,6 +297,11 @@ extern "C" int bcg_destroy(bcg_ctx* c)
                           c->mg[l].err2[sp], c->mg[l].errf2[sp]};
             for (void* q : ma) if (q) cudaFree(q);
         }
+    for (int b = 0; b < 2; b++)
+        for (int l = 0; l < BCG_MAX_AGAR_LEVELS; l++)
+            for (int sp = 0; sp < 4; sp++) if (c->leg[b][l][sp]) cudaFree(c->leg[b][l][sp]);
+    if (c->leg_snap) cudaFree(c->leg_snap);
+    if (c->leg_conv) cudaFree(c->leg_conv);
     for (int g = 0; g < 2; g++) if (c->nutrient_graph[g]) cudaGraphExecDestroy(c->nutrient_graph[g]);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (int t = 0; t < BCG_T_COUNT; t++) { if (c->ev[t][0]) cudaEventDestroy(c->ev[t][0]); if (c->ev[t][1]) cudaEventDestroy(c->ev[t][1]); }

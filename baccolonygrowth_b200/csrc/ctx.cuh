@@ -119,6 +119,15 @@ struct bcg_ctx {
     int mg_res0_stale;
     int pair_f32;          /* contact geometry in FP32 local to cell i (bcg_set_pair_precision) */
     int pending_error;     /* host-side set-up failure of a queued launch, returned by the next status check */
+    /* legacy explicit agar solver (allocated on its first call): FieldAgar
+     * [0] and oldFieldAgar [1] per composite level, species carbon, waste,
+     * oxygen, acetate, box_z_agar rows of box_x (row z contiguous); the
+     * multigrid solution rows 1..box_z_agar stand for FieldAgar elsewhere */
+    double* leg[2][BCG_MAX_AGAR_LEVELS][4];
+    double* leg_snap;      /* acetate before the last iteration's write (box_x*box_z) + wall row (box_x) */
+    unsigned long long* leg_conv;   /* convergence count per iteration */
+    int leg_conv_cap;
+    int leg_old_stale;     /* an agar solve ran since: oldFieldAgar := FieldAgar (copyFromMG) */
     double smooth_tune_ms; /* device time of one level-0 fused smoother launch at the tuned shape */
 };
 

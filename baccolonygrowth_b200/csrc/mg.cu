@@ -1583,6 +1583,7 @@ void mg_copy_to(bcg_ctx* c, const MgConst& m, int wall_buf)
 
 void mg_copy_from(bcg_ctx* c, const MgConst& m, int cur_wall)
 {
+    c->leg_old_stale = 1;        /* copyFromMG writes FieldAgar and oldFieldAgar alike */
     for (int l = 0; l < m.A; l++) {
         MgLvl L = mg_lvl(c, l);
         const WallBuf& cw = c->wal[cur_wall];

@@ -283,6 +283,36 @@ int bcg_initial_density(bcg_ctx* ctx);
  * n <= 0 selects params.solves_per_update; sweeps < 0 selects
  * params.sweeps_per_solve. */
 int bcg_nutrient_update(bcg_ctx* ctx, int n, int sweeps);
+
+/* The legacy explicit agar solver, which the reference keeps but no longer
+ * calls (its call sites, Simulation.cpp:215-216 and 283-284, are commented
+ * out); a host that restores them calls these two in place of
+ * bcg_nutrient_update.
+ *
+ * bcg_legacy_env_update replaces UpdateEnvArray_OxygenAcetate
+ * (Nutrients.cpp:45-197): pseudo-time Jacobi iterations over the colony
+ * (UpdateEnvironment_OxygenAcetate), the wall rows and every composite agar
+ * level (UpdateAgarMultigrid_OxygenAcetate), alternating direction, until
+ * after iteration `count` with count > min_iter no point of carbon, oxygen
+ * or acetate moved by more than conv_crit * max(0.1, |value|), or max_iter
+ * iterations (the reference's ConvCrit, minIter, maxIter: 1e-4, 500, 20000).
+ * *iterations receives the count, as the reference returns it.
+ *
+ * bcg_legacy_agar_depletion replaces nutrientDepletionAgar_OxygenAcetate
+ * (Nutrients.cpp:857-1074): the coarsest level takes each point from the
+ * finest level that holds it, runs int(3600 UpdateTime 740 / dt) + 1
+ * explicit steps of carbon and acetate diffusion (dt = min(D) h^2 / 10),
+ * and every finer level is interpolated back from it; *steps receives the
+ * steps run.
+ *
+ * Both keep their own FieldAgar / oldFieldAgar of the four species; the
+ * agar solution rows stand for FieldAgar elsewhere, so each call starts
+ * from them and writes them back.  On levels > 0 the reference leaves the
+ * agar points with BoxX/4 <= x < 3 BoxX/4, z < BoxZAgar/2 undefined
+ * (uninitialised second differences) and no other point reads them; they
+ * are not updated here. */
+int bcg_legacy_env_update(bcg_ctx* ctx, int min_iter, int max_iter, double conv_crit, int* iterations);
+int bcg_legacy_agar_depletion(bcg_ctx* ctx, int* steps);
 /* One Multigrid::solve (Multigrid.cpp:864-889) with `vcycles` V-cycles
  * (<=0: params.mg_vcycles): copyToMG, setup, V-cycles, reset, copyFromMG. */
 int bcg_mg_solve(bcg_ctx* ctx, int vcycles);

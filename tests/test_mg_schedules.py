@@ -23,6 +23,7 @@ the result.
   row segment it is the sequential order exactly, and with warm-started
   segments it agrees with it to rounding.
 """
+import math
 import random
 
 import pytest
@@ -303,3 +304,54 @@ def test_tma_smoother_warm_segments_agree_to_rounding():
         assert set(out) == set(ref)
         err = max(abs(out[p] - ref[p]) for p in ref)
         assert err < 1e-14, (nseg, err)
+
+
+def native_level_int(x, X, lv):
+    """csrc/nutrients.cu leg_native_level: the finest composite level whose
+    extent holds column x of a level-lv row, in integers."""
+    if x < X // 2:
+        k = 0
+        while (X - 2 * x) << (k + 1) <= X:
+            k += 1
+        return lv - k
+    if x > X // 2:
+        k = 0
+        while ((2 * x - X) << k) < X:
+            k += 1
+        return lv - k + 1
+    return 0
+
+
+def native_level_ref(x, X, lv):
+    """The reference's form (Nutrients.cpp:917-921, 947-951, 1027-1031)."""
+    if x < X // 2:
+        return math.ceil(math.log(1 - x * 2.0 / X) / math.log(2) + lv)
+    if x > X // 2:
+        return math.floor(math.log(x * 2.0 / X - 1) / math.log(2) + lv) + 1
+    return 0
+
+
+def row_level_int(z, ZA, A):
+    v = (1 + z) << (A - 1)
+    if v <= ZA:
+        return 0
+    k = 0
+    while (ZA << k) < v:
+        k += 1
+    return k
+
+
+def row_level_ref(z, ZA, A):
+    return max(math.ceil(math.log((1 + z) * (2 ** (A - 1)) * 1.0 / ZA) / math.log(2)), 0)
+
+
+@pytest.mark.parametrize("X,ZA,A", [(256, 32, 2), (2304, 512, 3), (4608, 1024, 3), (1520, 512, 3), (99, 17, 4),
+                                    (128, 64, 2)])
+def test_depletion_level_maps_in_integers(X, ZA, A):
+    """The GPU's integer forms of the legacy solver's level maps give the
+    reference's floating-point ceil/floor of log2 at every column and row."""
+    for lv in range(A):
+        for x in range(X):
+            assert native_level_int(x, X, lv) == native_level_ref(x, X, lv), (x, lv)
+    for z in range(ZA):
+        assert row_level_int(z, ZA, A) == row_level_ref(z, ZA, A), z
