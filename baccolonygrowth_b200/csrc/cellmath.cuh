@@ -123,40 +123,63 @@ __device__ __forceinline__ bool pair_force(const Cst& a, V3 acm, const Cst& b, c
     return pair_force_at(a, acm, b, mp, c1, c2, d, F, r);
 }
 
-/* min_distance in FP32 on offsets local to a reference point (the centre
- * of cell a): the offsets are a few um, so their FP32 rounding is ~1e-7 um
- * where absolute positions (up to 1e4 um) would lose ~1e-3 um */
+/* min_distance's search in FP32, on offsets local to a reference point
+ * (the centre of cell a): the offsets are a few um, so their FP32 rounding
+ * is ~1e-7 um where absolute positions (up to 1e4 um) would lose ~1e-3 um.
+ * Same clamping steps as seg_distance; returns which of its branches holds
+ * the minimum: 1 = t clamped to 0, 2 = t clamped to 1, 3 = t from the
+ * projection with s clamped to an end, 0 = both interior (crossing or
+ * nearly parallel segments). */
 struct F3 { float x, y, z; };
 __device__ __forceinline__ F3 f3_off(V3 a, V3 o) { F3 r; r.x = (float)(a.x - o.x); r.y = (float)(a.y - o.y); r.z = (float)(a.z - o.z); return r; }
 __device__ __forceinline__ float f3_dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float clamp01f(float n) { return n < 0.f ? 0.f : (n > 1.f ? 1.f : n); }
-__device__ __forceinline__ float seg_distance_f(F3 p1, F3 q1, F3 p2, F3 q2, F3& c1, F3& c2)
+__device__ __forceinline__ int seg_branch_f(F3 p1, F3 q1, F3 p2, F3 q2, float& s)
 {
     F3 v1 = {q1.x - p1.x, q1.y - p1.y, q1.z - p1.z}, v2 = {q2.x - p2.x, q2.y - p2.y, q2.z - p2.z};
     F3 r = {p1.x - p2.x, p1.y - p2.y, p1.z - p2.z};
     float l1 = f3_dot(v1, v1), l2 = f3_dot(v2, v2), f = f3_dot(v2, r), c = f3_dot(v1, r), b = f3_dot(v1, v2);
-    float denom = l1 * l2 - b * b, s, t;
+    float denom = l1 * l2 - b * b;
     if (denom != 0.f) s = clamp01f((b * f - c * l2) / denom);
     else s = 0.f;
     float tnom = b * s + f;
-    if (tnom < 0.f) { t = 0.f; s = clamp01f(-c / l1); }
-    else if (tnom > l2) { t = 1.f; s = clamp01f((b - c) / l1); }
-    else t = tnom / l2;
-    c1 = {p1.x + v1.x * s, p1.y + v1.y * s, p1.z + v1.z * s};
-    c2 = {p2.x + v2.x * t, p2.y + v2.y * t, p2.z + v2.z * t};
-    F3 cv = {c1.x - c2.x, c1.y - c2.y, c1.z - c2.z};
-    return sqrtf(f3_dot(cv, cv));
+    if (tnom < 0.f) return 1;
+    if (tnom > l2) return 2;
+    return (s == 0.f || s == 1.f) ? 3 : 0;
 }
 
-/* F_cc with the contact geometry in FP32 local to cell a; the force terms,
- * the contact point and the sums stay FP64 */
+/* F_cc with min_distance's branch found in FP32 local to cell a, and the
+ * branch's own formula (a projection of a pole, one division) then taken in
+ * FP64 from the FP64 poles: the closest points, their distance, the
+ * contact normal and the forces are FP64 values, which differ from the
+ * all-FP64 search only where FP32 rounding picks another branch at a
+ * branch boundary (the distance is continuous there).  Both-interior
+ * minima (crossing or nearly parallel segments) take the FP64 search. */
 __device__ __forceinline__ bool pair_force_f32geom(const Cst& a, V3 acm, const Cst& b, const MechParams& mp, V3& F, V3& r)
 {
-    F3 c1f, c2f;
-    float df = seg_distance_f(f3_off(a.p, acm), f3_off(a.q, acm), f3_off(b.p, acm), f3_off(b.q, acm), c1f, c2f);
-    V3 c1 = mk(acm.x + (double)c1f.x, acm.y + (double)c1f.y, acm.z + (double)c1f.z);
-    V3 c2 = mk(acm.x + (double)c2f.x, acm.y + (double)c2f.y, acm.z + (double)c2f.z);
-    return pair_force_at(a, acm, b, mp, c1, c2, (double)df, F, r);
+    float sf;
+    const int br = seg_branch_f(f3_off(a.p, acm), f3_off(a.q, acm), f3_off(b.p, acm), f3_off(b.q, acm), sf);
+    V3 c1, c2;
+    double d;
+    if (br == 0) {
+        d = seg_distance(a.p, a.q, b.p, b.q, c1, c2);
+    } else {
+        const V3 v1 = sub3(a.q, a.p), v2 = sub3(b.q, b.p), rr = sub3(a.p, b.p);
+        double s, t;
+        if (br == 3) {
+            s = (double)sf;
+            t = clamp01((dot3(v1, v2) * s + dot3(v2, rr)) / dot3(v2, v2));
+        } else {
+            const double l1 = dot3(v1, v1), c = dot3(v1, rr);
+            t = (br == 1) ? 0.0 : 1.0;
+            s = (br == 1) ? clamp01(-c / l1) : clamp01((dot3(v1, v2) - c) / l1);
+        }
+        c1 = add3(a.p, scl3(v1, s));
+        c2 = add3(b.p, scl3(v2, t));
+        const V3 cv = sub3(c1, c2);
+        d = sqrt(dot3(cv, cv));
+    }
+    return pair_force_at(a, acm, b, mp, c1, c2, d, F, r);
 }
 
 /* one locus of F_cw, Forces.cpp:96-152 (var_pos = 0, so the locus sits at
