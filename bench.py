@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--no-output", action="store_true", help="skip the output-step measurement")
+    ap.add_argument("--no-dense", action="store_true", help="skip the densely packed colony's mechanics line")
     ap.add_argument("--no-field-update", action="store_true",
                     help="skip the field update at the reference's cadence (266 solves + 200 sweeps each)")
     ap.add_argument("--smoother-warps", type=int, default=0,
@@ -306,6 +307,75 @@ def sim_rebuilds(lib, sim):
     f = ctypes.c_int64()
     lib.bcg_sim_counters(sim, ctypes.byref(r), ctypes.byref(f))
     return int(r.value)
+
+
+def mean_neighbours(lib, ctx):
+    """Mean length of the reduced neighbour lists (the k of the per-pair work)."""
+    import numpy as np
+    from baccolonygrowth_b200 import _abi
+    n = ctypes.c_int()
+    lib.bcg_num_cells(ctx, ctypes.byref(n))
+    counts = np.zeros(max(n.value, 1), dtype=np.int32)
+    lists = np.zeros(max(n.value, 1), dtype=np.int32)
+    _abi.check(lib.bcg_get_neighbours(ctx, _abi.ptr(counts, ctypes.c_int), _abi.ptr(lists, ctypes.c_int), 1),
+               "bcg_get_neighbours")
+    return float(counts[:n.value].mean()) if n.value else 0.0
+
+
+def dense_mechanics_bench(lib, p, steps, warmup):
+    """Mechanics alone (neighbour rebuild on its cadence, MoveCell/GrowCell,
+    divisions; no agar solve) on a densely packed 1M-cell colony
+    (colony.packed_colony: layers of touching cells, about 8 neighbours a
+    cell), on the bench grid, timed like the main line."""
+    import numpy as np
+    import torch
+    from baccolonygrowth_b200 import _abi, params as _params
+    from baccolonygrowth_b200.colony import packed_colony
+    out = {}
+    try:
+        n = 1048576
+        w, h = _params.dome_size(n, 25.0 / 600.0, 0.9)
+        cells = np.ascontiguousarray(packed_colony(n, w, h))
+        sim = ctypes.c_void_p()
+        _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(cells), n, 12345, 0, ctypes.byref(sim)), "dense sim")
+        try:
+            _abi.check(lib.bcg_sim_set_step_mode(sim, 0, 0), "dense mode")
+            ctx = lib.bcg_sim_ctx(sim)
+            g = np.full(p.box_x * p.box_z, 0.9)
+            _abi.check(lib.bcg_set_field(ctx, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size), "g")
+            _abi.check(lib.bcg_update_density(ctx), "density")
+            _abi.check(lib.bcg_rebuild_neighbours(ctx), "rebuild")
+            ch = ctypes.c_int()
+            _abi.check(lib.bcg_autotune(ctx, _abi.TUNE["FORCE_GROUP"], ctypes.byref(ch)), "autotune")
+            _abi.check(lib.bcg_sim_run(sim, warmup), "dense warmup")
+            stream = torch.cuda.ExternalStream(lib.bcg_stream(ctx))
+            rb0 = sim_rebuilds(lib, sim)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _abi.check(lib.bcg_sim_run(sim, steps), "dense steps")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            rb = time_rebuild(lib, ctx)
+            every = steps_per_update(p)
+            ms = ms - (sim_rebuilds(lib, sim) - rb0) * rb + steps * rb / every
+            _abi.check(lib.bcg_enable_timers(ctx, 1), "timers")
+            _abi.check(lib.bcg_sim_run(sim, min(steps, 10)), "dense timer steps")
+            mg = ctypes.c_double(); nl = ctypes.c_int64()
+            lib.bcg_get_timer(ctx, _abi.TIMERS["MOVE_GROW"], ctypes.byref(mg), ctypes.byref(nl))
+            _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
+            k = mean_neighbours(lib, ctx)
+            out.update(cells=n, mean_neighbours=k, force_group=ch.value, ms_per_step=ms / steps,
+                       move_grow_ms=mg.value / min(steps, 10), rebuild_ms=rb,
+                       cell_steps_per_s=n * steps / (ms / 1e3),
+                       note="mechanics only: no agar solve in the step")
+        finally:
+            lib.bcg_sim_destroy(sim)
+    except Exception as e:      # reported, not required
+        out["error"] = str(e)
+    return out
 
 
 def time_rebuild(lib, ctx, reps=3):
@@ -730,6 +800,7 @@ def b200_arm(args):
                               "holds 1e-10 against the oracle"}
     except Exception as e:      # reported, not required
         pair32 = {"error": str(e)}
+    k_mean_measured = mean_neighbours(lib, ctx)
     n_now = ctypes.c_int()
     lib.bcg_num_cells(ctx, ctypes.byref(n_now))
     colony = colony_sweep_bench(lib, ctx) if world == 1 else None
@@ -804,6 +875,10 @@ def b200_arm(args):
     if not args.no_ensemble and world == 1:
         ens = ensemble_bench(lib, args)
 
+    dense = None
+    if world == 1 and not args.no_dense:
+        dense = dense_mechanics_bench(lib, p, min(args.steps, 20), args.warmup)
+
     # an output step through the asynchronous writer, last so that its
     # file traffic does not disturb the measurements above
     out_step = None
@@ -837,8 +912,7 @@ def b200_arm(args):
     mg_ms = timers["MG_SOLVE"]
     mech_ms = timers["MOVE_GROW"]
     mg_bytes = mg_solve_bytes(p, args.vcycles)
-    k_mean = float(os.environ.get("BCG_K_MEAN", "0")) or None
-    mech_bytes = (280.0 + 4.0 * (k_mean or 2.0)) * cells_mean
+    mech_bytes = (280.0 + 4.0 * k_mean_measured) * cells_mean
     mg_gbs = mg_bytes / (mg_ms / 1e3) / 1e9 if mg_ms > 0 else 0.0
     mech_gbs = mech_bytes / (mech_ms / 1e3) / 1e9 if mech_ms > 0 else 0.0
     roof_mg = {"kernel": "multigrid solve (Multigrid::solve, %d V-cycle)" % args.vcycles, "bound": "hbm",
@@ -903,6 +977,8 @@ def b200_arm(args):
         "colony_sweeps": colony,
         "field_update": field_update,
         "pair_geometry_fp32": pair32,
+        "mean_neighbours": k_mean_measured,
+        "dense_mechanics": dense,
         "kernel_ms_per_step": timers,
         "divisions": d_.value,
         "roofline": roof,
