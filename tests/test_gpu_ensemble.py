@@ -65,3 +65,56 @@ def test_ensemble_equals_members_run_alone(gpu):
     lib.bcg_ensemble_destroy(ens)
     for s in sims:
         lib.bcg_sim_destroy(s)
+
+
+def test_ensemble_members_match_oracle(gpu):
+    """Each member of an ensemble against its own run of the C restatement
+    (oracle/, pinned to the reference): the same seed, the same wall draws,
+    the benchmark cadence (full neighbour rebuild at the first step, one
+    1-V-cycle agar solve and one mechanics step per step).  Lineage
+    bit-exact; cells within 1e-10 relative; agar solution within 1e-12."""
+    import checkers as ck
+    from test_gpu_mechanics import assert_cells_close, rel_err
+    lib = _abi.load()
+    steps = 8
+    sims, caps, models = [], [], []
+    for name, n, seed in MEMBERS:
+        sim, n0 = make_sim(lib, name, n, seed)
+        sims.append(sim); caps.append(2 * n0)
+        p = params.workload_params(name)
+        orc = ck.Oracle(p, seed=seed)
+        orc.load(np.ascontiguousarray(workload_colony(name, n=n, seed=seed)))
+        orc.set_field(_abi.FIELDS["ENV_GROWTH1"], np.full(p.box_x * p.box_z, 0.9))
+        orc.update_density()
+        models.append((p, orc))
+    arr = (ctypes.c_void_p * len(sims))(*[s.value for s in sims])
+    ens = ctypes.c_void_p()
+    _abi.check(lib.bcg_ensemble_create(arr, len(sims), ctypes.byref(ens)), "ensemble")
+    _abi.check(lib.bcg_ensemble_run(ens, steps), "ensemble run")
+    total = 0
+    for sim, cap, (p, orc) in zip(sims, caps, models):
+        orc.rebuild()
+        t = p.t0
+        lins = []
+        for s in range(steps):
+            orc.mg_solve(1, p.mg_dt)
+            _, _, lin = orc.step(p.dt, t)
+            lins.append(lin.reshape(-1))
+            t += p.dt
+        lin_o = np.concatenate(lins) if lins else np.zeros(0, np.int32)
+        cells, lin = state(lib, sim, cap)
+        assert np.array_equal(lin, lin_o)
+        total += len(lin) // 2
+        got = np.frombuffer(cells, dtype=_abi.CELL_DTYPE)
+        assert_cells_close(orc.cells(), got)
+        ctx = lib.bcg_sim_ctx(sim)
+        for sp in ("CARBON", "OXYGEN", "ACETATE"):
+            f = "MG_SOL_" + sp
+            a = orc.field(_abi.FIELDS[f], 0)
+            b = np.zeros(a.size)
+            _abi.check(lib.bcg_get_field(ctx, _abi.FIELDS[f], 0, _abi.ptr(b, ctypes.c_double), b.size), f)
+            assert rel_err(a, b) <= 1e-12, (f, rel_err(a, b))
+    assert total > 0
+    lib.bcg_ensemble_destroy(ens)
+    for s in sims:
+        lib.bcg_sim_destroy(s)
