@@ -49,6 +49,8 @@ def parse():
                     help="skip the field update at the reference's cadence (266 solves + 200 sweeps each)")
     ap.add_argument("--smoother-warps", type=int, default=0,
                     help="pin the agar smoother's resident-warp target instead of autotuning it (profiling)")
+    ap.add_argument("--force-group", type=int, default=0,
+                    help="pin the force loop's lanes per cell instead of autotuning it (profiling)")
     return ap.parse_args()
 
 
@@ -729,6 +731,10 @@ def b200_arm(args):
             if name == "SMOOTHER" and args.smoother_warps > 0:
                 _abi.check(lib.bcg_set_smoother_warps(ctx, args.smoother_warps), "set smoother warps")
                 tuned["smoother"] = args.smoother_warps
+                continue
+            if name == "FORCE_GROUP" and args.force_group > 0:
+                _abi.check(lib.bcg_set_force_group(ctx, args.force_group), "set force group")
+                tuned["force_group"] = args.force_group
                 continue
             ch = ctypes.c_int()
             _abi.check(lib.bcg_autotune(ctx, _abi.TUNE[name], ctypes.byref(ch)), "autotune " + name)
