@@ -311,6 +311,16 @@ def sim_rebuilds(lib, sim):
     return int(r.value)
 
 
+def apply_shapes(lib, ctx, tuned):
+    """Give a new context the kernel shapes chosen for the bench colony
+    (kernel choices belong to a context)."""
+    from baccolonygrowth_b200 import _abi
+    if tuned.get("smoother", 0) > 0:
+        _abi.check(lib.bcg_set_smoother_warps(ctx, tuned["smoother"]), "set smoother warps")
+    if tuned.get("force_group", 0) > 0:
+        _abi.check(lib.bcg_set_force_group(ctx, tuned["force_group"]), "set force group")
+
+
 def mean_neighbours(lib, ctx):
     """Mean length of the reduced neighbour lists (the k of the per-pair work)."""
     import numpy as np
@@ -824,8 +834,7 @@ def b200_arm(args):
         _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(hostbuf), 0, 12345 + rank, 0, ctypes.byref(sim2)), "sim2")
         _abi.check(lib.bcg_sim_set_step_mode(sim2, 0, args.vcycles), "mode2")
         ctx2 = lib.bcg_sim_ctx(sim2)
-        if args.smoother_warps > 0:
-            _abi.check(lib.bcg_set_smoother_warps(ctx2, args.smoother_warps), "set smoother warps")
+        apply_shapes(lib, ctx2, tuned)
         g = np.full(p.box_x * p.box_z, 0.9)
         lib.bcg_set_field(ctx2, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size)
         out_pinned = torch.empty((n0 + n0 // 4) * 208, dtype=torch.uint8, pin_memory=True)
@@ -893,8 +902,7 @@ def b200_arm(args):
         _abi.check(lib.bcg_sim_create(ctypes.byref(p), _abi.ptr(hostbuf), n0, 12345 + rank, 0, ctypes.byref(sim3)), "sim3")
         _abi.check(lib.bcg_sim_set_step_mode(sim3, 0, args.vcycles), "mode3")
         ctx3 = lib.bcg_sim_ctx(sim3)
-        if args.smoother_warps > 0:
-            _abi.check(lib.bcg_set_smoother_warps(ctx3, args.smoother_warps), "set smoother warps")
+        apply_shapes(lib, ctx3, tuned)
         g = np.full(p.box_x * p.box_z, 0.9)
         lib.bcg_set_field(ctx3, _abi.FIELDS["ENV_GROWTH1"], 0, _abi.ptr(g, ctypes.c_double), g.size)
         _abi.check(lib.bcg_update_density(ctx3), "density3")
