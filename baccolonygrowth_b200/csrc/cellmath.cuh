@@ -97,7 +97,9 @@ __device__ __forceinline__ bool pair_force_at(const Cst& a, V3 acm, const Cst& b
     double L2 = b.L + 4.0 / 3 * b.R, M2 = L2 * b.R * b.R * BCG_PI;
     double Meff = M1 * M2 / (M1 + M2);
     V3 vn = scl3(sub3(c2, c1), 1.0 / d);
-    double FE_mag = sqrt(a.R * b.R / (a.R + b.R)) * mp.k_cc * pow(delta, 3.0 / 2.0);
+    /* delta^(3/2) as delta sqrt(delta) (the reference calls pow; the two
+     * differ by rounding, and the double pow is a long instruction sequence) */
+    double FE_mag = sqrt(a.R * b.R / (a.R + b.R)) * mp.k_cc * (delta * sqrt(delta));
     V3 FE = scl3(vn, -FE_mag);
     r = scl3(add3(scl3(c1, b.R), scl3(c2, a.R)), 1 / sigma);
     if (FE_mag > DBL_EPSILON) {
@@ -191,7 +193,7 @@ __device__ __forceinline__ V3 wall_locus(const Cst& c, V3 cm, V3 pole, double wa
     rpos = mk(pole.x, 0.0, wall_z);
     double d = pole.z - wall_z;
     double delta = dmax_(c.R - d, 0.0);
-    double FE_mag = sqrt(c.R) * mp.k_wc * pow(delta, 3.0 / 2.0);
+    double FE_mag = sqrt(c.R) * mp.k_wc * (delta * sqrt(delta));
     if (FE_mag > DBL_EPSILON) {
         V3 FE = mk(0.0, 0.0, FE_mag);
         V3 rcm = sub3(rpos, cm);

@@ -108,6 +108,7 @@ struct bcg_ctx {
     /* kernel shapes of this context, chosen by bcg_autotune or set by the
      * caller (0 = default); no kernel choice is process-wide */
     int force_group;
+    int force_occ;         /* blocks an SM for the force loop's register budget (3 or 4) */
     int smooth_warps;
     int relax_mode;        /* agar smoother form, bcg_set_relax_mode (3 by default) */
     size_t cluster_smem[2];/* coarsest-level cluster kernel: shared-memory size checked */
@@ -138,7 +139,7 @@ void timer_begin(bcg_ctx* c, int t);
 void timer_end(bcg_ctx* c, int t, int launches);
 int ensure_pinned(bcg_ctx* c, size_t bytes);
 void nutrient_graphs_drop(bcg_ctx* c);
-int launch_move_grow(bcg_ctx* c, double dt, int group);
+int launch_move_grow(bcg_ctx* c, double dt, int group, int occ);
 /* output-step kernels queued on `s`: the colony as reference records,
  * old_cells or (moved != 0) new_cells (ctx.cu), mean_stress's 5 stress components per cell with the F_cw count
  * added to `fcw` (mech.cu), F_surf_tension's force, 3 per cell (mech.cu) */

@@ -299,8 +299,10 @@ __device__ __forceinline__ void sum_forces_group(const Cst& a, int me, const Cel
     Fnet = F; Tnet = T;
 }
 
-template <int G, bool GEOM32>
-__global__ void __launch_bounds__(128, 4) k_move_grow(int n, int nbinned, const int* __restrict__ order,
+/* MB = the blocks of 128 threads an SM is to hold: 4 caps the registers at
+ * 128 (some spill), 3 at 170 (none spill); the autotuner picks. */
+template <int G, bool GEOM32, int MB>
+__global__ void __launch_bounds__(128, MB) k_move_grow(int n, int nbinned, const int* __restrict__ order,
         const CellRec* __restrict__ old, CellRec* __restrict__ nw,
         const int* __restrict__ nbr, const int* __restrict__ ncount,
         CellSoA soa, FieldPtrs fp, MechParams mp, double dt,
@@ -386,6 +388,7 @@ __global__ void __launch_bounds__(128, 4) k_move_grow(int n, int nbinned, const 
 /* lanes per cell in the force loop: the context's choice (bcg_autotune or
  * bcg_set_force_group), else 4 */
 static int force_group_of(const bcg_ctx* c) { return c->force_group ? c->force_group : 4; }
+static int force_occ_of(const bcg_ctx* c) { return c->force_occ ? c->force_occ : 4; }
 extern "C" int bcg_set_force_group(bcg_ctx* c, int g)
 {
     if (!c || (g != 1 && g != 2 && g != 4 && g != 8 && g != 16)) return BCG_E_ARG;
@@ -397,7 +400,7 @@ extern "C" int bcg_set_force_group(bcg_ctx* c, int g)
 /* Cells are walked in the order of the last binning (spatially coherent,
  * so neighbouring groups share record lines in L1/L2); cells created after
  * that binning follow in id order. */
-int launch_move_grow(bcg_ctx* c, double dt, int group)
+int launch_move_grow(bcg_ctx* c, double dt, int group, int occ)
 {
     int n = c->n;
     BCG_CUDA_TRY(cudaMemsetAsync(c->div_count, 0, sizeof(int), c->stream));
@@ -411,25 +414,14 @@ int launch_move_grow(bcg_ctx* c, double dt, int group)
         unsigned blocks = (unsigned)((tot + threads - 1) / threads);
         const CellRec* old = c->rec[c->cur];
         CellRec* nw = c->rec[c->cur ^ 1];
-#define MG_ARGS(G, M) k_move_grow<G, M><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, \
+#define MG_ARGS(G, M, B) k_move_grow<G, M, B><<<blocks, threads, 0, c->stream>>>(n, nb, c->box_ids, old, nw, c->nbr, c->ncount, \
             c->soa, fp, mp, dt, c->div_list, c->div_count, c->fcw_count, c->status)
-        if (c->pair_f32) {
-            switch (group) {
-            case 1: MG_ARGS(1, true); break;
-            case 2: MG_ARGS(2, true); break;
-            case 4: MG_ARGS(4, true); break;
-            case 8: MG_ARGS(8, true); break;
-            default: MG_ARGS(16, true); break;
-            }
-        } else {
-            switch (group) {
-            case 1: MG_ARGS(1, false); break;
-            case 2: MG_ARGS(2, false); break;
-            case 4: MG_ARGS(4, false); break;
-            case 8: MG_ARGS(8, false); break;
-            default: MG_ARGS(16, false); break;
-            }
-        }
+#define MG_GROUPS(M, B) switch (group) { \
+            case 1: MG_ARGS(1, M, B); break; case 2: MG_ARGS(2, M, B); break; case 4: MG_ARGS(4, M, B); break; \
+            case 8: MG_ARGS(8, M, B); break; default: MG_ARGS(16, M, B); break; }
+        if (c->pair_f32) { if (occ == 3) { MG_GROUPS(true, 3) } else { MG_GROUPS(true, 4) } }
+        else { if (occ == 3) { MG_GROUPS(false, 3) } else { MG_GROUPS(false, 4) } }
+#undef MG_GROUPS
 #undef MG_ARGS
         c->launches++;
         BCG_CUDA_TRY(cudaGetLastError());
@@ -442,7 +434,7 @@ int launch_move_grow(bcg_ctx* c, double dt, int group)
  * finish waits for them */
 int move_grow_launch(bcg_ctx* c, double dt)
 {
-    int rc = launch_move_grow(c, dt, force_group_of(c));
+    int rc = launch_move_grow(c, dt, force_group_of(c), force_occ_of(c));
     if (rc) return rc;
     int* hp = (int*)c->pinned;
     BCG_CUDA_TRY(cudaMemcpyAsync(hp, c->div_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -465,7 +457,7 @@ extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_cal
 {
     if (!c) return BCG_E_ARG;
     timer_begin(c, BCG_T_MOVE_GROW);
-    int rc = launch_move_grow(c, dt, force_group_of(c));
+    int rc = launch_move_grow(c, dt, force_group_of(c), force_occ_of(c));
     if (rc) return rc;
     timer_end(c, BCG_T_MOVE_GROW, c->n > 0 ? 1 : 0);
     /* the two counters are the only values the host needs this step */
@@ -477,14 +469,14 @@ extern "C" int bcg_move_grow(bcg_ctx* c, double dt, int* n_div, int64_t* fcw_cal
 
 /* time `reps` launches of MoveCell+GrowCell with `group` lanes per cell;
  * the records of the current buffer are read only, so the state is kept */
-static int time_move_grow(bcg_ctx* c, int group, int reps, float* ms)
+static int time_move_grow(bcg_ctx* c, int group, int occ, int reps, float* ms)
 {
     cudaEvent_t a, b;
     BCG_CUDA_TRY(cudaEventCreate(&a));
     BCG_CUDA_TRY(cudaEventCreate(&b));
-    int rc = launch_move_grow(c, c->P.dt, group);           /* warm-up */
+    int rc = launch_move_grow(c, c->P.dt, group, occ);      /* warm-up */
     if (!rc) rc = (cudaEventRecord(a, c->stream) == cudaSuccess) ? BCG_OK : BCG_E_CUDA;
-    for (int r = 0; r < reps && !rc; r++) rc = launch_move_grow(c, c->P.dt, group);
+    for (int r = 0; r < reps && !rc; r++) rc = launch_move_grow(c, c->P.dt, group, occ);
     if (!rc) rc = (cudaEventRecord(b, c->stream) == cudaSuccess) ? BCG_OK : BCG_E_CUDA;
     if (!rc) rc = (cudaEventSynchronize(b) == cudaSuccess) ? BCG_OK : BCG_E_CUDA;
     if (!rc) cudaEventElapsedTime(ms, a, b);
@@ -518,13 +510,14 @@ extern "C" int bcg_autotune(bcg_ctx* c, int what, int* choice)
         BCG_CUDA_TRY(cudaMemcpyAsync(save + a * (size_t)c->n, keep[a], nb, cudaMemcpyDeviceToDevice, c->stream));
     const int groups[5] = {1, 2, 4, 8, 16};
     float best = 3.4e38f;
-    int best_g = force_group_of(c);
+    int best_g = force_group_of(c), best_o = force_occ_of(c);
     int rc = BCG_OK;
-    for (int gi = 0; gi < 5 && !rc; gi++) {
-        float ms = 0;
-        rc = time_move_grow(c, groups[gi], 3, &ms);
-        if (!rc && ms < best) { best = ms; best_g = groups[gi]; }
-    }
+    for (int gi = 0; gi < 5 && !rc; gi++)
+        for (int occ = 3; occ <= 4 && !rc; occ++) {
+            float ms = 0;
+            rc = time_move_grow(c, groups[gi], occ, 3, &ms);
+            if (!rc && ms < best) { best = ms; best_g = groups[gi]; best_o = occ; }
+        }
     for (int a = 0; a < 7; a++)
         cudaMemcpyAsync(keep[a], save + a * (size_t)c->n, nb, cudaMemcpyDeviceToDevice, c->stream);
     cudaFreeAsync(save, c->stream);
@@ -532,7 +525,7 @@ extern "C" int bcg_autotune(bcg_ctx* c, int what, int* choice)
     c->last_ndiv = saved_ndiv;
     if (rc) return rc;
     if (rc2) return rc2;
-    if (best_g != c->force_group) { c->force_group = best_g; nutrient_graphs_drop(c); }
+    if (best_g != c->force_group || best_o != c->force_occ) { c->force_group = best_g; c->force_occ = best_o; nutrient_graphs_drop(c); }
     if (choice) *choice = best_g;
     return BCG_OK;
 }
