@@ -49,6 +49,8 @@ def parse():
                     help="skip the field update at the reference's cadence (266 solves + 200 sweeps each)")
     ap.add_argument("--smoother-warps", type=int, default=0,
                     help="pin the agar smoother's resident-warp target instead of autotuning it (profiling)")
+    ap.add_argument("--relax-mode", type=int, default=-1,
+                    help="agar smoother form (bcg_set_relax_mode; default: the library's)")
     ap.add_argument("--force-group", type=int, default=0,
                     help="pin the force loop's lanes per cell instead of autotuning it (profiling)")
     return ap.parse_args()
@@ -315,6 +317,8 @@ def apply_shapes(lib, ctx, tuned):
     """Give a new context the kernel shapes chosen for the bench colony
     (kernel choices belong to a context)."""
     from baccolonygrowth_b200 import _abi
+    if tuned.get("relax_mode", -1) >= 0:
+        _abi.check(lib.bcg_set_relax_mode(ctx, tuned["relax_mode"]), "set relax mode")
     if tuned.get("smoother", 0) > 0:
         _abi.check(lib.bcg_set_smoother_warps(ctx, tuned["smoother"]), "set smoother warps")
     if tuned.get("force_group", 0) > 0:
@@ -737,6 +741,9 @@ def b200_arm(args):
         # kernel shapes for this colony and grid (project autotuner)
         _abi.check(lib.bcg_rebuild_neighbours(ctx), "rebuild")
         tuned = {}
+        if args.relax_mode >= 0:
+            _abi.check(lib.bcg_set_relax_mode(ctx, args.relax_mode), "set relax mode")
+            tuned["relax_mode"] = args.relax_mode
         for name in ("SMOOTHER", "FORCE_GROUP"):
             if name == "SMOOTHER" and args.smoother_warps > 0:
                 _abi.check(lib.bcg_set_smoother_warps(ctx, args.smoother_warps), "set smoother warps")
