@@ -1230,7 +1230,7 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         for (int j = 0; j < sweeps; j++) relax_level<T>(c, m, l);
         return;
     }
-    if (c->relax_mode == 3) {
+    if (c->relax_mode == 3 && mg_smooth_tma_fits(c->mg[l].nx)) {
         const int warm = warm_rows(m, l);
         const int target = c->smooth_warps > 0 ? c->smooth_warps : SMOOTH_TMA_WARPS_DEFAULT;
         while (sweeps > 0) {
@@ -1321,12 +1321,13 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     const int rows = c->mg[0].nz + 1;
     if (c->relax_mode < 2 || rows <= 96) { if (choice) *choice = 0; return BCG_OK; }
     MgConst m = mg_const(c, c->P.mg_dt);
-    int targets[10];
+    int targets[20];
     int nt = 0;
     if (c->relax_mode == 3) {
+        /* every segment count from 1 to 20: the best is usually the one that
+         * fills the resident warp slots in whole waves */
         const int per_seg = mg_smooth_tma_warps_per_segment(c->mg[0].nx);
-        const int segs[10] = {1, 2, 3, 4, 5, 6, 7, 8, 12, 16};
-        for (int i = 0; i < 10; i++) targets[nt++] = per_seg * segs[i];
+        for (int i = 1; i <= 20; i++) targets[nt++] = per_seg * i;
     } else {
         const int t6[6] = {700, 1400, 2800, 5600, 8400, 11200};
         for (int i = 0; i < 6; i++) targets[nt++] = t6[i];

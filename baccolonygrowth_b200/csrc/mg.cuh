@@ -41,6 +41,8 @@ int mg_smooth_tma(bcg_ctx* c, const MgConst& m, const MgLvl& L, int l, int S, in
 int mg_smooth_tma(bcg_ctx* c, const MgConst& m, const MgLvlF& L, int l, int S, int target_warps, int warm);
 /* warps of one row segment of a level with nx + 1 columns */
 int mg_smooth_tma_warps_per_segment(int nx);
+/* whether mg_smooth_tma takes a level with nx + 1 columns */
+int mg_smooth_tma_fits(int nx);
 
 /* One of three kernel-parameter array entries by a runtime index without
  * indexing the parameter array itself (a runtime index into a parameter
