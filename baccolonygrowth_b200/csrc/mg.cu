@@ -1181,7 +1181,7 @@ static void relax_level(bcg_ctx* c, const MgConst& m, int l)
 }
 
 #define SMOOTH_WARPS_DEFAULT 1400    /* resident-warp target of k_mg_smooth before tuning */
-#define SMOOTH_TMA_WARPS_DEFAULT 888 /* warps of k_mg_smooth_tma before tuning: 6 a streaming multiprocessor */
+#define SMOOTH_TMA_WARPS_DEFAULT 0   /* warps of k_mg_smooth_tma before tuning: 0 = one per resident slot */
 
 template <class T> static void swap_err(bcg_ctx* c, int l);
 template <> void swap_err<double>(bcg_ctx* c, int l)
@@ -1236,12 +1236,8 @@ static void smooth_level(bcg_ctx* c, const MgConst& m, int l, int sweeps)
         while (sweeps > 0) {
             const int S = sweeps >= 3 ? 3 : sweeps;
             MgLvlT<T> L = lvl<T>(c, l);
-            /* segments no shorter than the warm-up (16 rows at least) */
-            const int per_seg = mg_smooth_tma_warps_per_segment(L.nx);
-            const int min_len = warm > 16 ? warm : 16;
-            const int max_seg = rows / min_len > 1 ? rows / min_len : 1;
-            const int t = target < max_seg * per_seg ? target : max_seg * per_seg;
-            const int rc = mg_smooth_tma(c, m, L, l, S, t, warm);
+            /* the launch clamps the warp count to what the level's rows allow */
+            const int rc = mg_smooth_tma(c, m, L, l, S, target, warm);
             if (rc) { c->pending_error = rc; return; }
             swap_err<T>(c, l);
             sweeps -= S;
@@ -1309,7 +1305,7 @@ int mg_kernel_attributes()
         cudaFuncSetAttribute(k_mg_smooth<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_f) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_smooth<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_f) != cudaSuccess)
         return BCG_E_CUDA;
-    return BCG_OK;
+    return mg_smooth_tma_attributes();
 }
 
 /* bcg_autotune(BCG_TUNE_SMOOTHER): time the fused smoother on the finest
@@ -1324,10 +1320,11 @@ int mg_tune_smoother(bcg_ctx* c, int* choice)
     int targets[20];
     int nt = 0;
     if (c->relax_mode == 3) {
-        /* every segment count from 1 to 20: the best is usually the one that
-         * fills the resident warp slots in whole waves */
-        const int per_seg = mg_smooth_tma_warps_per_segment(c->mg[0].nx);
-        for (int i = 1; i <= 20; i++) targets[nt++] = per_seg * i;
+        /* fractions and multiples of the resident warp slots: one warp per
+         * slot balances the SMs; fewer, longer segments save warm-up rows */
+        const int slots = mg_smooth_tma_slots();
+        const int num[9] = {1, 2, 3, 5, 1, 5, 3, 2, 3}, den[9] = {2, 3, 4, 6, 1, 4, 2, 1, 1};
+        for (int i = 0; i < 9; i++) targets[nt++] = slots > 0 ? slots * num[i] / den[i] : 0;
     } else {
         const int t6[6] = {700, 1400, 2800, 5600, 8400, 11200};
         for (int i = 0; i < 6; i++) targets[nt++] = t6[i];

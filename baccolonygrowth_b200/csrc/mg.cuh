@@ -36,11 +36,14 @@ void mg_copy_to(bcg_ctx* c, const MgConst& m, int wall_buf);
 void mg_copy_from(bcg_ctx* c, const MgConst& m, int cur_wall);
 int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf);
 /* the TMA-staged fused smoother (mg_smooth.cu): S sweeps of level L from
- * E into E2, about `target_warps` warps (row segments x strips x species) */
+ * E into E2 with about `target_warps` warps (one row segment of one strip
+ * of one species each; 0 = one per resident slot) */
 int mg_smooth_tma(bcg_ctx* c, const MgConst& m, const MgLvl& L, int l, int S, int target_warps, int warm);
 int mg_smooth_tma(bcg_ctx* c, const MgConst& m, const MgLvlF& L, int l, int S, int target_warps, int warm);
-/* warps of one row segment of a level with nx + 1 columns */
-int mg_smooth_tma_warps_per_segment(int nx);
+/* resident warps of mg_smooth_tma on the current device */
+int mg_smooth_tma_slots();
+/* kernel attributes of mg_smooth_tma (on context creation) */
+int mg_smooth_tma_attributes();
 /* whether mg_smooth_tma takes a level with nx + 1 columns */
 int mg_smooth_tma_fits(int nx);
 

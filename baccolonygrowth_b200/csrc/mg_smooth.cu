@@ -37,22 +37,31 @@
  * warp, each stage with an mbarrier that its loads complete; the copy
  * engine zero-fills columns and rows outside the level, which is the value
  * the stencil reads there.  A step reads E at row r+1 and R at row r from
- * shared memory; rows r-1, r of E and r-5 .. r of R stay in registers,
- * whose slots the loop fixes by running six steps a trip (a stage is three
- * rows, so a trip covers two stages and the ring positions repeat).
- * Results go straight to global memory (E2, the other correction buffer).
- * Every wait on an mbarrier is bounded: past about a second the warp
- * records BCG_E_TIMEOUT, waits (bounded again) for its loads still in
- * flight, and returns.
+ * shared memory.  E rows r and r+1 live in two register sets that swap
+ * roles every step, and R rows r-5 .. r in a lane-private window in shared
+ * memory (each row stored twice, six slots apart, so that every read is a
+ * fixed offset from the trip's base); the loop runs two steps a trip, a
+ * stage is two rows, so a trip opens one stage and frees one.  The small
+ * trip keeps the hot loop inside the instruction cache.  Results go
+ * straight to global memory (E2, the other correction buffer).  Every wait
+ * on an mbarrier is bounded: past about a second the warp records
+ * BCG_E_TIMEOUT, waits (bounded again) for its loads still in flight, and
+ * returns.
  *
  * Boundaries: interior points of interior rows take rx_in.  The side
  * columns (0 and nx), row 0 and row nz take the other cases of relax_val
  * through one branch-free form (ts_point) with per-column flags; a point
- * that keeps its value before smoothing finds it in its R register slot,
- * where the row's load put E instead of R.  Steps whose rows are all
- * interior and inside the segment run without any per-step check; a warp
- * stores at most one side column, whose slot within the lane's four is a
- * template parameter, so only that slot pays for the general form.
+ * that keeps its value before smoothing finds it in its R slot, where the
+ * row's load put E instead of R.  Steps whose rows are all interior and
+ * inside the segment's relaxed range check only whether their finished row
+ * is stored; a warp stores at most one side column, whose slot within the
+ * lane's four is a template parameter, so only that slot pays for the
+ * general form.
+ *
+ * Work split: W warps (by default one per resident slot, so that every SM
+ * carries the same load) over the 3 x strips columns of the level, each
+ * column cut into segments of equal cost (the first segment has no
+ * warm-up rows and runs that many more rows of its own).
  */
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -61,7 +70,7 @@
 #include "mg.cuh"
 
 #define TS_COLS 128          /* columns a warp loads */
-#define TS_NR 3              /* rows per stage */
+#define TS_NR 2              /* rows per stage */
 #define TS_NS 3              /* stages per warp */
 #define TS_WARPS 2           /* warps per block, each with its own strip and ring */
 #define TS_WAIT_CYCLES (2000000000LL)   /* about one second at 2 GHz */
@@ -76,8 +85,13 @@ struct TsMaps { CUtensorMap e[3], r[3]; };
 /* one stage: NR rows of E, then NR rows of R, TS_COLS values each */
 template <class T> constexpr int ts_stage_elems() { return 2 * TS_NR * TS_COLS; }
 template <class T> constexpr int ts_stage_bytes() { return ts_stage_elems<T>() * (int)sizeof(T); }
-template <class T> constexpr int ts_ring_elems() { return TS_NS * ts_stage_elems<T>(); }
-template <class T> constexpr int ts_smem_bytes() { return TS_WARPS * (TS_NS * ts_stage_bytes<T>() + 8 * TS_NS); }
+/* the R window: 12 slots of [parity][lane] pairs (the lane's even
+ * columns, then its odd ones) */
+constexpr int ts_wslot_elems() { return 2 * 32; }
+template <class T> constexpr int ts_win_bytes() { return 12 * ts_wslot_elems() * 2 * (int)sizeof(T); }
+/* per warp: its ring, then its R window; after the warps', their mbarriers */
+template <class T> constexpr int ts_warp_bytes() { return TS_NS * ts_stage_bytes<T>() + ts_win_bytes<T>(); }
+template <class T> constexpr int ts_smem_bytes() { return TS_WARPS * (ts_warp_bytes<T>() + 8 * TS_NS); }
 
 /* ---- mbarrier and TMA primitives ---------------------------------------- */
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -112,17 +126,25 @@ __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map
                  :: "r"(dst), "l"(map), "r"(x), "r"(y), "r"(bar) : "memory");
 }
 
-/* 4 consecutive values of a row in shared memory (this lane's columns) */
-__device__ __forceinline__ void lds4(const double* p, double (&v)[4])
+/* this lane's 4 values at byte offset OFF from a shared-space address.
+ * Volatile, so that the loads stay after the mbarrier wait that covers
+ * them and before the proxy fence that hands their slot back to the copy
+ * engine. */
+template <int OFF>
+__device__ __forceinline__ void ts_lds(unsigned a, double (&v)[4])
 {
-    double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%4+%5];\n\tld.shared.v2.f64 {%2, %3}, [%4+%6];"
+                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "r"(a), "n"(OFF), "n"(OFF + 16));
 }
-__device__ __forceinline__ void lds4(const float* p, float (&v)[4])
+template <int OFF>
+__device__ __forceinline__ void ts_lds(unsigned a, float (&v)[4])
 {
-    float4 a = *reinterpret_cast<const float4*>(p);
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4+%5];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "r"(a), "n"(OFF));
 }
+template <class T> struct Pair;
+template <> struct Pair<double> { typedef double2 t; };
+template <> struct Pair<float> { typedef float2 t; };
 
 /* per-warp state that does not change along the rows */
 struct TsArgs {
@@ -133,7 +155,7 @@ struct TsArgs {
     int nstage;             /* stages this warp loads */
     unsigned fl;            /* ts_col_flags of the lane's 4 columns, 8 bits each */
     unsigned sub;           /* keep-old bits of the lane's columns, 3 each (row types) */
-    bool st[4];             /* the lane stores that column */
+    unsigned stm;           /* bit j: the lane stores its column j */
 };
 
 /* Row types of the update: interior rows, row 0, row nz. */
@@ -203,12 +225,13 @@ __device__ __forceinline__ T ts_point(int rt, unsigned f, bool s1p, T slot, T b,
 
 /* issue the loads of stage j (rows r0 + j NR ...) into slot j mod NS (lane 0) */
 template <class T>
-__device__ __forceinline__ void ts_issue(const TsMaps& maps, const TsArgs& g, T* ring, unsigned bar0, int j, int& issued)
+__device__ __forceinline__ void ts_issue(const TsMaps& maps, const TsArgs& g, unsigned ring_s, unsigned bar0, int j,
+                                         int& issued)
 {
     issued = j + 1;
     const int slot = j % TS_NS;
     const unsigned bar = bar0 + 8u * slot;
-    const unsigned dst = smem_u32(ring + (size_t)slot * ts_stage_elems<T>());
+    const unsigned dst = ring_s + (unsigned)(slot * ts_stage_bytes<T>());
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(bar, (unsigned)ts_stage_bytes<T>());
     const int y = g.r0 + j * TS_NR;
@@ -218,60 +241,63 @@ __device__ __forceinline__ void ts_issue(const TsMaps& maps, const TsArgs& g, T*
     tma_load_2d(dst + ts_stage_bytes<T>() / 2, mr, g.c0, y, bar);
 }
 
-/* Ring pointers of one trip of six row steps (trip t: rows kw + 6t ..,
- * staged rows 6t .. 6t + 8 counted from r0): the slots of stages 2t,
- * 2t+1 and 2t+2.  The next trip's are those of 2t+2, 2t+3 = 2t (mod 3)
- * and 2t+4 = 2t+1 (mod 3). */
+/* The shared-memory rows a trip reads.  Trip t (steps r = kw + 2t + P, P
+ * = 0, 1) reads E rows r+1 and R rows r, staged rows 2t+1 .. 2t+3 counted
+ * from r0: stage t (slot t mod NS) and stage t+1.  The R window keeps rows
+ * r-5 .. r: row q in slots (q - kw) mod 6 and (q - kw) mod 6 + 6, so that
+ * at step r row r-h sits h slots below slot (r - kw) mod 6 + 6, a fixed
+ * offset from the trip's window base. */
 template <class T>
 struct TsTrip {
-    const T* p[3];
+    unsigned cur, nxt;          /* shared-space address of this lane's columns in the slots of stages t, t+1 */
+    typename Pair<T>::t* win;   /* this lane's entry of window slot (2t) mod 6 */
     int t;
 };
-/* shared-memory row q (0..8 within the trip's stages) of E or R, at this
- * lane's columns */
 template <class T>
-__device__ __forceinline__ const T* ts_row(const TsTrip<T>& tr, int q, bool is_r)
+__device__ __forceinline__ void ts_trip(TsTrip<T>& tr, unsigned lane_ring, typename Pair<T>::t* lane_win, int t)
 {
-    return tr.p[q / TS_NR] + (is_r ? TS_NR * TS_COLS : 0) + (q % TS_NR) * TS_COLS + 4 * (threadIdx.x & 31);
+    tr.t = t;
+    tr.cur = lane_ring + (unsigned)((t % TS_NS) * ts_stage_bytes<T>());
+    tr.nxt = lane_ring + (unsigned)(((t + 1) % TS_NS) * ts_stage_bytes<T>());
+    tr.win = lane_win + ((2 * t) % 6) * ts_wslot_elems();
 }
 
-/* One row step at phase P = (r - kw) mod 6 (fixes the register slots and
- * the ring rows).  h1 = results of step r-1 (read only), h2 = results of
- * step r-2 on entry and of step r on exit; Ew[q mod 3] = E row q for q =
- * r-1, r, r+1 (row r+1 loaded here); Rs[(q - kw + 1) mod 6] = R row q for
- * q = r-5 .. r (row r loaded here).  Returns false after a timed-out wait
- * (recorded in the status word). */
+/* One row step, P = (r - kw) mod 2.  h1 = results of step r-1 (read only),
+ * h2 = results of step r-2 on entry and of step r on exit; e0 = E row r,
+ * ep = E row r+1 (loaded here; it held row r-1).  Returns false after a
+ * timed-out wait (recorded in the status word). */
 template <class T, int S, int SIDE, int P, bool CHECK>
-__device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTrip<T>& tr, T* ring, unsigned bar0,
-                                        const TsMaps& maps, int& issued, T (&h1)[2 * S][2], T (&h2)[2 * S][2], T (&Ew)[3][4],
-                                        T (&Rs)[6][4], T* __restrict__ EO, const RelaxK<T>& K, DevStatus* st)
+__device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTrip<T>& tr, unsigned ring_s,
+                                        unsigned bar0, const TsMaps& maps, int& issued, T (&h1)[2 * S][2],
+                                        T (&h2)[2 * S][2], const T (&e0)[4], T (&ep)[4], T* __restrict__ EO,
+                                        long long& orow, const RelaxK<T>& K, DevStatus* st)
 {
     constexpr int H = 2 * S;
+    typedef typename Pair<T>::t T2;
+    constexpr int RB = TS_NR * TS_COLS * (int)sizeof(T);    /* R box offset in a stage */
+    constexpr int RW = TS_COLS * (int)sizeof(T);            /* one staged row */
     const int lane = threadIdx.x & 31;
-    /* E row r+1 is ring row 2+P of the trip, R row r ring row 1+P; stage
-     * 2t+1 opens at P = 1 (E row 3), stage 2t+2 at P = 4 (E row 6) */
-    if (P == 1 || P == 4) {
-        const int j = 2 * tr.t + (P == 1 ? 1 : 2);
+    if (P == 0) {
+        /* E row r+1 opens stage t+1 */
+        const int j = tr.t + 1;
         if (j < g.nstage) {
-            const int slot = j % TS_NS;
-            const bool ok = mbar_wait(bar0 + 8u * slot, (unsigned)((j / TS_NS) & 1));
+            const bool ok = mbar_wait(bar0 + 8u * (j % TS_NS), (unsigned)((j / TS_NS) & 1));
             if (!__all_sync(0xffffffffu, ok)) {
                 if (lane == 0) dev_error(st, BCG_E_TIMEOUT, 0x5300 + g.sp);
                 return false;
             }
         }
-    }
-    /* stage 2t was last read at P = 1 (R row 2), stage 2t+1 at P = 4 (R
-     * row 5): their slots take stages 2t+3 and 2t+4 */
-    if (P == 2 || P == 5) {
-        const int j = 2 * tr.t + (P == 2 ? 3 : 4);
+    } else {
+        /* stage t was last read at P = 0 (R row 2t+1): its slot takes
+         * stage t + NS */
+        const int j = tr.t + TS_NS;
         __syncwarp();
-        if (lane == 0 && j < g.nstage) ts_issue<T>(maps, g, ring, bar0, j, issued);
+        if (lane == 0 && j < g.nstage) ts_issue<T>(maps, g, ring_s, bar0, j, issued);
     }
-    lds4(ts_row<T>(tr, 2 + P, false), Ew[(2 + P) % 3]);
-    lds4(ts_row<T>(tr, 1 + P, true), Rs[(1 + P) % 6]);
-    const T (&e0)[4] = Ew[(1 + P) % 3];     /* row r */
-    const T (&ep)[4] = Ew[(2 + P) % 3];     /* row r+1 */
+    T rr[4];
+    ts_lds<P * RW>(tr.nxt, ep);                              /* E row r+1: stage t+1, row P */
+    if (P == 0) ts_lds<RB + RW>(tr.cur, rr);                 /* R row r: stage t, row 1 */
+    else ts_lds<RB>(tr.nxt, rr);                             /*          stage t+1, row 0 */
     {
         /* a point that keeps its value before smoothing gets that value in
          * its R slot, which is what ts_point keeps (on interior rows only
@@ -279,7 +305,12 @@ __device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTr
         const int rt = !CHECK ? TS_ROW_IN : (r == 0 ? TS_ROW_BOT : (r == g.nz ? TS_ROW_TOP : TS_ROW_IN));
 #pragma unroll
         for (int j = 0; j < 4; j++)
-            if ((CHECK || j == SIDE) && ((g.sub >> (3 * j + rt)) & 1u)) Rs[(1 + P) % 6][j] = e0[j];
+            if ((CHECK || j == SIDE) && ((g.sub >> (3 * j + rt)) & 1u)) rr[j] = e0[j];
+        T2 ev, od;
+        ev.x = rr[0]; ev.y = rr[2]; od.x = rr[1]; od.y = rr[3];
+        T2* w = tr.win + P * ts_wslot_elems();
+        w[0] = ev; w[32] = od;
+        w[6 * ts_wslot_elems()] = ev; w[6 * ts_wslot_elems() + 32] = od;
     }
     /* neighbours from other lanes: even half h reads the left lane's last
      * odd column, odd half h the right lane's first even column */
@@ -294,8 +325,11 @@ __device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTr
     const bool inner = !CHECK || (lo > 0 && r < g.nz);
 #pragma unroll
     for (int h = H - 1; h >= 0; h--) {
-        const T (&rk)[4] = Rs[(1 + P - h + 6) % 6];
         const int j0 = h & 1;
+        /* R of row r-h at this half's columns */
+        T2 rk;
+        if (h == 0) { rk.x = rr[0]; rk.y = rr[2]; }
+        else rk = tr.win[(P + 6 - h) * ts_wslot_elems() + 32 * j0];
         T x0m, x0p, x1m, x1p, u0v, u1v;
         if (j0) {
             x0m = h1[h - 1][0]; x0p = h1[h - 1][1]; x1m = h1[h - 1][1]; x1p = nb[h];
@@ -312,16 +346,16 @@ __device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTr
             /* interior rows: the plain form, except in the column slot that
              * holds the warp's side column (flags 0 give the plain form's
              * operations there too) */
-            h2[h][0] = SIDE == c0 ? ts_point<T>(TS_ROW_IN, (g.fl >> (8 * c0)) & 3u, (g.fl >> (8 * c0 + 6)) & 1u, rk[c0],
+            h2[h][0] = SIDE == c0 ? ts_point<T>(TS_ROW_IN, (g.fl >> (8 * c0)) & 3u, (g.fl >> (8 * c0 + 6)) & 1u, rk.x,
                                                 h1[h][0], u0v, x0m, x0p, K)
-                                  : rx_in(rk[c0], h1[h][0], u0v, x0m, x0p, K);
-            h2[h][1] = SIDE == c1 ? ts_point<T>(TS_ROW_IN, (g.fl >> (8 * c1)) & 3u, (g.fl >> (8 * c1 + 6)) & 1u, rk[c1],
+                                  : rx_in(rk.x, h1[h][0], u0v, x0m, x0p, K);
+            h2[h][1] = SIDE == c1 ? ts_point<T>(TS_ROW_IN, (g.fl >> (8 * c1)) & 3u, (g.fl >> (8 * c1 + 6)) & 1u, rk.y,
                                                 h1[h][1], u1v, x1m, x1p, K)
-                                  : rx_in(rk[c1], h1[h][1], u1v, x1m, x1p, K);
+                                  : rx_in(rk.y, h1[h][1], u1v, x1m, x1p, K);
         } else {
-            h2[h][0] = ts_point<T>(rt, (g.fl >> (8 * c0 + 2 * rt)) & 3u, (g.fl >> (8 * c0 + 6)) & 1u, rk[c0], h1[h][0],
+            h2[h][0] = ts_point<T>(rt, (g.fl >> (8 * c0 + 2 * rt)) & 3u, (g.fl >> (8 * c0 + 6)) & 1u, rk.x, h1[h][0],
                                    u0v, x0m, x0p, K);
-            h2[h][1] = ts_point<T>(rt, (g.fl >> (8 * c1 + 2 * rt)) & 3u, (g.fl >> (8 * c1 + 6)) & 1u, rk[c1], h1[h][1],
+            h2[h][1] = ts_point<T>(rt, (g.fl >> (8 * c1 + 2 * rt)) & 3u, (g.fl >> (8 * c1 + 6)) & 1u, rk.y, h1[h][1],
                                    u1v, x1m, x1p, K);
         }
     }
@@ -338,111 +372,129 @@ __device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTr
     /* row r - (H-1) is final: even columns from the last even half one step
      * ago, odd columns from the last odd half now */
     const int kS = r - (H - 1);
-    if (!CHECK || (kS >= g.ks && kS < g.ke)) {
-        T* dst = EO + (size_t)kS * g.pitch + g.col;
+    if (kS >= g.ks && (!CHECK || kS < g.ke)) {
+        T* dst = EO + orow;
         const T v[4] = {h1[H - 2][0], h2[H - 1][0], h1[H - 2][1], h2[H - 1][1]};
-        if (g.st[0] && g.st[3]) {
+        if (SIDE < 0) {
+            /* a strip without a side column stores whole pairs (FP64) or a
+             * whole group of four (FP32): its stored range starts on a pair
+             * (group) boundary and ends inside the level */
             if (sizeof(T) == 8) {
                 double2* d2 = reinterpret_cast<double2*>(dst);
-                d2[0] = make_double2((double)v[0], (double)v[1]);
-                d2[1] = make_double2((double)v[2], (double)v[3]);
-            } else {
+                if (g.stm & 1u) d2[0] = make_double2((double)v[0], (double)v[1]);
+                if (g.stm & 4u) d2[1] = make_double2((double)v[2], (double)v[3]);
+            } else if (g.stm & 1u) {
                 *reinterpret_cast<float4*>(dst) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
             }
         } else {
 #pragma unroll
             for (int j = 0; j < 4; j++)
-                if (g.st[j]) dst[j] = v[j];
+                if ((g.stm >> j) & 1u) dst[j] = v[j];
         }
     }
+    orow += g.pitch;
     return true;
 }
 
-/* the row loop, six steps a trip (the phases fix every register slot) */
+/* the row loop, two steps a trip (E rows and the half-sweep results
+ * alternate between two register sets) */
 template <class T, int S, int SIDE>
-__device__ __forceinline__ bool ts_rows(const TsArgs& g, T* ring, unsigned bar0, const TsMaps& maps, int& issued, T (&Ew)[3][4],
-                                        T* __restrict__ EO, const RelaxK<T>& K, DevStatus* st)
+__device__ __forceinline__ bool ts_rows(const TsArgs& g, unsigned ring_s, typename Pair<T>::t* lane_win, unsigned bar0,
+                                        const TsMaps& maps, int& issued, T (&EA)[4], T* __restrict__ EO,
+                                        const RelaxK<T>& K, DevStatus* st)
 {
     constexpr int H = 2 * S;
     const int r_end = g.ke - 1 + (H - 1);
-    T Rs[6][4];
-#pragma unroll
-    for (int q = 0; q < 6; q++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) Rs[q][j] = T(0);
+    const unsigned lane_ring = ring_s + 4 * sizeof(T) * (threadIdx.x & 31);
+    T EB[4];
     T a[H][2], b[H][2];
+    {
+        /* the half-sweeps start from row kw-1 (stage 0, row 0) */
+        T e[4];
+        ts_lds<0>(lane_ring, e);
 #pragma unroll
-    for (int h = 0; h < H; h++) {
-        a[h][0] = b[h][0] = Ew[0][(h & 1)];
-        a[h][1] = b[h][1] = Ew[0][(h & 1) + 2];
-    }
-    TsTrip<T> tr;
-    tr.t = 0;
-    tr.p[0] = ring;
-    tr.p[1] = ring + ts_stage_elems<T>();
-    tr.p[2] = ring + 2 * ts_stage_elems<T>();
-    /* steps r >= st_lo have rows r-H+1 .. r at or above the warm start, the
-     * first stored row and row 1; steps r <= st_hi at or below the last
-     * stored row and row nz-1: such steps need no checks */
-    const int st_lo = max(max(g.kw, g.ks), 1) + (H - 1);
-    const int st_hi = min(g.ke - 1, g.nz - 1);
-    for (int r = g.kw; r <= r_end; r += 6) {
-        if (r >= st_lo && r + 5 <= st_hi) {
-            if (!ts_step<T, S, SIDE, 0, false>(r, g, tr, ring, bar0, maps, issued, a, b, Ew, Rs, EO, K, st)) return false;
-            if (!ts_step<T, S, SIDE, 1, false>(r + 1, g, tr, ring, bar0, maps, issued, b, a, Ew, Rs, EO, K, st)) return false;
-            if (!ts_step<T, S, SIDE, 2, false>(r + 2, g, tr, ring, bar0, maps, issued, a, b, Ew, Rs, EO, K, st)) return false;
-            if (!ts_step<T, S, SIDE, 3, false>(r + 3, g, tr, ring, bar0, maps, issued, b, a, Ew, Rs, EO, K, st)) return false;
-            if (!ts_step<T, S, SIDE, 4, false>(r + 4, g, tr, ring, bar0, maps, issued, a, b, Ew, Rs, EO, K, st)) return false;
-            if (!ts_step<T, S, SIDE, 5, false>(r + 5, g, tr, ring, bar0, maps, issued, b, a, Ew, Rs, EO, K, st)) return false;
-        } else {
-            if (!ts_step<T, S, SIDE, 0, true>(r, g, tr, ring, bar0, maps, issued, a, b, Ew, Rs, EO, K, st)) return false;
-            if (r + 1 > r_end) break;
-            if (!ts_step<T, S, SIDE, 1, true>(r + 1, g, tr, ring, bar0, maps, issued, b, a, Ew, Rs, EO, K, st)) return false;
-            if (r + 2 > r_end) break;
-            if (!ts_step<T, S, SIDE, 2, true>(r + 2, g, tr, ring, bar0, maps, issued, a, b, Ew, Rs, EO, K, st)) return false;
-            if (r + 3 > r_end) break;
-            if (!ts_step<T, S, SIDE, 3, true>(r + 3, g, tr, ring, bar0, maps, issued, b, a, Ew, Rs, EO, K, st)) return false;
-            if (r + 4 > r_end) break;
-            if (!ts_step<T, S, SIDE, 4, true>(r + 4, g, tr, ring, bar0, maps, issued, a, b, Ew, Rs, EO, K, st)) return false;
-            if (r + 5 > r_end) break;
-            if (!ts_step<T, S, SIDE, 5, true>(r + 5, g, tr, ring, bar0, maps, issued, b, a, Ew, Rs, EO, K, st)) return false;
+        for (int h = 0; h < H; h++) {
+            a[h][0] = b[h][0] = e[(h & 1)];
+            a[h][1] = b[h][1] = e[(h & 1) + 2];
         }
-        const T* q0 = tr.p[0];
-        tr.p[0] = tr.p[2];
-        tr.p[2] = tr.p[1];
-        tr.p[1] = q0;
-        tr.t++;
+#pragma unroll
+        for (int q = 0; q < 4; q++) EB[q] = e[q];
+    }
+    /* offset of the lane's columns in row r - (H-1), the row a step finishes */
+    long long orow = (long long)(g.kw - (H - 1)) * g.pitch + g.col;
+    TsTrip<T> tr;
+    ts_trip<T>(tr, lane_ring, lane_win, 0);
+    /* steps r >= st_lo have rows r-H+1 .. r at or above the warm start and
+     * row 1; steps r <= st_hi at or below the last stored row and row nz-1:
+     * such steps check only whether their finished row is stored (not in
+     * the warm-up rows), so that the few checked trips of a segment are
+     * all that leave the trip the warp spends its time in */
+    const int st_lo = max(g.kw, 1) + (H - 1);
+    const int st_hi = min(g.ke - 1, g.nz - 1);
+    for (int r = g.kw; r <= r_end; r += 2) {
+        if (r >= st_lo && r + 1 <= st_hi) {
+            if (!ts_step<T, S, SIDE, 0, false>(r, g, tr, ring_s, bar0, maps, issued, a, b, EA, EB, EO, orow, K, st)) return false;
+            if (!ts_step<T, S, SIDE, 1, false>(r + 1, g, tr, ring_s, bar0, maps, issued, b, a, EB, EA, EO, orow, K, st)) return false;
+        } else {
+            if (!ts_step<T, S, SIDE, 0, true>(r, g, tr, ring_s, bar0, maps, issued, a, b, EA, EB, EO, orow, K, st)) return false;
+            if (r + 1 > r_end) break;
+            if (!ts_step<T, S, SIDE, 1, true>(r + 1, g, tr, ring_s, bar0, maps, issued, b, a, EB, EA, EO, orow, K, st)) return false;
+        }
+        ts_trip<T>(tr, lane_ring, lane_win, tr.t + 1);
     }
     return true;
 }
 
-/* Four blocks (eight warps) an SM: the row step's twelve independent
- * updates need about 220 registers a thread to be scheduled side by side;
- * capping them at 168 for a third warp per scheduler spills and measured
- * slower (0.152-0.166 ms against 0.123 ms per level-0 launch of the
- * 4609 x 1025 grid). */
+/* How a launch cuts the level: W warps over C = 3 x strips columns (a
+ * strip of one species), the first `extra` columns in base+1 row segments,
+ * the others in base.  The segments of a column cost the same: the first
+ * runs `chunk` rows, the others chunk - warm rows after their warm rows. */
+struct TsPlan { int W, nstrips, base, extra, warm, rows; };
+
+/* warp gw's strip, species and stored rows ks .. ke-1; false: no rows */
+__device__ __forceinline__ bool ts_assign(int gw, const TsPlan& pl, int& strip, int& sp, int& ks, int& ke)
+{
+    if (gw >= pl.W) return false;
+    int c, s, n;
+    const int big = pl.extra * (pl.base + 1);
+    if (gw < big) {
+        n = pl.base + 1; c = gw / n; s = gw - c * n;
+    } else {
+        n = pl.base;
+        const int q = gw - big;
+        c = pl.extra + q / n; s = q - (c - pl.extra) * n;
+    }
+    sp = c / pl.nstrips;
+    strip = c - sp * pl.nstrips;
+    const int chunk = (pl.rows + (n - 1) * pl.warm + n - 1) / n;
+    ks = s == 0 ? 0 : chunk + (s - 1) * (chunk - pl.warm);
+    ke = min(ks + (s == 0 ? chunk : chunk - pl.warm), pl.rows);
+    return ks < pl.rows;
+}
+
+/* Four blocks (eight warps) an SM; the shared memory of a block (two rings
+ * and two R windows) allows no more. */
 template <class T, int S>
 __global__ void __launch_bounds__(32 * TS_WARPS, 4) k_mg_smooth_tma(const __grid_constant__ TsMaps maps, const __grid_constant__ MgConst m,
-                                                      const __grid_constant__ MgLvlT<T> L, int l, int seg_len, int warm,
+                                                      const __grid_constant__ MgLvlT<T> L, int l, TsPlan pl,
                                                       const double* __restrict__ inside0, DevStatus* st)
 {
     constexpr int H = 2 * S;
     extern __shared__ __align__(128) unsigned char ts_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int strip = (int)blockIdx.x * TS_WARPS + warp;
     TsArgs g;
-    g.nx = L.nx; g.nz = L.nz; g.pitch = L.pitch; g.l = l; g.sp = blockIdx.z;
+    int strip, sp;
+    if (!ts_assign((int)blockIdx.x * TS_WARPS + warp, pl, strip, sp, g.ks, g.ke)) return;    /* whole warp (no block-wide barrier follows) */
+    g.nx = L.nx; g.nz = L.nz; g.pitch = L.pitch; g.l = l; g.sp = sp;
     g.c0 = strip * TsGeom<T>::WV - TsGeom<T>::HL;
     g.col = g.c0 + 4 * lane;
-    g.ks = (int)blockIdx.y * seg_len;
-    if (g.ks > g.nz || strip * TsGeom<T>::WV > g.nx) return;     /* whole warp (no block-wide barrier follows) */
-    g.ke = min(g.ks + seg_len, g.nz + 1);
-    g.kw = max(0, g.ks - warm);
+    g.kw = max(0, g.ks - pl.warm);
     g.r0 = g.kw - 1;
     const int r_end = g.ke - 1 + (H - 1);
     /* rows r0 .. r_end + 1 */
     g.nstage = (r_end + 1 - g.r0) / TS_NR + 1;
     int side_slot = -1;
+    g.stm = 0;
     g.fl = 0;
     g.sub = 0;
 #pragma unroll
@@ -451,18 +503,21 @@ __global__ void __launch_bounds__(32 * TS_WARPS, 4) k_mg_smooth_tma(const __grid
         unsigned sb;
         g.fl |= ts_col_flags(m, i, g.nx, l, g.sp, inside0, &sb) << (8 * j);
         g.sub |= sb << (3 * j);
-        g.st[j] = i >= g.c0 + TsGeom<T>::HL && i < g.c0 + TsGeom<T>::HL + TsGeom<T>::WV && i >= 0 && i <= g.nx;
+        const bool st = i >= g.c0 + TsGeom<T>::HL && i < g.c0 + TsGeom<T>::HL + TsGeom<T>::WV && i >= 0 && i <= g.nx;
+        g.stm |= (unsigned)st << j;
         /* a side column in the strip's halo is in the columns that go
          * stale anyway: only a stored one needs its own form */
-        if (g.st[j] && (i == 0 || i == g.nx)) side_slot = j;
+        if (st && (i == 0 || i == g.nx)) side_slot = j;
     }
     /* the column slot of the warp's side column, -1 if it stores none (the
      * host gives this kernel only levels whose two sides are in different
      * strips) */
     side_slot = __reduce_max_sync(0xffffffffu, side_slot);
-    /* the rings of the block's warps, then their mbarriers */
-    T* ring = reinterpret_cast<T*>(ts_smem) + (size_t)warp * ts_ring_elems<T>();
-    const unsigned bar0 = smem_u32(ts_smem + TS_WARPS * TS_NS * ts_stage_bytes<T>() + 8 * TS_NS * warp);
+    /* the warps' rings and R windows, then their mbarriers */
+    unsigned char* wbase = ts_smem + (size_t)warp * ts_warp_bytes<T>();
+    const unsigned ring_s = smem_u32(wbase);
+    typename Pair<T>::t* lane_win = reinterpret_cast<typename Pair<T>::t*>(wbase + TS_NS * ts_stage_bytes<T>()) + lane;
+    const unsigned bar0 = smem_u32(ts_smem + TS_WARPS * ts_warp_bytes<T>() + 8 * TS_NS * warp);
     if (lane == 0) {
         for (int s = 0; s < TS_NS; s++) mbar_init(bar0 + 8u * s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -470,7 +525,7 @@ __global__ void __launch_bounds__(32 * TS_WARPS, 4) k_mg_smooth_tma(const __grid
     __syncwarp();
     int issued = 0;             /* stages issued so far (kept by lane 0) */
     if (lane == 0)
-        for (int j = 0; j < TS_NS && j < g.nstage; j++) ts_issue<T>(maps, g, ring, bar0, j, issued);
+        for (int j = 0; j < TS_NS && j < g.nstage; j++) ts_issue<T>(maps, g, ring_s, bar0, j, issued);
     /* rows kw-1 and kw (stage 0) into registers */
     bool ok = __all_sync(0xffffffffu, mbar_wait(bar0, 0));
     if (!ok) {
@@ -478,17 +533,15 @@ __global__ void __launch_bounds__(32 * TS_WARPS, 4) k_mg_smooth_tma(const __grid
     } else {
         const RelaxK<T> K = relax_k<T>(m, l, g.sp);
         T* __restrict__ EO = g.sp == 0 ? L.e2[0] : (g.sp == 1 ? L.e2[1] : L.e2[2]);
-        T Ew[3][4];
-        lds4(ring + 4 * lane, Ew[0]);
-        lds4(ring + TS_COLS + 4 * lane, Ew[1]);
-#pragma unroll
-        for (int q = 0; q < 4; q++) Ew[2][q] = T(0);
+        /* E row kw: stage 0, row 1 */
+        T EA[4];
+        ts_lds<TS_COLS * (int)sizeof(T)>(ring_s + 4 * sizeof(T) * lane, EA);
         switch (side_slot) {
-        case 0: ok = ts_rows<T, S, 0>(g, ring, bar0, maps, issued, Ew, EO, K, st); break;
-        case 1: ok = ts_rows<T, S, 1>(g, ring, bar0, maps, issued, Ew, EO, K, st); break;
-        case 2: ok = ts_rows<T, S, 2>(g, ring, bar0, maps, issued, Ew, EO, K, st); break;
-        case 3: ok = ts_rows<T, S, 3>(g, ring, bar0, maps, issued, Ew, EO, K, st); break;
-        default: ok = ts_rows<T, S, -1>(g, ring, bar0, maps, issued, Ew, EO, K, st); break;
+        case 0: ok = ts_rows<T, S, 0>(g, ring_s, lane_win, bar0, maps, issued, EA, EO, K, st); break;
+        case 1: ok = ts_rows<T, S, 1>(g, ring_s, lane_win, bar0, maps, issued, EA, EO, K, st); break;
+        case 2: ok = ts_rows<T, S, 2>(g, ring_s, lane_win, bar0, maps, issued, EA, EO, K, st); break;
+        case 3: ok = ts_rows<T, S, 3>(g, ring_s, lane_win, bar0, maps, issued, EA, EO, K, st); break;
+        default: ok = ts_rows<T, S, -1>(g, ring_s, lane_win, bar0, maps, issued, EA, EO, K, st); break;
         }
     }
     /* every issued stage must have landed before the block's shared memory
@@ -546,12 +599,32 @@ static int ts_encode(CUtensorMap* map, const T* base, int nx, int nz, int pitch)
 
 /* strips of a level (one warp each per segment and species) */
 template <class T> static int ts_strips(int nx) { return (nx + 1 + TsGeom<T>::WV - 1) / TsGeom<T>::WV; }
-template <class T> static int ts_blocks_x(int nx) { return (ts_strips<T>(nx) + TS_WARPS - 1) / TS_WARPS; }
 
-/* S (1..3) fused sweeps of level L: E -> E2, the level cut into `nseg` row
- * segments that start `warm` rows early */
+/* resident warps of the kernel on the current device (blocks an SM x SMs
+ * x warps a block); looked up once per device and precision */
 template <class T>
-static int ts_launch(bcg_ctx* c, const MgConst& m, const MgLvlT<T>& L, int l, int S, int nseg, int warm)
+static int ts_slots()
+{
+    static int slots[2][64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return 0; }
+    int& v = slots[sizeof(T) == 8][dev];
+    if (v == 0) {
+        int sms = 0, nb = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mg_smooth_tma<T, 3>, 32 * TS_WARPS, ts_smem_bytes<T>()) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        v = sms * nb * TS_WARPS;
+    }
+    return v;
+}
+
+/* S (1..3) fused sweeps of level L: E -> E2 with about W warps (0: one per
+ * resident slot), segments starting `warm` rows early */
+template <class T>
+static int ts_launch(bcg_ctx* c, const MgConst& m, const MgLvlT<T>& L, int l, int S, int W, int warm)
 {
     TsMaps maps;
     memset(&maps, 0, sizeof(maps));
@@ -560,17 +633,32 @@ static int ts_launch(bcg_ctx* c, const MgConst& m, const MgLvlT<T>& L, int l, in
         if (!rc) rc = ts_encode<T>(&maps.r[sp], L.r[sp], L.nx, L.nz, L.pitch);
         if (rc) return rc;
     }
-    const int rows = L.nz + 1;
-    if (nseg < 1) nseg = 1;
-    if (nseg > rows) nseg = rows;
-    const int seg_len = (rows + nseg - 1) / nseg;
-    nseg = (rows + seg_len - 1) / seg_len;
-    dim3 grid((unsigned)ts_blocks_x<T>(L.nx), (unsigned)nseg, 3);
+    TsPlan pl;
+    pl.rows = L.nz + 1;
+    pl.warm = warm;
+    pl.nstrips = ts_strips<T>(L.nx);
+    const int C = 3 * pl.nstrips;
+    /* segments a column may take: every segment after the first keeps at
+     * least 16 rows of its own beyond its warm rows */
+    int max_seg = 1;
+    while (max_seg < pl.rows) {
+        const int n = max_seg + 1;
+        const int chunk = (pl.rows + (n - 1) * warm + n - 1) / n;
+        if (chunk - warm < 16) break;
+        max_seg = n;
+    }
+    if (W <= 0) W = ts_slots<T>();
+    if (W < C) W = C;
+    if (W > C * max_seg) W = C * max_seg;
+    pl.W = W;
+    pl.base = W / C;
+    pl.extra = W % C;
+    const dim3 grid((unsigned)((W + TS_WARPS - 1) / TS_WARPS));
     const size_t smem = ts_smem_bytes<T>();
     const int block = 32 * TS_WARPS;
-    if (S == 3) k_mg_smooth_tma<T, 3><<<grid, block, smem, c->stream>>>(maps, m, L, l, seg_len, warm, c->inside, c->status);
-    else if (S == 2) k_mg_smooth_tma<T, 2><<<grid, block, smem, c->stream>>>(maps, m, L, l, seg_len, warm, c->inside, c->status);
-    else k_mg_smooth_tma<T, 1><<<grid, block, smem, c->stream>>>(maps, m, L, l, seg_len, warm, c->inside, c->status);
+    if (S == 3) k_mg_smooth_tma<T, 3><<<grid, block, smem, c->stream>>>(maps, m, L, l, pl, c->inside, c->status);
+    else if (S == 2) k_mg_smooth_tma<T, 2><<<grid, block, smem, c->stream>>>(maps, m, L, l, pl, c->inside, c->status);
+    else k_mg_smooth_tma<T, 1><<<grid, block, smem, c->stream>>>(maps, m, L, l, pl, c->inside, c->status);
     c->launches++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
@@ -579,15 +667,27 @@ static int ts_launch(bcg_ctx* c, const MgConst& m, const MgLvlT<T>& L, int l, in
 
 int mg_smooth_tma(bcg_ctx* c, const MgConst& m, const MgLvl& L, int l, int S, int target_warps, int warm)
 {
-    const int per_seg = 3 * ts_strips<double>(L.nx);
-    return ts_launch<double>(c, m, L, l, S, (target_warps + per_seg / 2) / per_seg, warm);
+    return ts_launch<double>(c, m, L, l, S, target_warps, warm);
 }
 int mg_smooth_tma(bcg_ctx* c, const MgConst& m, const MgLvlF& L, int l, int S, int target_warps, int warm)
 {
-    const int per_seg = 3 * ts_strips<float>(L.nx);
-    return ts_launch<float>(c, m, L, l, S, (target_warps + per_seg / 2) / per_seg, warm);
+    return ts_launch<float>(c, m, L, l, S, target_warps, warm);
 }
-int mg_smooth_tma_warps_per_segment(int nx) { return 3 * ts_strips<double>(nx); }
+int mg_smooth_tma_slots() { return ts_slots<double>(); }
+/* a block's shared memory (two rings and two R windows) passes the 48 KB
+ * that needs no opt-in */
+int mg_smooth_tma_attributes()
+{
+    const int d = ts_smem_bytes<double>(), f = ts_smem_bytes<float>();
+    if (cudaFuncSetAttribute(k_mg_smooth_tma<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, d) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, d) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, d) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, f) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, f) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, f) != cudaSuccess)
+        return BCG_E_CUDA;
+    return BCG_OK;
+}
 /* the kernel keeps one side-column form per warp: a level whose columns 0
  * and nx fall in one strip goes to the other smoother */
 int mg_smooth_tma_fits(int nx) { return ts_strips<double>(nx) >= 2 && ts_strips<float>(nx) >= 2; }
