@@ -952,8 +952,11 @@ def b200_arm(args):
     sm_bytes = 24.0 * lvl0_pts
     if mg_ms >= mech_ms and sm_ms > 0:
         sm_gbs = sm_bytes / (sm_ms / 1e3) / 1e9
-        traffic, traffic_src = profiled_traffic("k_mg_smooth_mixed_1m.md", args.workload)
-        roof = {"kernel": "k_mg_smooth<double,3> (finest agar level, 3 fused zebra sweeps)", "bound": "hbm",
+        # the smoother form in use (bcg_set_relax_mode; the library's default is 3)
+        tma = tuned.get("relax_mode", 3) == 3
+        kname = "k_mg_smooth_tma" if tma else "k_mg_smooth"
+        traffic, traffic_src = profiled_traffic(kname + "_" + args.workload + ".md", args.workload)
+        roof = {"kernel": kname + "<double,3> (finest agar level, 3 fused zebra sweeps)", "bound": "hbm",
                 "achieved": sm_gbs, "peak": peak_gbs, "unit": "GB/s", "frac": sm_gbs / peak_gbs,
                 "traffic": traffic, "traffic_source": traffic_src,
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": sm_bytes,
