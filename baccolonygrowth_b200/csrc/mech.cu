@@ -607,15 +607,16 @@ __device__ void divide_compute(int m, int d, const float* u, double t, const Cel
  * list it can rebuild (the mother before and after, her listed neighbours,
  * the daughter).  Every box a rebuild scans, and every box whose content
  * the division changes, lies inside it.  Divisions whose footprints overlap
- * are joined (union-find) into one group, and a group runs its divisions in
- * ascending order on one warp.  Divisions of different groups neither
- * change a box the other scans nor rebuild a common list, so the lists
- * come out as in the sequential loop.
+ * are joined into one group (connected components), and a group runs its
+ * divisions in ascending order on one block.  Divisions of different groups
+ * neither change a box the other scans nor rebuild a common list, so the
+ * lists come out as in the sequential loop.
  *
  * k_div_plan (one CTA): sort the parents, apply the reference's MaxCells
  * cut, compute all divisions' geometry (divide_compute; SoA fields written
- * here), footprints, groups, and the group-ordered division list.
- * k_div_groups (one warp per group): store the records, mark the mother
+ * here), footprints, groups (label propagation over the overlapping pairs,
+ * then a sort by (group, division)), and the group-ordered division list.
+ * k_div_groups (one block per group): store the records, mark the mother
  * moved, append both cells to the group's delta list, rebuild the lists. */
 __global__ void __launch_bounds__(1024) k_div_plan(int n_start, int ndiv, int cap, double t,
         const float* __restrict__ draws, const CellRec* __restrict__ rec, CellSoA soa, MechParams mp,
@@ -717,54 +718,121 @@ __global__ void __launch_bounds__(1024) k_div_plan(int n_start, int ndiv, int ca
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const int npairs = s_npairs;
-        if (npairs > DIV_PAIR_CAP) {
-            for (int d = 0; d < nd; d++) par[d] = 0;      /* too many: one sequential group */
-        } else {
-            for (int k = 0; k < npairs; k++) {
-                int a = pairs[k].x, b = pairs[k].y;
-                while (par[a] != a) a = par[a];
-                while (par[b] != b) b = par[b];
-                if (a != b) { if (a < b) par[b] = a; else par[a] = b; }
+    const int npairs = s_npairs;
+    if (npairs > DIV_PAIR_CAP) {
+        /* too many overlaps to list: one sequential group */
+        for (int d = threadIdx.x; d < nd; d += blockDim.x) par[d] = 0;
+        __syncthreads();
+    } else {
+        /* connected components by label propagation: every division takes
+         * the smallest label among the divisions its footprint overlaps,
+         * then follows its label's label, until nothing changes; the label
+         * ends as the smallest division of its component */
+        for (;;) {
+            __shared__ int s_changed;
+            if (threadIdx.x == 0) s_changed = 0;
+            __syncthreads();
+            for (int k = threadIdx.x; k < npairs; k += blockDim.x) {
+                const int a = pairs[k].x, b = pairs[k].y;
+                const int la = par[a], lb = par[b];
+                if (la != lb) {
+                    const int lo = la < lb ? la : lb;
+                    atomicMin(&par[a], lo);
+                    atomicMin(&par[b], lo);
+                    atomicMin(&par[la], lo);
+                    atomicMin(&par[lb], lo);
+                    s_changed = 1;
+                }
             }
-            for (int d = 0; d < nd; d++) { int r = d; while (par[r] != r) r = par[r]; par[d] = r; }
+            __syncthreads();
+            for (int d = threadIdx.x; d < nd; d += blockDim.x) {
+                const int l = par[d], ll = par[l];
+                if (ll < l) { atomicMin(&par[d], ll); s_changed = 1; }
+            }
+            __syncthreads();
+            const int ch = s_changed;
+            __syncthreads();
+            if (!ch) break;
         }
-        /* groups in order of their first division; members ascending.
-         * grp[2g] = start in order[], grp[2g+1] = length; roots count
-         * their members in sd[] (free after the sort) */
-        int ng = 0;
-        for (int d = 0; d < nd; d++) sd[d] = 0;
-        for (int d = 0; d < nd; d++) sd[par[d]]++;
-        int pos = 0;
-        for (int d = 0; d < nd; d++)
-            if (par[d] == d) { grp[2 * ng] = pos; grp[2 * ng + 1] = sd[d]; fill[ng] = pos; sd[d] = ng; pos += grp[2 * ng + 1]; ng++; }
-        /* members in ascending d */
-        for (int d = 0; d < nd; d++) order[fill[sd[par[d]]]++] = d;
-        out[0] = nd; out[1] = n_start + nd; out[2] = ng;
     }
+    /* groups in order of their first division, members ascending: sort the
+     * keys (label, division) and cut the sorted list where the label
+     * changes.  grp[2g] = start in order[], grp[2g+1] = length. */
+    int P2n = 1;
+    while (P2n < nd) P2n <<= 1;
+    for (int i = threadIdx.x; i < P2n; i += blockDim.x) sd[i] = i < nd ? par[i] * DIV_SORT_MAX + i : 0x7fffffff;
+    __syncthreads();
+    for (int k = 2; k <= P2n; k <<= 1)
+        for (int jj = k >> 1; jj > 0; jj >>= 1) {
+            for (int i = threadIdx.x; i < P2n; i += blockDim.x) {
+                int ixj = i ^ jj;
+                if (ixj > i) {
+                    int a = sd[i], b = sd[ixj];
+                    bool up = (i & k) == 0;
+                    if ((a > b) == up) { sd[i] = b; sd[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    /* fill[i] = 1 where a group starts, then its inclusive prefix sum */
+    for (int i = threadIdx.x; i < P2n; i += blockDim.x)
+        fill[i] = (i < nd && (i == 0 || sd[i] / DIV_SORT_MAX != sd[i - 1] / DIV_SORT_MAX)) ? 1 : 0;
+    __syncthreads();
+    for (int off = 1; off < P2n; off <<= 1) {
+        int v[DIV_SORT_MAX / 1024];
+        int c = 0;
+        for (int i = threadIdx.x; i < P2n; i += blockDim.x) v[c++] = i >= off ? fill[i - off] : 0;
+        __syncthreads();
+        c = 0;
+        for (int i = threadIdx.x; i < P2n; i += blockDim.x) fill[i] += v[c++];
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) {
+        const int d = sd[i] - (sd[i] / DIV_SORT_MAX) * DIV_SORT_MAX;
+        order[i] = d;
+        const int g = fill[i] - 1;
+        const bool start = i == 0 || sd[i] / DIV_SORT_MAX != sd[i - 1] / DIV_SORT_MAX;
+        if (start) grp[2 * g] = i;
+    }
+    __syncthreads();
+    /* the group's length, from its last member and its start */
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) {
+        const bool last = i == nd - 1 || sd[i] / DIV_SORT_MAX != sd[i + 1] / DIV_SORT_MAX;
+        if (last) {
+            const int g = fill[i] - 1;
+            grp[2 * g + 1] = i + 1 - grp[2 * g];
+        }
+    }
+    if (threadIdx.x == 0) { out[0] = nd; out[1] = n_start + nd; out[2] = nd > 0 ? fill[nd - 1] : 0; }
     (void)par_out;
 }
 
-__global__ void __launch_bounds__(128) k_div_groups(int n_start, const int* __restrict__ div_out,
+/* One block per group.  The group's divisions run in ascending order; the
+ * lists one division rebuilds (the mother's, her listed neighbours', the
+ * daughter's) each depend only on the records and the boxes, which the
+ * rebuilds do not change, so the block's warps share them out. */
+#define DIV_GROUP_WARPS 4
+__global__ void __launch_bounds__(32 * DIV_GROUP_WARPS) k_div_groups(int n_start, const int* __restrict__ div_out,
         const int* __restrict__ grp, const int* __restrict__ order, const int* __restrict__ lineage,
         const CellRec* __restrict__ new_rec, const int* __restrict__ new_box,
         CellRec* rec, MechParams mp, int* nbr, int* ncount,
         const int* __restrict__ box_start, const int* __restrict__ box_ids,
         int* moved, int* delta_ids, int* delta_box, DevStatus* st)
 {
-    __shared__ int idl_all[4][1 + 1024 + 1];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int g = blockIdx.x * 4 + w;
-    if (g >= div_out[2]) return;                       /* whole warp */
-    int* idl = idl_all[w];
+    __shared__ int idl[1 + 1024 + 1];
+    const int w = threadIdx.x >> 5;
+    const int g = blockIdx.x;
+    if (g >= div_out[2]) return;                       /* whole block */
     const int gs = grp[2 * g], gl = grp[2 * g + 1];
     int* dids = delta_ids + 2 * gs;
     int* dbox = delta_box + 2 * gs;
     for (int j = 0; j < gl; j++) {
         const int d = order[gs + j];
         const int m = lineage[2 * d], N = n_start + d;
-        if (lane == 0) {
+        /* the previous division's rebuilds are done (they may have written
+         * this mother's list) before her records and list change hands */
+        __syncthreads();
+        if (threadIdx.x == 0) {
             rec[m] = new_rec[2 * d];
             rec[N] = new_rec[2 * d + 1];
             moved[m] = 1;
@@ -772,16 +840,15 @@ __global__ void __launch_bounds__(128) k_div_groups(int n_start, const int* __re
             dids[2 * j + 1] = N; dbox[2 * j + 1] = new_box[2 * d + 1];
         }
         const int cnt = ncount[m];
-        for (int i = lane; i < cnt; i += 32) idl[1 + i] = nbr[(size_t)m * mp.kmax + i];
-        if (lane == 0) { idl[0] = m; idl[cnt + 1] = N; }
-        __threadfence_block();
-        __syncwarp();
-        for (int k = 0; k < cnt + 2; k++)
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) idl[1 + i] = nbr[(size_t)m * mp.kmax + i];
+        if (threadIdx.x == 0) { idl[0] = m; idl[cnt + 1] = N; }
+        /* every thread has read the mother's old list before a warp rewrites it */
+        __syncthreads();
+        for (int k = w; k < cnt + 2; k += DIV_GROUP_WARPS)
             warp_rebuild_one<true>(idl[k], rec, mp, box_start, box_ids, moved, dids, dbox, 2 * (j + 1), nbr, ncount, st);
-        __syncwarp();
     }
-    __syncwarp();
-    for (int j = lane; j < gl; j += 32) moved[lineage[2 * order[gs + j]]] = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < gl; j += blockDim.x) moved[lineage[2 * order[gs + j]]] = 0;
 }
 
 /* the division planner's shared memory: sorted parents, union-find
@@ -830,7 +897,7 @@ int divide_launch(bcg_ctx* c, const float* draws, int n_draw_sets, double t)
     k_div_plan<<<1, 1024, DIV_PLAN_SMEM, c->stream>>>(c->n, ndiv, c->cap, t, c->draws_dev, c->rec[nb], c->soa, mp,
         c->div_list, c->cell_box, c->nbr, c->ncount, c->div_rec, c->div_box, c->div_rect, c->div_pairs,
         c->div_par, c->div_order, c->div_grp, c->lineage, c->n_done_dev, c->status);
-    k_div_groups<<<(ndiv + 3) / 4, 128, 0, c->stream>>>(c->n, c->n_done_dev, c->div_grp, c->div_order,
+    k_div_groups<<<ndiv, 32 * DIV_GROUP_WARPS, 0, c->stream>>>(c->n, c->n_done_dev, c->div_grp, c->div_order,
         c->lineage, c->div_rec, c->div_box, c->rec[nb], mp, c->nbr, c->ncount, c->box_start, c->box_ids,
         c->moved, c->delta_ids, c->delta_box, c->status);
     c->launches += 2;
