@@ -182,41 +182,68 @@ __device__ void warp_rebuild_one(int me, const CellRec* rec, MechParams mp,
     int xi, yi, zi;
     int abox = box_address(acm, mp, xi, yi, zi);
     if (abox < 0) { if (lane == 0) dev_error(st, BCG_E_OUT_OF_GRID, me); return; }
-    int cnt = 0;
     int* out = nbr + (size_t)me * mp.kmax;
     const int YZ = mp.box_y * mp.box_z;
-    for (int za = max(zi - 1, 0); za < min(zi + 2, mp.box_z); za++)
-        for (int ya = max(yi - 1, 0); ya < min(yi + 2, mp.box_y); ya++)
-            for (int xa = max(xi - 1, 0); xa < min(xi + 2, mp.box_x); xa++) {
-                int b = xa * YZ + ya * mp.box_z + za;
-                int s = box_start[b], e = box_start[b + 1];
-                if (e - s > mp.box_cap) e = s + mp.box_cap;   /* overfull: error already raised by the binning */
-                for (int t = s; t < e; t += 32) {
-                    int j = (t + lane < e) ? box_ids[t + lane] : -1;
-                    bool keep = false;
-                    if (j >= 0 && j != me && !(moved && moved[j])) {
-                        Cst bj = COH ? load_cst_coh(&rec[j]) : load_cst(&rec[j]);
-                        keep = keep_neighbour(a.p, a.q, a.L, a.R, acm, bj.p, bj.q, mp.rc);
-                    }
-                    unsigned m = __ballot_sync(0xffffffffu, keep);
-                    int pos = cnt + __popc(m & ((1u << lane) - 1));
-                    if (keep && pos < mp.kmax) out[pos] = j;
-                    cnt += __popc(m);
-                }
-                for (int t = 0; t < ndelta; t += 32) {
-                    int j = -1;
-                    if (t + lane < ndelta && delta_box[t + lane] == b) j = delta_ids[t + lane];
-                    bool keep = false;
-                    if (j >= 0 && j != me) {
-                        Cst bj = COH ? load_cst_coh(&rec[j]) : load_cst(&rec[j]);
-                        keep = keep_neighbour(a.p, a.q, a.L, a.R, acm, bj.p, bj.q, mp.rc);
-                    }
-                    unsigned m = __ballot_sync(0xffffffffu, keep);
-                    int pos = cnt + __popc(m & ((1u << lane) - 1));
-                    if (keep && pos < mp.kmax) out[pos] = j;
-                    cnt += __popc(m);
-                }
+    /* the stencil's boxes in scan order, one a lane: lane i takes
+     * (dz, dy, dx) = i / 9, i / 3 % 3, i % 3 around the cell's box, boxes
+     * off the grid counting nothing.  Each box contributes its binned cells
+     * (in bin order), then the delta cells listed in it. */
+    int bs = 0, nbin = 0, ndel = 0, b = -1;
+    if (lane < 27) {
+        const int za = zi - 1 + lane / 9, ya = yi - 1 + (lane / 3) % 3, xa = xi - 1 + lane % 3;
+        if (za >= 0 && za < mp.box_z && ya >= 0 && ya < mp.box_y && xa >= 0 && xa < mp.box_x) {
+            b = xa * YZ + ya * mp.box_z + za;
+            bs = box_start[b];
+            int e = box_start[b + 1];
+            if (e - bs > mp.box_cap) e = bs + mp.box_cap;   /* overfull: error already raised by the binning */
+            nbin = e - bs;
+            for (int t = 0; t < ndelta; t++) ndel += (delta_box[t] == b);
+        }
+    }
+    /* exclusive prefix of the boxes' candidate counts */
+    const int tot_i = nbin + ndel;
+    int incl = tot_i;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int off = incl - tot_i;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    int cnt = 0;
+    for (int t0 = 0; t0 < total; t0 += 32) {
+        const int f = t0 + lane;
+        /* the box holding candidate f: the last lane whose offset is <= f */
+        int box = 0;
+        for (int q = 1; q < 27; q++) {
+            const int oq = __shfl_sync(0xffffffffu, off, q), tq = __shfl_sync(0xffffffffu, tot_i, q);
+            if (tq > 0 && oq <= f) box = q;
+        }
+        const int ob = __shfl_sync(0xffffffffu, off, box), nb_ = __shfl_sync(0xffffffffu, nbin, box);
+        const int sb = __shfl_sync(0xffffffffu, bs, box), bb = __shfl_sync(0xffffffffu, b, box);
+        int j = -1;
+        bool from_delta = false;
+        if (f < total) {
+            const int r = f - ob;
+            if (r < nb_) {
+                j = box_ids[sb + r];
+            } else {
+                /* the (r - nb_)-th delta cell listed in this box */
+                int k = r - nb_;
+                for (int t = 0; t < ndelta; t++)
+                    if (delta_box[t] == bb) { if (k == 0) { j = delta_ids[t]; break; } k--; }
+                from_delta = true;
             }
+        }
+        bool keep = false;
+        if (j >= 0 && j != me && (from_delta || !(moved && moved[j]))) {
+            Cst bj = COH ? load_cst_coh(&rec[j]) : load_cst(&rec[j]);
+            keep = keep_neighbour(a.p, a.q, a.L, a.R, acm, bj.p, bj.q, mp.rc);
+        }
+        unsigned m = __ballot_sync(0xffffffffu, keep);
+        int pos = cnt + __popc(m & ((1u << lane) - 1));
+        if (keep && pos < mp.kmax) out[pos] = j;
+        cnt += __popc(m);
+    }
     if (cnt > mp.kmax) { if (lane == 0) dev_error(st, BCG_E_NEIGH_OVERFLOW, me); cnt = mp.kmax; }
     if (lane == 0) ncount[me] = cnt;
 }
