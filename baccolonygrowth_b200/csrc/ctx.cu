@@ -303,6 +303,7 @@ extern "C" int bcg_destroy(bcg_ctx* c)
     if (c->leg_snap) cudaFree(c->leg_snap);
     if (c->leg_conv) cudaFree(c->leg_conv);
     for (int g = 0; g < 2; g++) if (c->nutrient_graph[g]) cudaGraphExecDestroy(c->nutrient_graph[g]);
+    if (c->solve_graph) cudaGraphExecDestroy(c->solve_graph);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (int t = 0; t < BCG_T_COUNT; t++) { if (c->ev[t][0]) cudaEventDestroy(c->ev[t][0]); if (c->ev[t][1]) cudaEventDestroy(c->ev[t][1]); }
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -99,6 +99,11 @@ struct bcg_ctx {
     cudaGraphExec_t nutrient_graph[2];
     int nutrient_graph_sweeps;           /* 0: none captured (dropped whenever a kernel choice changes) */
     int nutrient_graph_launches[2];
+    /* the captured per-step solve (bcg_mg_solve): its key (V-cycles, wall
+     * buffer, whether Err and Res were clean on entry; -1: none) */
+    cudaGraphExec_t solve_graph;
+    int solve_graph_key;
+    int solve_graph_launches;
     /* timers */
     int timers_on;
     cudaEvent_t ev[BCG_T_COUNT][2];

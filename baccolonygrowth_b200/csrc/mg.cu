@@ -1605,13 +1605,49 @@ int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf)
     return cudaGetLastError() == cudaSuccess ? BCG_OK : BCG_E_CUDA;
 }
 
+/* Multigrid::solve as one graph launch.  A solve issues the same kernels
+ * with the same arguments every time it starts from the same state: the
+ * V-cycle count, the wall buffer and whether Err and Res are clean (the
+ * first solve of a context runs the full setup(), later ones the clean
+ * form).  The graph is captured on first use for a key and dropped with the
+ * nutrient graphs, whenever a kernel shape of the context changes or a
+ * caller writes a multigrid array. */
+static int mg_solve_graphed(bcg_ctx* c, int vcycles, int wall_buf)
+{
+    const int key = (vcycles << 2) | (wall_buf << 1) | (c->mg_clean ? 1 : 0);
+    if (!c->solve_graph || c->solve_graph_key != key) {
+        if (c->solve_graph) { cudaGraphExecDestroy(c->solve_graph); c->solve_graph = nullptr; }
+        cudaGraph_t g;
+        BCG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const long long l0 = c->launches;
+        const int rc = mg_solve_impl(c, vcycles, wall_buf);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->solve_graph_launches = (int)(c->launches - l0);
+        c->launches = l0;
+        if (rc) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
+        e = cudaGraphInstantiate(&c->solve_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { c->solve_graph = nullptr; bcg_set_cuda_error(e); return BCG_E_CUDA; }
+        c->solve_graph_key = key;
+    } else {
+        /* the host state a solve leaves (mg_setup, mg_reset, mg_copy_from) */
+        c->mg_res0_stale = 1;
+        c->mg_clean = 1;
+        c->leg_old_stale = 1;
+    }
+    BCG_CUDA_TRY(cudaGraphLaunch(c->solve_graph, c->stream));
+    c->launches += c->solve_graph_launches;
+    return BCG_OK;
+}
+
 extern "C" int bcg_mg_solve(bcg_ctx* c, int vcycles)
 {
     if (!c) return BCG_E_ARG;
     if (vcycles <= 0) vcycles = c->P.mg_vcycles;
     timer_begin(c, BCG_T_MG_SOLVE);
     long long l0 = c->launches;
-    int rc = mg_solve_impl(c, vcycles, 0);
+    int rc = mg_solve_graphed(c, vcycles, 0);
     if (rc) return rc;
     timer_end(c, BCG_T_MG_SOLVE, (int)(c->launches - l0));
     return ctx_check_status(c);

@@ -416,12 +416,14 @@ extern "C" int bcg_colony_sweeps(bcg_ctx* c, int sweeps, int count0)
  * count the local buffer indices and the sweep-count parity are back where
  * they started after each unit, so every unit issues the same kernels with
  * the same arguments. */
-/* drop the cached graphs (a kernel shape of this context changed) */
+/* drop the cached graphs, the nutrient units' and the per-step solve's (a
+ * kernel shape of this context changed, or Err and Res stopped being clean) */
 void nutrient_graphs_drop(bcg_ctx* c)
 {
     for (int g = 0; g < 2; g++)
         if (c->nutrient_graph[g]) { cudaGraphExecDestroy(c->nutrient_graph[g]); c->nutrient_graph[g] = nullptr; }
     c->nutrient_graph_sweeps = 0;
+    if (c->solve_graph) { cudaGraphExecDestroy(c->solve_graph); c->solve_graph = nullptr; }
 }
 
 static int nutrient_unit_graph(bcg_ctx* c, int sweeps, int last, cudaGraphExec_t* out)
