@@ -160,6 +160,12 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
     c->relax_mode = 3;
     cudaGetDevice(&c->device);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { free(c); return BCG_E_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        bcg_destroy(c);
+        return BCG_E_CUDA;
+    }
     for (int t = 0; t < BCG_T_COUNT; t++) { cudaEventCreate(&c->ev[t][0]); cudaEventCreate(&c->ev[t][1]); }
     const size_t cap = (size_t)p->max_cells;
     c->cap = p->max_cells;
@@ -306,6 +312,9 @@ extern "C" int bcg_destroy(bcg_ctx* c)
     if (c->solve_graph) cudaGraphExecDestroy(c->solve_graph);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (int t = 0; t < BCG_T_COUNT; t++) { if (c->ev[t][0]) cudaEventDestroy(c->ev[t][0]); if (c->ev[t][1]) cudaEventDestroy(c->ev[t][1]); }
+    if (c->aux_stream) { cudaStreamSynchronize(c->aux_stream); cudaStreamDestroy(c->aux_stream); }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->stream) cudaStreamDestroy(c->stream);
     free(c);
     return BCG_OK;

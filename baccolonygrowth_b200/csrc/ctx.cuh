@@ -104,6 +104,11 @@ struct bcg_ctx {
     cudaGraphExec_t solve_graph;
     int solve_graph_key;
     int solve_graph_launches;
+    /* the second stream of the benchmark step's agar solve, which runs beside
+     * the step's mechanics; ev_fork orders it after the work before it,
+     * ev_join orders the work after the step after it */
+    cudaStream_t aux_stream;
+    cudaEvent_t ev_fork, ev_join;
     /* timers */
     int timers_on;
     cudaEvent_t ev[BCG_T_COUNT][2];

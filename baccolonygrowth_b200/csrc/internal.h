@@ -16,6 +16,12 @@ int bcg_int_divide_finish(bcg_ctx* ctx, int* n_done, int* lineage);
 /* queue Multigrid::solve with `vcycles` V-cycles (errors surface at the
  * next synchronising call) */
 int bcg_int_mg_solve_launch(bcg_ctx* ctx, int vcycles);
+/* queue Multigrid::solve on the context's second stream, beside what is
+ * queued after it until bcg_int_join; nothing queued in between may touch
+ * the multigrid arrays, the agar and wall fields or the density */
+int bcg_int_mg_solve_aside(bcg_ctx* ctx, int vcycles);
+/* order the context's stream after its second stream's work */
+int bcg_int_join(bcg_ctx* ctx);
 
 /* Output-step snapshots (output.cu), used by the writer (writer.cpp).
  * One snapshot is a byte image laid out by bcg_out_layout: cell records,

@@ -1612,7 +1612,7 @@ int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf)
  * form).  The graph is captured on first use for a key and dropped with the
  * nutrient graphs, whenever a kernel shape of the context changes or a
  * caller writes a multigrid array. */
-static int mg_solve_graphed(bcg_ctx* c, int vcycles, int wall_buf)
+static int mg_solve_graphed(bcg_ctx* c, int vcycles, int wall_buf, cudaStream_t launch)
 {
     const int key = (vcycles << 2) | (wall_buf << 1) | (c->mg_clean ? 1 : 0);
     if (!c->solve_graph || c->solve_graph_key != key) {
@@ -1636,7 +1636,7 @@ static int mg_solve_graphed(bcg_ctx* c, int vcycles, int wall_buf)
         c->mg_clean = 1;
         c->leg_old_stale = 1;
     }
-    BCG_CUDA_TRY(cudaGraphLaunch(c->solve_graph, c->stream));
+    BCG_CUDA_TRY(cudaGraphLaunch(c->solve_graph, launch));
     c->launches += c->solve_graph_launches;
     return BCG_OK;
 }
@@ -1647,7 +1647,7 @@ extern "C" int bcg_mg_solve(bcg_ctx* c, int vcycles)
     if (vcycles <= 0) vcycles = c->P.mg_vcycles;
     timer_begin(c, BCG_T_MG_SOLVE);
     long long l0 = c->launches;
-    int rc = mg_solve_graphed(c, vcycles, 0);
+    int rc = mg_solve_graphed(c, vcycles, 0, c->stream);
     if (rc) return rc;
     timer_end(c, BCG_T_MG_SOLVE, (int)(c->launches - l0));
     return ctx_check_status(c);
@@ -1806,5 +1806,39 @@ extern "C" int bcg_int_mg_solve_launch(bcg_ctx* c, int vcycles)
     if (!c) return BCG_E_ARG;
     if (vcycles <= 0) vcycles = c->P.mg_vcycles;
     return mg_solve_impl(c, vcycles, 0);
+}
+
+/* Multigrid::solve on the context's second stream, after the work queued
+ * before it, beside the work queued after it until bcg_int_join.  The
+ * caller queues nothing that reads or writes the multigrid arrays, the
+ * agar and wall fields or the colony's density before the join.  With the
+ * timers on, the solve is timed on its own stream (and waited for). */
+extern "C" int bcg_int_mg_solve_aside(bcg_ctx* c, int vcycles)
+{
+    if (!c) return BCG_E_ARG;
+    if (vcycles <= 0) vcycles = c->P.mg_vcycles;
+    BCG_CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
+    BCG_CUDA_TRY(cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
+    if (c->timers_on) cudaEventRecord(c->ev[BCG_T_MG_SOLVE][0], c->aux_stream);
+    long long l0 = c->launches;
+    int rc = mg_solve_graphed(c, vcycles, 0, c->aux_stream);
+    if (rc) return rc;
+    c->timer_launches[BCG_T_MG_SOLVE] += (int)(c->launches - l0);
+    if (c->timers_on) {
+        cudaEventRecord(c->ev[BCG_T_MG_SOLVE][1], c->aux_stream);
+        cudaEventSynchronize(c->ev[BCG_T_MG_SOLVE][1]);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[BCG_T_MG_SOLVE][0], c->ev[BCG_T_MG_SOLVE][1]);
+        c->timer_ms[BCG_T_MG_SOLVE] += ms;
+    }
+    return BCG_OK;
+}
+/* the context's stream waits for the second stream's work */
+extern "C" int bcg_int_join(bcg_ctx* c)
+{
+    if (!c) return BCG_E_ARG;
+    BCG_CUDA_TRY(cudaEventRecord(c->ev_join, c->aux_stream));
+    BCG_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    return BCG_OK;
 }
 

@@ -142,7 +142,7 @@ static void sim_draws(bcg_sim* s, int nd, int64_t calls)
  * before MoveCell, whose F_cw draws the host skips, and with a writer
  * attached writes the step's files (Simulation.cpp:316-327, 340-372) and
  * the lineage lines (Simulation.cpp:392). */
-static int sim_step(bcg_sim* s)
+static int sim_step_body(bcg_sim* s, bool* aside)
 {
     int rc;
     const bool out = s->reference_cadence && s->out_flag;
@@ -168,7 +168,13 @@ static int sim_step(bcg_sim* s)
             if ((rc = bcg_rebuild_neighbours(s->ctx))) return rc;
             s->rebuilds++;
         }
-        if (s->vcycles_per_step > 0 && (rc = bcg_mg_solve(s->ctx, s->vcycles_per_step))) return rc;
+        /* the solve touches only the multigrid arrays and the agar and wall
+         * fields; the step's mechanics and divisions touch none of them, so
+         * the solve runs on the context's second stream beside them */
+        if (s->vcycles_per_step > 0) {
+            if ((rc = bcg_int_mg_solve_aside(s->ctx, s->vcycles_per_step))) return rc;
+            *aside = true;
+        }
     }
     s->first_step = false;
     if (out) {
@@ -194,6 +200,19 @@ static int sim_step(bcg_sim* s)
         if (lrc && !rc) rc = lrc;
     }
     return sim_advance(s, base, done, rc);
+}
+
+/* One step; the context's stream waits for the step's agar solve before
+ * anything queued after the step */
+static int sim_step(bcg_sim* s)
+{
+    bool aside = false;
+    int rc = sim_step_body(s, &aside);
+    if (aside) {
+        const int jr = bcg_int_join(s->ctx);
+        if (!rc) rc = jr;
+    }
+    return rc;
 }
 
 extern "C" int bcg_sim_run(bcg_sim* s, int steps)
