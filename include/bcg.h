@@ -147,7 +147,10 @@ int bcg_create(const bcg_params* p, bcg_ctx** out);
 int bcg_destroy(bcg_ctx* ctx);
 /* Last device error word (0 if none) and a static message for a status. */
 const char* bcg_status_string(int status);
-/* The CUDA stream all work of this context is queued on (cudaStream_t). */
+/* The CUDA stream all work of this context is queued on (cudaStream_t).
+ * Inside a benchmark-cadence step of bcg_sim_run the agar solve runs on a
+ * second stream of the context; the step ends with this stream waiting for
+ * it, so work queued here after any call sees every result of that call. */
 void* bcg_stream(bcg_ctx* ctx);
 /* Block until all queued work of ctx is done; returns the first pending error. */
 int bcg_synchronize(bcg_ctx* ctx);
@@ -626,7 +629,9 @@ int bcg_sim_counters(bcg_sim* sim, int64_t* neighbour_rebuilds, int64_t* field_u
 int bcg_sim_lineage(bcg_sim* sim, int* pairs, int capacity, int* n);
 /* Per-step mode used by benchmarks: each step runs the mechanics step and
  * `vcycles` V-cycles of the agar solve instead of the reference's field
- * cadence (0 = mechanics only). */
+ * cadence (0 = mechanics only).  The solve touches no data of the
+ * mechanics in this cadence, so it runs beside them on the context's second
+ * stream; results are the same as in sequence. */
 int bcg_sim_set_step_mode(bcg_sim* sim, int field_cadence_reference, int vcycles_per_step);
 
 /* Ensembles of independent colonies (no reference counterpart; the
