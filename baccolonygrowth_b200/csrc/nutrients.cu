@@ -159,8 +159,13 @@ __device__ __forceinline__ void colony_point(const NutConst& n, int x, int z, co
             buffer_solve(n, Agr, ph, hy, ac, bu);
             prev.ph[id] = ph; prev.hyd[id] = hy; prev.ace[id] = ac; prev.buf[id] = bu;
         }
-        double fCgr_aer = Cgr / (Cgr + n.kc_aer), fCgr_ana = Cgr / (Cgr + n.kc_ana);
-        double fAgr = Agr / (Agr + n.ka), fOgr = Ogr / (Ogr + n.ko), fIgr = 0;
+        /* x / (x + k): for x = 0 and k > 0 the quotient is x itself, taken
+         * here without the division, whose zero dividend leaves its fast
+         * path (the species start at zero, acetate everywhere) */
+        double fCgr_aer = (Cgr == 0.0 && n.kc_aer > 0.0) ? Cgr : Cgr / (Cgr + n.kc_aer);
+        double fCgr_ana = (Cgr == 0.0 && n.kc_ana > 0.0) ? Cgr : Cgr / (Cgr + n.kc_ana);
+        double fAgr = (Agr == 0.0 && n.ka > 0.0) ? Agr : Agr / (Agr + n.ka);
+        double fOgr = (Ogr == 0.0 && n.ko > 0.0) ? Ogr : Ogr / (Ogr + n.ko), fIgr = 0;
         double l1 = mx((n.max_gr_car_aer + n.mgrCarAers) * fCgr_aer - n.mgrCarAers, 0.0);
         double l2 = mx((n.max_gr_car_ana + n.mgrCarAnas) * fCgr_ana - n.mgrCarAnas, 0.0);
         double l3 = mx((n.max_gr_ace_aer + n.mgrAceAers) * fAgr - n.mgrAceAers, 0.0);
