@@ -103,6 +103,8 @@ struct bcg_ctx {
      * buffer, whether Err and Res were clean on entry; -1: none) */
     cudaGraphExec_t solve_graph;
     int solve_graph_key;
+    int solve_graph_seen;         /* key of the last solve run uncaptured (0: none) */
+    int solve_graph_off;          /* 1: a capture failed, the context solves with plain launches */
     int solve_graph_launches;
     /* the second stream of the benchmark step's agar solve, which runs beside
      * the step's mechanics; ev_fork orders it after the work before it,

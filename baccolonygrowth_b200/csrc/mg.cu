@@ -1609,26 +1609,50 @@ int mg_solve_impl(bcg_ctx* c, int vcycles, int wall_buf)
  * with the same arguments every time it starts from the same state: the
  * V-cycle count, the wall buffer and whether Err and Res are clean (the
  * first solve of a context runs the full setup(), later ones the clean
- * form).  The graph is captured on first use for a key and dropped with the
+ * form).  The first solve from a state runs as plain launches, the second
+ * is captured and later ones replay it; the graph is dropped with the
  * nutrient graphs, whenever a kernel shape of the context changes or a
  * caller writes a multigrid array. */
 static int mg_solve_graphed(bcg_ctx* c, int vcycles, int wall_buf, cudaStream_t launch)
 {
     const int key = (vcycles << 2) | (wall_buf << 1) | (c->mg_clean ? 1 : 0);
+    if (c->solve_graph_off) return mg_solve_impl(c, vcycles, wall_buf);
     if (!c->solve_graph || c->solve_graph_key != key) {
         if (c->solve_graph) { cudaGraphExecDestroy(c->solve_graph); c->solve_graph = nullptr; }
-        cudaGraph_t g;
+        if (c->solve_graph_seen != key) {
+            /* the first solve from a state runs as plain launches on the
+             * context's stream: it makes the one-time queries (occupancy,
+             * kernel attributes) a capture may not contain */
+            c->solve_graph_seen = key;
+            const long long l0 = c->launches;
+            const int rc = mg_solve_impl(c, vcycles, wall_buf);
+            c->solve_graph_launches = (int)(c->launches - l0);
+            return rc;
+        }
+        /* the host state the captured pass changes, restored if the
+         * capture fails (it ran nothing on the device) */
+        const int s_clean = c->mg_clean, s_res0 = c->mg_res0_stale, s_leg = c->leg_old_stale;
+        cudaGraph_t g = nullptr;
         BCG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         const long long l0 = c->launches;
         const int rc = mg_solve_impl(c, vcycles, wall_buf);
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         c->solve_graph_launches = (int)(c->launches - l0);
         c->launches = l0;
-        if (rc) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
-        if (e != cudaSuccess) { bcg_set_cuda_error(e); return BCG_E_CUDA; }
-        e = cudaGraphInstantiate(&c->solve_graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) { c->solve_graph = nullptr; bcg_set_cuda_error(e); return BCG_E_CUDA; }
+        if (!rc && e == cudaSuccess) {
+            e = cudaGraphInstantiate(&c->solve_graph, g, 0);
+            if (e != cudaSuccess) c->solve_graph = nullptr;
+        }
+        if (g) cudaGraphDestroy(g);
+        if (rc || e != cudaSuccess) {
+            /* a solve this context cannot capture: plain launches from now
+             * on (a real error shows again there) */
+            cudaGetLastError();
+            c->mg_clean = s_clean; c->mg_res0_stale = s_res0; c->leg_old_stale = s_leg;
+            c->pending_error = BCG_OK;
+            c->solve_graph_off = 1;
+            return mg_solve_impl(c, vcycles, wall_buf);
+        }
         c->solve_graph_key = key;
     } else {
         /* the host state a solve leaves (mg_setup, mg_reset, mg_copy_from) */

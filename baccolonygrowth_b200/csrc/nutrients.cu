@@ -429,6 +429,7 @@ void nutrient_graphs_drop(bcg_ctx* c)
         if (c->nutrient_graph[g]) { cudaGraphExecDestroy(c->nutrient_graph[g]); c->nutrient_graph[g] = nullptr; }
     c->nutrient_graph_sweeps = 0;
     if (c->solve_graph) { cudaGraphExecDestroy(c->solve_graph); c->solve_graph = nullptr; }
+    c->solve_graph_seen = 0;
 }
 
 static int nutrient_unit_graph(bcg_ctx* c, int sweeps, int last, cudaGraphExec_t* out)

@@ -307,6 +307,9 @@ static int ens_step(bcg_ensemble* e)
         if (!first_rc) first_rc = rc;
     };
     int rc;
+    /* each member's agar solve runs on its second stream beside its
+     * mechanics (as in bcg_sim_run), joined once the step is done */
+    std::vector<char> aside(n, 0);
     for (int i = 0; i < n; i++) {
         bcg_sim* s = e->m[i];
         if (s->update_flag || s->first_step) {
@@ -314,7 +317,10 @@ static int ens_step(bcg_ensemble* e)
             if ((rc = bcg_rebuild_neighbours(s->ctx))) { fail(i, rc); continue; }
             s->rebuilds++;
         }
-        if (s->vcycles_per_step > 0 && (rc = bcg_int_mg_solve_launch(s->ctx, s->vcycles_per_step))) { fail(i, rc); continue; }
+        if (s->vcycles_per_step > 0) {
+            if ((rc = bcg_int_mg_solve_aside(s->ctx, s->vcycles_per_step))) { fail(i, rc); continue; }
+            aside[i] = 1;
+        }
         s->first_step = false;
         if ((rc = bcg_int_move_grow_launch(s->ctx, s->dt))) fail(i, rc);
     }
@@ -337,6 +343,10 @@ static int ens_step(bcg_ensemble* e)
         rc = bcg_int_divide_finish(s->ctx, &done, e->nd[i] > 0 ? s->lineage.data() + e->base[i] : nullptr);
         rc = sim_advance(s, e->base[i], done, rc);
         if (rc) fail(i, rc);
+    }
+    for (int i = 0; i < n; i++) {
+        if (!aside[i]) continue;
+        if ((rc = bcg_int_join(e->m[i]->ctx))) fail(i, rc);
     }
     return first_rc;
 }
