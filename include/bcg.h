@@ -317,7 +317,10 @@ int bcg_nutrient_update(bcg_ctx* ctx, int n, int sweeps);
 int bcg_legacy_env_update(bcg_ctx* ctx, int min_iter, int max_iter, double conv_crit, int* iterations);
 int bcg_legacy_agar_depletion(bcg_ctx* ctx, int* steps);
 /* One Multigrid::solve (Multigrid.cpp:864-889) with `vcycles` V-cycles
- * (<=0: params.mg_vcycles): copyToMG, setup, V-cycles, reset, copyFromMG. */
+ * (<=0: params.mg_vcycles): copyToMG, setup, V-cycles, reset, copyFromMG.
+ * Queued on the context's stream.  The second call from the same starting
+ * state captures the launches as a CUDA graph and later calls replay it;
+ * a context whose capture fails keeps issuing plain launches. */
 int bcg_mg_solve(bcg_ctx* ctx, int vcycles);
 /* `sweeps` colony/interface sweeps (the inner loop of Multigrid.cpp:
  * 1017-1120) starting at sweep parity `count0`. */
