@@ -85,10 +85,11 @@ struct TsMaps { CUtensorMap e[3], r[3]; };
 /* one stage: NR rows of E, then NR rows of R, TS_COLS values each */
 template <class T> constexpr int ts_stage_elems() { return 2 * TS_NR * TS_COLS; }
 template <class T> constexpr int ts_stage_bytes() { return ts_stage_elems<T>() * (int)sizeof(T); }
-/* the R window: 12 slots of [parity][lane] pairs (the lane's even
- * columns, then its odd ones) */
+/* the R window: 6 slots of [parity][lane] pairs (the lane's even
+ * columns, then its odd ones); row r of the walk sits in slot
+ * (r - kw) mod 6 */
 constexpr int ts_wslot_elems() { return 2 * 32; }
-template <class T> constexpr int ts_win_bytes() { return 12 * ts_wslot_elems() * 2 * (int)sizeof(T); }
+template <class T> constexpr int ts_win_bytes() { return 6 * ts_wslot_elems() * 2 * (int)sizeof(T); }
 /* per warp: its ring, then its R window; after the warps', their mbarriers */
 template <class T> constexpr int ts_warp_bytes() { return TS_NS * ts_stage_bytes<T>() + ts_win_bytes<T>(); }
 template <class T> constexpr int ts_smem_bytes() { return TS_WARPS * (ts_warp_bytes<T>() + 8 * TS_NS); }
@@ -250,16 +251,20 @@ __device__ __forceinline__ void ts_issue(const TsMaps& maps, const TsArgs& g, un
 template <class T>
 struct TsTrip {
     unsigned cur, nxt;          /* shared-space address of this lane's columns in the slots of stages t, t+1 */
-    typename Pair<T>::t* win;   /* this lane's entry of window slot (2t) mod 6 */
+    typename Pair<T>::t* win;   /* this lane's entry of window slot b = 2 (t mod 3), which takes row 2t of the walk */
     int t;
+    int wrap;                   /* 6 - b: the window offsets m >= wrap lie at slot b + m - 6 */
 };
 template <class T>
 __device__ __forceinline__ void ts_trip(TsTrip<T>& tr, unsigned lane_ring, typename Pair<T>::t* lane_win, int t)
 {
+    static_assert(TS_NS == 3, "the window's slot follows the stage slot");
+    const int q = t % TS_NS;
     tr.t = t;
-    tr.cur = lane_ring + (unsigned)((t % TS_NS) * ts_stage_bytes<T>());
-    tr.nxt = lane_ring + (unsigned)(((t + 1) % TS_NS) * ts_stage_bytes<T>());
-    tr.win = lane_win + ((2 * t) % 6) * ts_wslot_elems();
+    tr.cur = lane_ring + (unsigned)(q * ts_stage_bytes<T>());
+    tr.nxt = lane_ring + (unsigned)((q == TS_NS - 1 ? 0 : q + 1) * ts_stage_bytes<T>());
+    tr.win = lane_win + 2 * q * ts_wslot_elems();
+    tr.wrap = 6 - 2 * q;
 }
 
 /* One row step, P = (r - kw) mod 2.  h1 = results of step r-1 (read only),
@@ -310,7 +315,6 @@ __device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTr
         ev.x = rr[0]; ev.y = rr[2]; od.x = rr[1]; od.y = rr[3];
         T2* w = tr.win + P * ts_wslot_elems();
         w[0] = ev; w[32] = od;
-        w[6 * ts_wslot_elems()] = ev; w[6 * ts_wslot_elems() + 32] = od;
     }
     /* neighbours from other lanes: even half h reads the left lane's last
      * odd column, odd half h the right lane's first even column */
@@ -329,7 +333,15 @@ __device__ __forceinline__ bool ts_step(const int r, const TsArgs& g, const TsTr
         /* R of row r-h at this half's columns */
         T2 rk;
         if (h == 0) { rk.x = rr[0]; rk.y = rr[2]; }
-        else rk = tr.win[(P + 6 - h) * ts_wslot_elems() + 32 * j0];
+        else {
+            /* row r-h sits at offset m = P + 6 - h (1..6) from slot b,
+             * wrapped into the 6 slots: m = 6 always wraps (slot b), m = 1
+             * never does (b <= 4), the others when m >= 6 - b */
+            const int m = P + 6 - h;
+            const T2* base = m == 6 ? tr.win - 6 * ts_wslot_elems()
+                           : (m == 1 ? tr.win : (m >= tr.wrap ? tr.win - 6 * ts_wslot_elems() : tr.win));
+            rk = base[m * ts_wslot_elems() + 32 * j0];
+        }
         T x0m, x0p, x1m, x1p, u0v, u1v;
         if (j0) {
             x0m = h1[h - 1][0]; x0p = h1[h - 1][1]; x1m = h1[h - 1][1]; x1p = nb[h];
@@ -472,10 +484,10 @@ __device__ __forceinline__ bool ts_assign(int gw, const TsPlan& pl, int& strip, 
     return ks < pl.rows;
 }
 
-/* Four blocks (eight warps) an SM; the shared memory of a block (two rings
- * and two R windows) allows no more. */
+/* Six blocks (twelve warps) an SM; the shared memory of a block (two rings
+ * and two R windows, 36.9 KB in FP64) allows no more. */
 template <class T, int S>
-__global__ void __launch_bounds__(32 * TS_WARPS, 4) k_mg_smooth_tma(const __grid_constant__ TsMaps maps, const __grid_constant__ MgConst m,
+__global__ void __launch_bounds__(32 * TS_WARPS, 6) k_mg_smooth_tma(const __grid_constant__ TsMaps maps, const __grid_constant__ MgConst m,
                                                       const __grid_constant__ MgLvlT<T> L, int l, TsPlan pl,
                                                       const double* __restrict__ inside0, DevStatus* st)
 {
@@ -674,11 +686,20 @@ int mg_smooth_tma(bcg_ctx* c, const MgConst& m, const MgLvlF& L, int l, int S, i
     return ts_launch<float>(c, m, L, l, S, target_warps, warm);
 }
 int mg_smooth_tma_slots() { return ts_slots<double>(); }
-/* a block's shared memory (two rings and two R windows) passes the 48 KB
- * that needs no opt-in */
+/* each form's dynamic shared memory, and the whole of the SM's shared
+ * memory for blocks (six FP64 blocks take 227.6 of its 228 KB with the
+ * per-block reserve) */
 int mg_smooth_tma_attributes()
 {
     const int d = ts_smem_bytes<double>(), f = ts_smem_bytes<float>();
+    const int all = cudaSharedmemCarveoutMaxShared;
+    if (cudaFuncSetAttribute(k_mg_smooth_tma<double, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, all) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<double, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, all) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<double, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, all) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<float, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, all) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<float, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, all) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mg_smooth_tma<float, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, all) != cudaSuccess)
+        return BCG_E_CUDA;
     if (cudaFuncSetAttribute(k_mg_smooth_tma<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, d) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_smooth_tma<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, d) != cudaSuccess ||
         cudaFuncSetAttribute(k_mg_smooth_tma<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, d) != cudaSuccess ||

@@ -306,6 +306,33 @@ def test_tma_smoother_warm_segments_agree_to_rounding():
         assert err < 1e-14, (nseg, err)
 
 
+def test_tma_smoother_r_window_slots():
+    """The R window of k_mg_smooth_tma (ts_trip, ts_step): 6 slots, row
+    2t + P of the walk written to slot b + P at trip t (b = 2 (t mod 3)),
+    and row r - h read at offset m = P + 6 - h from b, wrapped when
+    m >= 6 - b.  Every read must find the row it wants, in a slot no later
+    row has taken."""
+    slots = [None] * 6
+    for t in range(30):
+        q = t % 3
+        b, wrap = 2 * q, 6 - 2 * q
+        for P in (0, 1):
+            r = 2 * t + P
+            assert b + P < 6
+            slots[b + P] = r
+            for h in range(1, 6):
+                m = P + 6 - h
+                if m == 6:
+                    idx = b
+                elif m == 1:
+                    idx = b + 1
+                else:
+                    idx = b + m - 6 if m >= wrap else b + m
+                assert 0 <= idx < 6
+                if r - h >= 0:
+                    assert slots[idx] == r - h, (t, P, h)
+
+
 def native_level_int(x, X, lv):
     """csrc/nutrients.cu leg_native_level: the finest composite level whose
     extent holds column x of a level-lv row, in integers."""
