@@ -172,6 +172,8 @@ extern "C" int bcg_create(const bcg_params* p, bcg_ctx** out)
     c->kmax = p->max_neighbours;
     DALLOC(c->rec[0], cap * sizeof(CellRec));
     DALLOC(c->rec[1], cap * sizeof(CellRec));
+    c->stage_cells = c->cap < CTX_STAGE_CELLS ? (c->cap > 0 ? c->cap : 1) : CTX_STAGE_CELLS;
+    DALLOC(c->stage, (size_t)c->stage_cells * sizeof(bcg_cell));
     CellSoA& s = c->soa;
     DALLOC(s.ldiv, cap * 8); DALLOC(s.gr, cap * 8); DALLOC(s.tp, cap * 8); DALLOC(s.tq, cap * 8);
     DALLOC(s.ap, cap * 4); DALLOC(s.aq, cap * 4);
@@ -279,7 +281,7 @@ extern "C" int bcg_destroy(bcg_ctx* c)
 {
     if (!c) return BCG_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* ptrs[] = {c->rec[0], c->rec[1], c->soa.ldiv, c->soa.gr, c->soa.tp, c->soa.tq, c->soa.ap, c->soa.aq,
+    void* ptrs[] = {c->rec[0], c->rec[1], c->stage, c->soa.ldiv, c->soa.gr, c->soa.tp, c->soa.tq, c->soa.ap, c->soa.aq,
                     c->soa.dfx, c->soa.dfy, c->soa.dfz, c->soa.sfx, c->soa.sfy, c->soa.sfz, c->soa.type, c->soa.anc,
                     c->nbr, c->ncount, c->box_cnt, c->box_start, c->box_ids, c->cell_box, c->scan_tmp,
                     c->div_list, c->div_count, c->fcw_count, c->moved, c->delta_ids, c->delta_box, c->lineage,
@@ -323,11 +325,13 @@ extern "C" int bcg_destroy(bcg_ctx* c)
 /* ----------------------------------------------------------------------- */
 /* AoS <-> device layout                                                    */
 /* ----------------------------------------------------------------------- */
-__global__ void k_unpack(int n, const bcg_cell* __restrict__ in, CellRec* __restrict__ rec, CellSoA s)
+/* records in[0..n) are cells off..off+n-1 */
+__global__ void k_unpack(int n, int off, const bcg_cell* __restrict__ in, CellRec* __restrict__ rec, CellSoA s)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const bcg_cell& c = in[i];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const bcg_cell& c = in[j];
+    const int i = off + j;
     CellRec r;
     r.pL = make_double4(c.p.x, c.p.y, c.p.z, c.length);
     r.qR = make_double4(c.q.x, c.q.y, c.q.z, c.radius);
@@ -340,10 +344,12 @@ __global__ void k_unpack(int n, const bcg_cell* __restrict__ in, CellRec* __rest
     s.sfx[i] = c.sta_fric.x; s.sfy[i] = c.sta_fric.y; s.sfz[i] = c.sta_fric.z;
     s.type[i] = c.type; s.anc[i] = c.ancestor;
 }
-__global__ void k_pack(int n, bcg_cell* __restrict__ out, const CellRec* __restrict__ rec, CellSoA s)
+/* cells off..off+n-1 into out[0..n) */
+__global__ void k_pack(int n, int off, bcg_cell* __restrict__ out, const CellRec* __restrict__ rec, CellSoA s)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int i = off + j;
     bcg_cell c;
     CellRec r = rec[i];
     c.p.x = r.pL.x; c.p.y = r.pL.y; c.p.z = r.pL.z; c.length = r.pL.w;
@@ -355,29 +361,26 @@ __global__ void k_pack(int n, bcg_cell* __restrict__ out, const CellRec* __restr
     c.dyn_fric.x = s.dfx[i]; c.dyn_fric.y = s.dfy[i]; c.dyn_fric.z = s.dfz[i];
     c.sta_fric.x = s.sfx[i]; c.sta_fric.y = s.sfy[i]; c.sta_fric.z = s.sfz[i];
     c.type = s.type[i]; c.ancestor = s.anc[i];
-    out[i] = c;
+    out[j] = c;
 }
 
 void launch_pack_cells(bcg_ctx* c, bcg_cell* dst, cudaStream_t s, int moved)
 {
     if (c->n <= 0) return;
-    k_pack<<<(c->n + 255) / 256, 256, 0, s>>>(c->n, dst, c->rec[moved ? c->cur ^ 1 : c->cur], c->soa);
+    k_pack<<<(c->n + 255) / 256, 256, 0, s>>>(c->n, 0, dst, c->rec[moved ? c->cur ^ 1 : c->cur], c->soa);
     c->launches++;
 }
 
-/* the AoS staging buffer reuses the second record buffer's space when it is
- * large enough (208 B per cell vs 128 B per record), otherwise a transient
- * allocation */
+/* The records pass through the context's staging buffer a chunk at a
+ * time, copy and unpack in stream order (no allocation per call). */
 extern "C" int bcg_upload_cells(bcg_ctx* c, const bcg_cell* cells, int n)
 {
     if (!c || n < 0 || n > c->cap || (n > 0 && !cells)) return BCG_E_ARG;
-    if (n > 0) {
-        bcg_cell* dstage = nullptr;
-        BCG_CUDA_TRY(cudaMallocAsync((void**)&dstage, sizeof(bcg_cell) * (size_t)n, c->stream));
-        BCG_CUDA_TRY(cudaMemcpyAsync(dstage, cells, sizeof(bcg_cell) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-        k_unpack<<<(n + 255) / 256, 256, 0, c->stream>>>(n, dstage, c->rec[c->cur], c->soa);
+    for (int off = 0; off < n; off += c->stage_cells) {
+        const int m = n - off < c->stage_cells ? n - off : c->stage_cells;
+        BCG_CUDA_TRY(cudaMemcpyAsync(c->stage, cells + off, sizeof(bcg_cell) * (size_t)m, cudaMemcpyHostToDevice, c->stream));
+        k_unpack<<<(m + 255) / 256, 256, 0, c->stream>>>(m, off, c->stage, c->rec[c->cur], c->soa);
         c->launches++;
-        BCG_CUDA_TRY(cudaFreeAsync(dstage, c->stream));
     }
     BCG_CUDA_TRY(cudaMemsetAsync(c->ncount, 0, sizeof(int) * (size_t)c->cap, c->stream));
     c->n = n;
@@ -392,14 +395,12 @@ extern "C" int bcg_download_cells(bcg_ctx* c, bcg_cell* cells, int capacity, int
     if (!c) return BCG_E_ARG;
     if (n) *n = c->n;
     int m = c->n < capacity ? c->n : capacity;
-    if (m > 0) {
-        if (!cells) return BCG_E_ARG;
-        bcg_cell* dstage = nullptr;
-        BCG_CUDA_TRY(cudaMallocAsync((void**)&dstage, sizeof(bcg_cell) * (size_t)m, c->stream));
-        k_pack<<<(m + 255) / 256, 256, 0, c->stream>>>(m, dstage, c->rec[c->cur], c->soa);
+    if (m > 0 && !cells) return BCG_E_ARG;
+    for (int off = 0; off < m; off += c->stage_cells) {
+        const int k = m - off < c->stage_cells ? m - off : c->stage_cells;
+        k_pack<<<(k + 255) / 256, 256, 0, c->stream>>>(k, off, c->stage, c->rec[c->cur], c->soa);
         c->launches++;
-        BCG_CUDA_TRY(cudaMemcpyAsync(cells, dstage, sizeof(bcg_cell) * (size_t)m, cudaMemcpyDeviceToHost, c->stream));
-        BCG_CUDA_TRY(cudaFreeAsync(dstage, c->stream));
+        BCG_CUDA_TRY(cudaMemcpyAsync(cells + off, c->stage, sizeof(bcg_cell) * (size_t)k, cudaMemcpyDeviceToHost, c->stream));
     }
     return ctx_check_status(c);
 }

@@ -6,6 +6,8 @@
 
 #define BCG_MAX_MG_LEVELS 16
 #define BCG_MAX_AGAR_LEVELS 8
+/* records a context's host<->device staging buffer holds (27 MB) */
+#define CTX_STAGE_CELLS (1 << 17)
 
 /* one multigrid level: three species, Sol/Res/Err, (nx+1) x (nz+1) points
  * stored k-major (row k holds i = 0..nx contiguously, row pitch `pitch`) */
@@ -45,6 +47,10 @@ struct bcg_ctx {
     int cur;               /* index of the "old" record buffer */
     CellRec* rec[2];
     CellSoA soa;
+    /* reference-layout records between host and device: uploads and
+     * downloads pass through it stage_cells records at a time */
+    bcg_cell* stage;
+    int stage_cells;
     /* neighbours */
     int kmax;
     int* nbr;

@@ -75,3 +75,23 @@ def test_overfull_box_is_reported(gpu):
         col.rebuild_neighbours()
         col.synchronize()
     assert e.value.code == _abi.E_BOX_OVERFLOW
+
+
+def test_upload_download_round_trip_in_chunks(gpu):
+    """Records pass between host and device through the context's staging
+    buffer, 131,072 at a time: a ragged count, a download into a smaller
+    buffer and a second, shorter upload all come back byte for byte."""
+    p = params.workload_params("scale_262k")
+    cells = np.ascontiguousarray(workload_colony("scale_262k"))[:262144 - 12345]
+    col = Colony(p, cells)
+    assert col.n_cells() == len(cells)
+    assert col.cells().tobytes() == cells.tobytes()
+    part = np.zeros(140000, dtype=_abi.CELL_DTYPE)
+    got = ctypes.c_int()
+    _abi.check(col.lib.bcg_download_cells(col.h, _abi.ptr(part), len(part), ctypes.byref(got)), "download")
+    assert got.value == len(cells)
+    assert part.tobytes() == cells[:len(part)].tobytes()
+    short = cells[1000:1000 + 131073]
+    col.upload(short)
+    assert col.cells().tobytes() == short.tobytes()
+    col.close()
