@@ -33,7 +33,7 @@
  *
  * Staging: the rows of E (the correction before smoothing) and R (the
  * right-hand side) of the strip arrive as 128 x NR boxes through plain
- * (non-multicast) cp.async.bulk.tensor loads into a ring of NS stages per
+ * cp.async.bulk.tensor loads, each into its own CTA, into a ring of NS stages per
  * warp, each stage with an mbarrier that its loads complete; the copy
  * engine zero-fills columns and rows outside the level, which is the value
  * the stencil reads there.  A step reads E at row r+1 and R at row r from
