@@ -159,9 +159,13 @@ int bcg_synchronize(bcg_ctx* ctx);
 /* cells                                                                */
 /* ------------------------------------------------------------------ */
 /* Replace the colony with n cells (AoS records, host memory); replaces
- * LoadCells' copy + Grid.Add (InputOutput.cpp:394-431). */
+ * LoadCells' copy + Grid.Add (InputOutput.cpp:394-431).  Records pass
+ * through the context's staging buffer (created with it, up to 131,072
+ * records) a chunk at a time; nothing is allocated per call.  Pinned host
+ * memory gives the full copy rate. */
 int bcg_upload_cells(bcg_ctx* ctx, const bcg_cell* cells, int n);
-/* Copy the colony back as AoS records; *n receives the cell count. */
+/* Copy the first min(n, capacity) cells back as AoS records through the
+ * same staging buffer; *n receives the cell count. */
 int bcg_download_cells(bcg_ctx* ctx, bcg_cell* cells, int capacity, int* n);
 int bcg_num_cells(bcg_ctx* ctx, int* n);
 
