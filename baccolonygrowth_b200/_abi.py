@@ -210,6 +210,8 @@ PROTOTYPES = {
     "bcg_steady_vjp": (_I, [_VP, _PD, _PD, _PD, _D]),
     "bcg_enable_timers": (_I, [_VP, _I]),
     "bcg_get_timer": (_I, [_VP, _I, _PD, _PI64]),
+    "bcg_timeline_enable": (_I, [_VP, _I]),
+    "bcg_timeline_read": (_I, [_VP, _PI, _PF, _I, _PI]),
     "bcg_rng_seed": (None, [ctypes.POINTER(Rng), ctypes.c_uint32]),
     "bcg_rng_next": (ctypes.c_int32, [ctypes.POINTER(Rng)]),
     "bcg_rng_skip": (None, [ctypes.POINTER(Rng), ctypes.c_int64]),

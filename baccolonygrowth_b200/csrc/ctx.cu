@@ -115,6 +115,65 @@ extern "C" int bcg_get_timer(bcg_ctx* c, int t, double* ms, int64_t* launches)
     return BCG_OK;
 }
 
+static void timeline_free(bcg_ctx* c)
+{
+    for (int i = 0; i < c->tl_cap; i++)
+        if (c->tl_ev[i]) cudaEventDestroy(c->tl_ev[i]);
+    free(c->tl_ev);
+    free(c->tl_tag);
+    c->tl_ev = nullptr;
+    c->tl_tag = nullptr;
+    c->tl_cap = c->tl_n = 0;
+}
+
+extern "C" int bcg_timeline_enable(bcg_ctx* c, int capacity)
+{
+    if (!c || capacity < 0) return BCG_E_ARG;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->aux_stream) cudaStreamSynchronize(c->aux_stream);
+    timeline_free(c);
+    if (capacity == 0) return BCG_OK;
+    c->tl_ev = (cudaEvent_t*)calloc((size_t)capacity, sizeof(cudaEvent_t));
+    c->tl_tag = (int*)calloc((size_t)capacity, sizeof(int));
+    if (!c->tl_ev || !c->tl_tag) { free(c->tl_ev); free(c->tl_tag); c->tl_ev = nullptr; c->tl_tag = nullptr; return BCG_E_ARG; }
+    c->tl_cap = capacity;
+    for (int i = 0; i < capacity; i++) {
+        if (cudaEventCreate(&c->tl_ev[i]) != cudaSuccess) {
+            g_last_cuda = cudaGetLastError();
+            timeline_free(c);
+            return BCG_E_CUDA;
+        }
+    }
+    return BCG_OK;
+}
+
+/* one mark on the context's stream (aux = 0) or its second stream */
+extern "C" void bcg_int_tl_mark(bcg_ctx* c, int aux, int tag)
+{
+    if (!c || c->tl_n >= c->tl_cap) return;
+    if (cudaEventRecord(c->tl_ev[c->tl_n], aux ? c->aux_stream : c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    c->tl_tag[c->tl_n++] = tag;
+}
+
+extern "C" int bcg_timeline_read(bcg_ctx* c, int* tags, float* ms, int capacity, int* n)
+{
+    if (!c || capacity < 0 || (capacity > 0 && (!tags || !ms))) return BCG_E_ARG;
+    if (c->aux_stream) BCG_CUDA_TRY(cudaStreamSynchronize(c->aux_stream));
+    const int rc = ctx_check_status(c);
+    const int m = c->tl_n < capacity ? c->tl_n : capacity;
+    for (int i = 0; i < m; i++) {
+        tags[i] = c->tl_tag[i];
+        ms[i] = 0.0f;
+        BCG_CUDA_TRY(cudaEventElapsedTime(&ms[i], c->tl_ev[0], c->tl_ev[i]));
+    }
+    if (n) *n = m;
+    c->tl_n = 0;
+    return rc;
+}
+
 extern "C" void* bcg_stream(bcg_ctx* c) { return c ? (void*)c->stream : nullptr; }
 extern "C" int bcg_synchronize(bcg_ctx* c) { return c ? ctx_check_status(c) : BCG_E_ARG; }
 extern "C" long long bcg_kernel_launches(bcg_ctx* c) { return c ? c->launches : 0; }
@@ -313,6 +372,7 @@ extern "C" int bcg_destroy(bcg_ctx* c)
     for (int g = 0; g < 2; g++) if (c->nutrient_graph[g]) cudaGraphExecDestroy(c->nutrient_graph[g]);
     if (c->solve_graph) cudaGraphExecDestroy(c->solve_graph);
     if (c->pinned) cudaFreeHost(c->pinned);
+    timeline_free(c);
     for (int t = 0; t < BCG_T_COUNT; t++) { if (c->ev[t][0]) cudaEventDestroy(c->ev[t][0]); if (c->ev[t][1]) cudaEventDestroy(c->ev[t][1]); }
     if (c->aux_stream) { cudaStreamSynchronize(c->aux_stream); cudaStreamDestroy(c->aux_stream); }
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);

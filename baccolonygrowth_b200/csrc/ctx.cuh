@@ -119,6 +119,10 @@ struct bcg_ctx {
     cudaEvent_t ev_fork, ev_join;
     /* timers */
     int timers_on;
+    /* step timeline (bcg_timeline_*): tl_cap events, tl_n of them recorded */
+    cudaEvent_t* tl_ev;
+    int* tl_tag;
+    int tl_cap, tl_n;
     cudaEvent_t ev[BCG_T_COUNT][2];
     double timer_ms[BCG_T_COUNT];
     long long timer_launches[BCG_T_COUNT];

@@ -22,6 +22,9 @@ int bcg_int_mg_solve_launch(bcg_ctx* ctx, int vcycles);
 int bcg_int_mg_solve_aside(bcg_ctx* ctx, int vcycles);
 /* order the context's stream after its second stream's work */
 int bcg_int_join(bcg_ctx* ctx);
+/* a step-timeline mark (bcg_timeline_tag) on the context's stream (aux 0)
+ * or its second stream; nothing when no timeline is running */
+void bcg_int_tl_mark(bcg_ctx* ctx, int aux, int tag);
 
 /* Output-step snapshots (output.cu), used by the writer (writer.cpp).
  * One snapshot is a byte image laid out by bcg_out_layout: cell records,

@@ -1845,8 +1845,10 @@ extern "C" int bcg_int_mg_solve_aside(bcg_ctx* c, int vcycles)
     BCG_CUDA_TRY(cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
     if (c->timers_on) cudaEventRecord(c->ev[BCG_T_MG_SOLVE][0], c->aux_stream);
     long long l0 = c->launches;
+    bcg_int_tl_mark(c, 1, BCG_TL_SOLVE_BEGIN);
     int rc = mg_solve_graphed(c, vcycles, 0, c->aux_stream);
     if (rc) return rc;
+    bcg_int_tl_mark(c, 1, BCG_TL_SOLVE_END);
     c->timer_launches[BCG_T_MG_SOLVE] += (int)(c->launches - l0);
     if (c->timers_on) {
         cudaEventRecord(c->ev[BCG_T_MG_SOLVE][1], c->aux_stream);

@@ -147,6 +147,7 @@ static int sim_step_body(bcg_sim* s, bool* aside)
     int rc;
     const bool out = s->reference_cadence && s->out_flag;
     int64_t stress_calls = 0;
+    bcg_int_tl_mark(s->ctx, 0, BCG_TL_STEP);
     if (s->reference_cadence) {
         if (s->update_flag) {
             s->update_flag = false;
@@ -184,7 +185,9 @@ static int sim_step_body(bcg_sim* s, bool* aside)
     }
     int nd = 0;
     int64_t calls = 0;
+    bcg_int_tl_mark(s->ctx, 0, BCG_TL_MECH_BEGIN);
     if ((rc = bcg_move_grow(s->ctx, s->dt, &nd, &calls))) return rc;
+    bcg_int_tl_mark(s->ctx, 0, BCG_TL_MECH_END);
     if (out) {
         s->out_flag = false;
         if (s->writer && (rc = bcg_output_fields(s->writer, s->ctx, s->koutput, s->t, s->dt))) return rc;
@@ -195,6 +198,7 @@ static int sim_step_body(bcg_sim* s, bool* aside)
     s->lineage.resize(base + 2 * (size_t)(nd > 0 ? nd : 0));
     int done = 0;
     rc = bcg_divide(s->ctx, s->draws.data(), nd, s->t, &done, nd > 0 ? s->lineage.data() + base : nullptr);
+    bcg_int_tl_mark(s->ctx, 0, BCG_TL_DIVIDE_END);
     if (s->writer && done > 0) {
         int lrc = bcg_writer_lineage(s->writer, s->lineage.data() + base, done);
         if (lrc && !rc) rc = lrc;
@@ -211,6 +215,7 @@ static int sim_step(bcg_sim* s)
     if (aside) {
         const int jr = bcg_int_join(s->ctx);
         if (!rc) rc = jr;
+        bcg_int_tl_mark(s->ctx, 0, BCG_TL_STEP_END);
     }
     return rc;
 }

@@ -436,6 +436,31 @@ typedef enum bcg_timer_id {
 int bcg_enable_timers(bcg_ctx* ctx, int on);
 int bcg_get_timer(bcg_ctx* ctx, int timer, double* ms, int64_t* launches);
 
+/* Step timeline: CUDA events recorded at the phases of each bcg_sim step,
+ * on the stream each phase runs on.  Unlike the timers above it never
+ * synchronises, so the benchmark cadence's solve still runs beside the
+ * mechanics.  Marks past the capacity are dropped.  The first solve from a
+ * starting state runs in order on the context stream (it is captured as a
+ * graph from the second one on): that step's two solve marks bracket
+ * nothing. */
+typedef enum bcg_timeline_tag {
+    BCG_TL_STEP = 1,          /* step start (context stream) */
+    BCG_TL_SOLVE_BEGIN = 2,   /* agar solve queued on the second stream: its start */
+    BCG_TL_SOLVE_END = 3,     /* its end (second stream) */
+    BCG_TL_MECH_BEGIN = 4,    /* before MoveCell + GrowCell (context stream) */
+    BCG_TL_MECH_END = 5,      /* after their counters were read back */
+    BCG_TL_DIVIDE_END = 6,    /* after the division loop */
+    BCG_TL_STEP_END = 7       /* context stream after it waited for the solve */
+} bcg_timeline_tag;
+/* capacity > 0: (re)start a timeline of up to `capacity` marks; 0: stop
+ * and release its events. */
+int bcg_timeline_enable(bcg_ctx* ctx, int capacity);
+/* Wait for the context's streams, then give the marks so far in the order
+ * they were queued: tags[i] and ms[i], the time since the first mark
+ * (at most `capacity` of them, *n = their count).  The timeline restarts
+ * empty. */
+int bcg_timeline_read(bcg_ctx* ctx, int* tags, float* ms, int capacity, int* n);
+
 /* ------------------------------------------------------------------ */
 /* host helpers                                                         */
 /* ------------------------------------------------------------------ */

@@ -98,3 +98,42 @@ def test_overlapped_solve_equals_sequential(gpu):
     assert cells_a == cells_b
     assert np.array_equal(lin_a, lin_b)
     assert len(lin_a) > 0
+
+
+def test_timeline_marks_steps_without_changing_them(gpu):
+    """bcg_timeline_*: every step of the benchmark cadence queues its seven
+    marks in order; times rise along each stream, the step ends after its
+    solve and before the next step starts; a run with the timeline equals
+    one without, and a read empties the timeline."""
+    lib = _abi.load()
+    p = params.workload_params("scale_262k")
+    cells = np.ascontiguousarray(workload_colony("scale_262k", n=20000, seed=21))
+    sim, ctx = sim_with(lib, p, cells, 21, 1)
+    _abi.check(lib.bcg_timeline_enable(ctx, 256), "timeline")
+    _abi.check(lib.bcg_sim_run(sim, STEPS), "run")
+    tags = np.zeros(256, dtype=np.int32)
+    ms = np.zeros(256, dtype=np.float32)
+    n = ctypes.c_int()
+    _abi.check(lib.bcg_timeline_read(ctx, _abi.ptr(tags, ctypes.c_int), _abi.ptr(ms, ctypes.c_float), 256,
+                                     ctypes.byref(n)), "read")
+    assert n.value == 7 * STEPS
+    assert list(tags[:n.value]) == [1, 2, 3, 4, 5, 6, 7] * STEPS
+    t = ms[:n.value].reshape(STEPS, 7).astype(np.float64)
+    main = t[:, [0, 3, 4, 5, 6]].ravel()
+    assert np.all(np.diff(main) >= 0)
+    assert np.all(np.diff(t[:, [1, 2]].ravel()) >= 0)
+    assert np.all(t[:, 6] >= t[:, 2] - 1e-3)
+    n2 = ctypes.c_int(-1)
+    _abi.check(lib.bcg_timeline_read(ctx, _abi.ptr(tags, ctypes.c_int), _abi.ptr(ms, ctypes.c_float), 256,
+                                     ctypes.byref(n2)), "read again")
+    assert n2.value == 0
+    _abi.check(lib.bcg_timeline_enable(ctx, 0), "stop")
+    cells_a, lin_a = cells_and_lineage(lib, sim, 2 * len(cells))
+    lib.bcg_sim_destroy(sim)
+
+    sim0, _ = sim_with(lib, p, cells, 21, 1)
+    _abi.check(lib.bcg_sim_run(sim0, STEPS), "run")
+    cells_b, lin_b = cells_and_lineage(lib, sim0, 2 * len(cells))
+    lib.bcg_sim_destroy(sim0)
+    assert cells_a == cells_b
+    assert np.array_equal(lin_a, lin_b)
