@@ -306,6 +306,46 @@ def profiled_traffic(summary, workload):
     return total, "ncu capture of one launch of the same source (profiles/%s), not this run" % summary
 
 
+def timeline_summary(tags, ms):
+    """Median phase ends of the steps whose seven marks (bcg_timeline_tag)
+    all came back, in ms from each step's start; the period is the start
+    of one step to the start of the next."""
+    import numpy as np
+    steps, cur = [], None
+    for t, m in zip(tags, ms):
+        if t == 1:
+            cur = {}
+            steps.append(cur)
+        if cur is not None:
+            cur[int(t)] = float(m)
+    full = [s for s in steps if len(s) == 7]
+    if not full:
+        return None
+    rel = lambda k: float(np.median([s[k] - s[1] for s in full]))
+    periods = [steps[i + 1][1] - steps[i][1] for i in range(len(steps) - 1) if len(steps[i]) == 7]
+    return {"steps": len(full), "solve_end_ms": rel(3), "move_grow_end_ms": rel(5), "divide_end_ms": rel(6),
+            "step_end_ms": rel(7), "period_ms": float(np.median(periods)) if periods else None,
+            "source": "bcg_timeline marks, median over the steps"}
+
+
+def timeline_bench(lib, sim, ctx, steps):
+    """`steps` steps of the bench schedule with the step timeline on."""
+    import numpy as np
+    from baccolonygrowth_b200 import _abi
+    cap = 7 * steps + 8
+    _abi.check(lib.bcg_timeline_enable(ctx, cap), "timeline")
+    try:
+        _abi.check(lib.bcg_sim_run(sim, steps), "timeline steps")
+        tags = np.zeros(cap, dtype=np.int32)
+        ms = np.zeros(cap, dtype=np.float32)
+        n = ctypes.c_int()
+        _abi.check(lib.bcg_timeline_read(ctx, _abi.ptr(tags, ctypes.c_int), _abi.ptr(ms, ctypes.c_float), cap,
+                                         ctypes.byref(n)), "timeline read")
+    finally:
+        lib.bcg_timeline_enable(ctx, 0)
+    return timeline_summary(tags[:n.value], ms[:n.value])
+
+
 def sim_rebuilds(lib, sim):
     r = ctypes.c_int64()
     f = ctypes.c_int64()
@@ -806,6 +846,13 @@ def b200_arm(args):
         lib.bcg_get_timer(ctx, tid, ctypes.byref(msx), ctypes.byref(nl))
         timers[name] = msx.value / kt_steps
     _abi.check(lib.bcg_enable_timers(ctx, 0), "timers off")
+    # the same schedule with its phases marked by CUDA events on the stream
+    # each phase runs on (bcg_timeline_*), which do not synchronise: where
+    # the overlapped step's time goes
+    try:
+        step_timeline = timeline_bench(lib, sim, ctx, 10)
+    except Exception as e:      # reported, not required
+        step_timeline = {"error": str(e)}
     # MoveCell + GrowCell with the contact search in FP32 (the precision
     # form), same schedule, device time per step against the FP64 search
     pair32 = None
@@ -1004,6 +1051,7 @@ def b200_arm(args):
         "mean_neighbours": k_mean_measured,
         "dense_mechanics": dense,
         "kernel_ms_per_step": timers,
+        "step_timeline": step_timeline,
         "divisions": d_.value,
         "roofline": roof,
         "roofline_mg_solve": roof_mg,

@@ -6,7 +6,9 @@ that summary names the digest of the kernel's current source file
   file that exists, and its digest is the file's current one;
 - the dominant kernel's summary yields its DRAM bytes;
 - a summary whose digest does not match, or of another workload, yields no
-  bytes.
+  bytes;
+- the step-timeline summary of the bench line takes the medians of the
+  complete steps.
 """
 import os
 import re
@@ -55,3 +57,22 @@ def test_mismatched_digest_or_workload_gives_no_bytes(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "ROOT", ROOT)
     traffic, src = bench.profiled_traffic("k_mg_smooth_tma_mixed_1m.md", "scale_262k")
     assert traffic is None
+
+
+def test_timeline_summary():
+    """bench.timeline_summary: median phase ends of the steps whose seven
+    marks came back, relative to each step's start, and the median period;
+    a step cut short by the capacity is left out."""
+    import numpy as np
+    step = [0.0, 0.01, 2.28, 0.01, 0.47, 1.0, 2.29]
+    tags, ms = [], []
+    for k in range(3):
+        tags += [1, 2, 3, 4, 5, 6, 7]
+        ms += [v + 2.3 * k for v in step]
+    tags += [1, 2]
+    ms += [6.9, 6.91]
+    out = bench.timeline_summary(np.array(tags, np.int32), np.array(ms, np.float32))
+    assert out["steps"] == 3
+    assert abs(out["solve_end_ms"] - 2.28) < 1e-5 and abs(out["divide_end_ms"] - 1.0) < 1e-5
+    assert abs(out["period_ms"] - 2.3) < 1e-5
+    assert bench.timeline_summary(np.zeros(0, np.int32), np.zeros(0, np.float32)) is None
